@@ -23,6 +23,10 @@
 
 extern "C" {
 
+// The same definitions appear in spai_b200.h; the guard lets both headers be
+// included together.
+#ifndef SPAI_ABI_STRUCTS_DEFINED
+#define SPAI_ABI_STRUCTS_DEFINED
 struct MatrixData {
   int64_t rows;
   int64_t cols;
@@ -63,6 +67,7 @@ struct Result {
   SingleIterationData* history;
   char* error_message;
 };
+#endif  // SPAI_ABI_STRUCTS_DEFINED
 
 // Global SPAI conjugate gradient   (reference src/global_spai/conjugate_gradient.cpp:15-83)
 Result spai_global_cg(MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params);

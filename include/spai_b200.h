@@ -1,0 +1,143 @@
+#ifndef SPAI_B200_H_
+#define SPAI_B200_H_
+/*
+ * Extensions of the drop-in C ABI (methods_c_api.h) served by libspai_b200.so.
+ * C-clean: every declaration is extern "C" with plain pointers and sizes.
+ * The structs MatrixData / MethodParams / SingleIterationData / Result are
+ * the ones of methods_c_api.h, repeated here under an include guard so C
+ * callers can use this header alone.
+ *
+ * Errors: functions returning Result put the message in error_message (the
+ * reference's convention, methods_c_api.cpp:59-64); the others return a
+ * negative value and copy the message into the caller's `error` buffer.
+ */
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same layout as methods_c_api.h (reference include/methods_c_api.h:7-46). */
+#ifndef SPAI_ABI_STRUCTS_DEFINED
+#define SPAI_ABI_STRUCTS_DEFINED
+struct MatrixData {
+  int64_t rows;
+  int64_t cols;
+  int64_t nnz;
+  const int64_t* col_offsets;
+  const int64_t* row_indices;
+  const double* values;
+};
+struct MethodParams {
+  int64_t max_iterations;
+  double tolerance;
+  double max_density;
+  int64_t enable_dropping;
+  int64_t num_threads;
+  int64_t use_initial_m;
+  int64_t use_preconditioner;
+  int64_t inner_iterations;
+};
+struct SingleIterationData {
+  int64_t iteration;
+  double residual_norm;
+  double density_m;
+  double density_direction;
+};
+struct Result {
+  int64_t rows;
+  int64_t cols;
+  int64_t nnz;
+  int64_t iterations;
+  int64_t converged;
+  int64_t history_size;
+  int64_t* col_offsets;
+  int64_t* row_indices;
+  double* values;
+  struct SingleIterationData* history;
+  char* error_message;
+};
+#endif
+
+/* Precision and selection knobs that the reference's MethodParams lacks. */
+typedef struct SpaiExtParams {
+  int64_t precision;       /* 0: FP64 storage (bit-compatible with the reference's arithmetic order inside each
+                              column); 1: FP32 storage of M, R, Z, P, A with FP64 reductions */
+  int64_t topk_per_column; /* 0: the reference's global budget max(n, floor(max_density*n^2)) (dropping.cpp:122-224);
+                              K > 0: keep at most K entries per column by magnitude (diagonal of M protected) */
+  int64_t device;          /* CUDA device ordinal; -1: the calling thread's current device */
+  int64_t reserved;        /* must be 0 */
+} SpaiExtParams;
+
+/* Method ids for spai_run_ex / sessions. */
+enum {
+  SPAI_GLOBAL_CG = 0,
+  SPAI_GLOBAL_MR = 1,
+  SPAI_GLOBAL_LOMR = 2,
+  SPAI_INNER_OUTER_MR = 3,
+  SPAI_INNER_OUTER_LOMR = 4
+};
+
+/* One call of any method with the extension knobs; ext may be NULL (FP64,
+ * global budget, current device).  Replaces the five reference entry points
+ * of methods_c_api.h:48-56 (same inputs, same Result ownership via free_mem). */
+struct Result spai_run_ex(int64_t method, struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                          struct MethodParams params, const SpaiExtParams* ext);
+
+typedef struct PcgParams {
+  int64_t max_iterations; /* length limit of the history, initial entry included (backward_error.pyx:69-72) */
+  double tolerance;       /* relative residual ||r|| / ||b|| */
+  int64_t refresh_period; /* 0: the reference's refresh at convergence only; K > 0: also r = b - A x every K steps */
+  int64_t m_precision;    /* 0: M applied in FP64; 1: M stored in FP32, vectors and dots in FP64 */
+  int64_t device;         /* CUDA device ordinal; -1: current device */
+} PcgParams;
+
+/* PCG with x0 = 0 on CSR A and CSR M (int64 indices), the device form of the
+ * reference's methods_cython/backward_error.pyx:69-144 `pcg`.  history must
+ * hold params.max_iterations doubles; returns the number of entries written
+ * (history[0] = 1), sets *status to 0 (iteration limit), 1 (converged),
+ * 2 (recurrence breakdown) or 3 (non-finite residual); x_out (n doubles) may
+ * be NULL.  Returns -1 and fills `error` on invalid input or CUDA failure. */
+int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, const int64_t* a_offsets,
+                 const double* m_values, const int64_t* m_indices, const int64_t* m_offsets, const double* b,
+                 PcgParams params, double* history, int64_t* status, double* x_out, char* error,
+                 int64_t error_capacity);
+
+/* y = A x for CSR A (backward_error.pyx:56-66 `matvec`); returns 0, or -1 with `error`. */
+int64_t spai_matvec(int64_t n, const double* values, const int64_t* indices, const int64_t* offsets,
+                    const double* x, double* y, int64_t device, char* error, int64_t error_capacity);
+
+/* ---- Sessions: the problem stays resident in HBM across repeated runs ---- */
+typedef struct SpaiSession SpaiSession;
+
+/* Validates and uploads A (and M0 / Pr when params.use_initial_m /
+ * use_preconditioner), builds the row-compressed copy of A, the column norms
+ * and the preconditioner.  Returns NULL and fills `error` on failure. */
+SpaiSession* spai_session_create(int64_t method, struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                                 struct MethodParams params, const SpaiExtParams* ext, char* error,
+                                 int64_t error_capacity);
+/* Runs the method from M0 on the resident problem; M stays on the device.
+ * Returns 0 (sets *iterations, *converged, *nnz_m), or -1 with `error`. */
+int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* converged, int64_t* nnz_m,
+                         char* error, int64_t error_capacity);
+/* Copies up to `capacity` history rows of the last run; returns the row count. */
+int64_t spai_session_history(SpaiSession* session, struct SingleIterationData* out, int64_t capacity);
+/* M of the last run as a Result (free with free_mem). */
+struct Result spai_session_result(SpaiSession* session);
+/* Uploads the right-hand side b (n doubles) used by spai_session_pcg. */
+int64_t spai_session_set_rhs(SpaiSession* session, const double* b, char* error, int64_t error_capacity);
+/* PCG on the resident A, the M of the last run (row-compressed on the device,
+ * FP32 when params.m_precision == 1) and the resident b.  Same outputs as
+ * spai_pcg (x_out may be NULL). */
+int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history, int64_t* status, double* x_out,
+                         char* error, int64_t error_capacity);
+void spai_session_destroy(SpaiSession* session);
+
+/* Number of kernels this library has launched since load (diagnostics). */
+int64_t spai_kernel_launches(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPAI_B200_H_ */

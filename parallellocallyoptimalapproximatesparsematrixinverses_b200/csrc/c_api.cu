@@ -1,0 +1,451 @@
+// C-ABI entry points of libspai_b200.so: the reference's five methods and
+// free_mem (include/methods_c_api.h), plus the extensions of spai_b200.h.
+// Every entry point converts exceptions into the reference's error
+// convention; nothing throws across the boundary.
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstring>
+#include <exception>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/methods_c_api.h"
+#include "../../include/spai_b200.h"
+#include "device.cuh"
+#include "ops.cuh"
+#include "pcg.cuh"
+#include "solver.cuh"
+
+namespace spai {
+
+namespace {
+std::atomic<int64_t> g_launches{0};
+}  // namespace
+
+void CountLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+namespace {
+
+void CopyError(const std::string& message, char* out, int64_t capacity) {
+  if (out == nullptr || capacity <= 0) return;
+  const size_t n = std::min<size_t>(message.size(), static_cast<size_t>(capacity - 1));
+  std::memcpy(out, message.data(), n);
+  out[n] = '\0';
+}
+
+Result ErrorResult(const std::string& message) {
+  Result out{};
+  out.error_message = new char[message.size() + 1];
+  std::memcpy(out.error_message, message.c_str(), message.size() + 1);
+  return out;
+}
+
+// GetSuccessResult (methods_c_api.cpp:66-114): host arrays allocated with new[].
+Result SuccessResult(const SolveOutput& s) {
+  Result out{};
+  out.rows = s.rows;
+  out.cols = s.cols;
+  out.nnz = static_cast<int64_t>(s.idx.size());
+  out.iterations = s.iterations;
+  out.converged = s.converged ? 1 : 0;
+  out.history_size = static_cast<int64_t>(s.history.size());
+  try {
+    out.col_offsets = new int64_t[s.cols + 1];
+    out.row_indices = new int64_t[out.nnz];
+    out.values = new double[out.nnz];
+    out.history = new SingleIterationData[s.history.size()];
+  } catch (...) {
+    delete[] out.col_offsets;
+    delete[] out.row_indices;
+    delete[] out.values;
+    delete[] out.history;
+    throw;
+  }
+  std::memcpy(out.col_offsets, s.ptr.data(), sizeof(int64_t) * (s.cols + 1));
+  if (out.nnz > 0) {
+    std::memcpy(out.row_indices, s.idx.data(), sizeof(int64_t) * out.nnz);
+    std::memcpy(out.values, s.val.data(), sizeof(double) * out.nnz);
+  }
+  for (size_t i = 0; i < s.history.size(); ++i) out.history[i] = s.history[i];
+  return out;
+}
+
+int ResolveDevice(int64_t requested) {
+  int count = 0;
+  const cudaError_t err = cudaGetDeviceCount(&count);
+  if (err != cudaSuccess || count == 0) {
+    throw CudaError("no CUDA device is available to libspai_b200 (" + std::string(cudaGetErrorString(err)) + ")");
+  }
+  if (requested < 0) {
+    int current = 0;
+    SPAI_CUDA(cudaGetDevice(&current));
+    return current;
+  }
+  if (requested >= count) throw std::invalid_argument("device ordinal out of range");
+  return static_cast<int>(requested);
+}
+
+struct CtxGuard {
+  Ctx ctx;
+  explicit CtxGuard(int device) { ctx.Init(device); }
+  ~CtxGuard() { ctx.Destroy(); }
+};
+
+struct Inputs {
+  HostCsc a;
+  HostCsc m0;
+  HostCsc pr;
+  bool has_m0 = false;
+  bool has_pr = false;
+};
+
+SolveOptions CheckInputs(int64_t method, const MatrixData& A, const MatrixData& M0, const MatrixData& Pr,
+                         const MethodParams& params, const SpaiExtParams* ext, Inputs& in) {
+  if (method < 0 || method > 4) throw std::invalid_argument("unknown method id");
+  in.a = CheckedMatrix(A);
+  in.has_m0 = params.use_initial_m != 0;
+  if (in.has_m0) in.m0 = CheckedMatrix(M0);
+  in.has_pr = params.use_preconditioner != 0;
+  if (in.has_pr) in.pr = CheckedMatrix(Pr);
+  const bool inner_outer = method >= 3;
+  if (inner_outer && params.inner_iterations <= 0) {
+    throw std::invalid_argument("inner_iterations must be positive");
+  }
+  ValidateProblem(in.a, in.has_m0 ? &in.m0 : nullptr, in.has_pr ? &in.pr : nullptr, params);
+  SolveOptions opt;
+  opt.method = static_cast<Method>(method);
+  opt.max_iterations = params.max_iterations;
+  opt.tolerance = params.tolerance;
+  opt.max_density = params.max_density;
+  opt.dropping = params.enable_dropping != 0;
+  opt.inner_iterations = params.inner_iterations;
+  if (ext != nullptr) {
+    if (ext->precision != 0 && ext->precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
+    if (ext->topk_per_column < 0) throw std::invalid_argument("topk_per_column must be non-negative");
+    if (ext->reserved != 0) throw std::invalid_argument("SpaiExtParams.reserved must be 0");
+    opt.precision = static_cast<int>(ext->precision);
+    opt.topk = ext->topk_per_column;
+  }
+  return opt;
+}
+
+Result RunMethod(int64_t method, MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params,
+                 const SpaiExtParams* ext) {
+  try {
+    Inputs in;
+    const SolveOptions opt = CheckInputs(method, A, M0, Pr, params, ext, in);
+    CtxGuard guard(ResolveDevice(ext != nullptr ? ext->device : -1));
+    auto solver = MakeSolver(guard.ctx, opt);
+    solver->Upload(in.a, in.has_m0 ? &in.m0 : nullptr, in.has_pr ? &in.pr : nullptr);
+    solver->Run();
+    SolveOutput out;
+    solver->Download(out);
+    return SuccessResult(out);
+  } catch (const std::exception& ex) {
+    return ErrorResult(ex.what());
+  } catch (...) {
+    return ErrorResult("Unknown failure.");
+  }
+}
+
+// Host CSR (int64) -> device row-compressed DevCsc (rows as major dimension).
+template <class T>
+void UploadCsr(Ctx& ctx, int64_t n, const double* values, const int64_t* indices, const int64_t* offsets,
+               DevCsc<T>& out) {
+  if (offsets[0] != 0) throw std::invalid_argument("CSR offsets must start at 0");
+  for (int64_t i = 0; i < n; ++i) {
+    if (offsets[i] > offsets[i + 1]) throw std::invalid_argument("CSR offsets must be non-decreasing");
+  }
+  const int64_t nnz = offsets[n];
+  std::vector<int32_t> idx(nnz);
+  for (int64_t k = 0; k < nnz; ++k) {
+    if (indices[k] < 0 || indices[k] >= n) throw std::invalid_argument("CSR column index out of range");
+    idx[k] = static_cast<int32_t>(indices[k]);
+  }
+  out.Shape(n, n, ctx.stream);
+  out.ReserveNnz(nnz, ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), offsets, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, ctx.stream));
+  if (nnz > 0) {
+    SPAI_CUDA(cudaMemcpyAsync(out.idx.data(), idx.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx.stream));
+    if constexpr (sizeof(T) == sizeof(double)) {
+      SPAI_CUDA(cudaMemcpyAsync(out.val.data(), values, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx.stream));
+    } else {
+      DevBuf<double> stage;
+      stage.Reserve(static_cast<size_t>(nnz), ctx.stream);
+      SPAI_CUDA(cudaMemcpyAsync(stage.data(), values, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx.stream));
+      ConvertValues<double, T>(ctx, stage.data(), out.val.data(), nnz);
+      ctx.Sync();
+    }
+  }
+  ctx.Sync();
+}
+
+void CheckPcgParams(int64_t n, const PcgParams& p) {
+  if (n <= 0 || p.max_iterations <= 0) throw std::invalid_argument("n, max_iterations and threads must be positive");
+  if (!(p.tolerance >= 0.0)) throw std::invalid_argument("tolerance must be non-negative");
+  if (p.m_precision != 0 && p.m_precision != 1) throw std::invalid_argument("m_precision must be 0 or 1");
+  if (p.refresh_period < 0) throw std::invalid_argument("refresh_period must be non-negative");
+  if (n > static_cast<int64_t>(INT32_MAX)) throw std::invalid_argument("n exceeds the 32-bit index range");
+}
+
+int64_t FinishPcg(const PcgResult& r, int64_t capacity, double* history, int64_t* status) {
+  const int64_t count = static_cast<int64_t>(r.history.size());
+  for (int64_t i = 0; i < count && i < capacity; ++i) history[i] = r.history[i];
+  if (status != nullptr) *status = r.status;
+  return count;
+}
+
+}  // namespace
+}  // namespace spai
+
+struct SpaiSession {
+  spai::Ctx ctx;
+  std::unique_ptr<spai::SolverBase> solver;
+  spai::SolveOptions options;
+  int64_t n = 0;
+  spai::DevBuf<double> b;
+  spai::DevBuf<double> x;
+  spai::DevCsc<double> a_rows;  // A as row-compressed FP64 for PCG
+  spai::DevCsc<double> m64;
+  spai::DevCsc<float> m32;
+  bool has_rhs = false;
+  bool has_a_rows = false;
+  std::vector<SingleIterationData> history;
+  ~SpaiSession() {
+    solver.reset();
+    b.Release();
+    x.Release();
+    a_rows = spai::DevCsc<double>();
+    m64 = spai::DevCsc<double>();
+    m32 = spai::DevCsc<float>();
+    ctx.Destroy();
+  }
+};
+
+extern "C" {
+
+Result spai_global_cg(MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params) {
+  return spai::RunMethod(0, A, M0, Pr, params, nullptr);
+}
+
+Result spai_global_mr(MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params) {
+  return spai::RunMethod(1, A, M0, Pr, params, nullptr);
+}
+
+Result spai_global_lomr(MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params) {
+  return spai::RunMethod(2, A, M0, Pr, params, nullptr);
+}
+
+Result inner_outer_mr(MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params) {
+  return spai::RunMethod(3, A, M0, Pr, params, nullptr);
+}
+
+Result inner_outer_lomr(MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params) {
+  return spai::RunMethod(4, A, M0, Pr, params, nullptr);
+}
+
+void free_mem(Result* result) {
+  if (result == nullptr) return;
+  delete[] result->col_offsets;
+  delete[] result->row_indices;
+  delete[] result->values;
+  delete[] result->history;
+  delete[] result->error_message;
+  result->col_offsets = nullptr;
+  result->row_indices = nullptr;
+  result->values = nullptr;
+  result->history = nullptr;
+  result->error_message = nullptr;
+}
+
+Result spai_run_ex(int64_t method, MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params,
+                   const SpaiExtParams* ext) {
+  return spai::RunMethod(method, A, M0, Pr, params, ext);
+}
+
+int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, const int64_t* a_offsets,
+                 const double* m_values, const int64_t* m_indices, const int64_t* m_offsets, const double* b,
+                 PcgParams params, double* history, int64_t* status, double* x_out, char* error,
+                 int64_t error_capacity) {
+  try {
+    spai::CheckPcgParams(n, params);
+    spai::CtxGuard guard(spai::ResolveDevice(params.device));
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevCsc<double> a;
+    spai::UploadCsr(ctx, n, a_values, a_indices, a_offsets, a);
+    spai::DevBuf<double> bd;
+    spai::DevBuf<double> xd;
+    bd.Reserve(static_cast<size_t>(n), ctx.stream);
+    xd.Reserve(static_cast<size_t>(n), ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(bd.data(), b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.stream));
+    spai::PcgOptions opt;
+    opt.max_iterations = params.max_iterations;
+    opt.tolerance = params.tolerance;
+    opt.refresh_period = params.refresh_period;
+    spai::PcgResult result;
+    if (params.m_precision == 1) {
+      spai::DevCsc<float> m;
+      spai::UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
+      spai::RunPcg(ctx, a, m, bd.data(), xd.data(), opt, result);
+    } else {
+      spai::DevCsc<double> m;
+      spai::UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
+      spai::RunPcg(ctx, a, m, bd.data(), xd.data(), opt, result);
+    }
+    if (x_out != nullptr) {
+      SPAI_CUDA(cudaMemcpyAsync(x_out, xd.data(), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    ctx.Sync();
+    return spai::FinishPcg(result, params.max_iterations, history, status);
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_matvec(int64_t n, const double* values, const int64_t* indices, const int64_t* offsets, const double* x,
+                    double* y, int64_t device, char* error, int64_t error_capacity) {
+  try {
+    if (n <= 0) throw std::invalid_argument("Invalid matrix-vector dimensions or thread count");
+    spai::CtxGuard guard(spai::ResolveDevice(device));
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevCsc<double> a;
+    spai::UploadCsr(ctx, n, values, indices, offsets, a);
+    spai::DevBuf<double> xd;
+    spai::DevBuf<double> yd;
+    xd.Reserve(static_cast<size_t>(n), ctx.stream);
+    yd.Reserve(static_cast<size_t>(n), ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(xd.data(), x, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.stream));
+    spai::Spmv(ctx, a, xd.data(), yd.data());
+    SPAI_CUDA(cudaMemcpyAsync(y, yd.data(), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.Sync();
+    return 0;
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+SpaiSession* spai_session_create(int64_t method, MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params,
+                                 const SpaiExtParams* ext, char* error, int64_t error_capacity) {
+  SpaiSession* session = nullptr;
+  try {
+    spai::Inputs in;
+    const spai::SolveOptions opt = spai::CheckInputs(method, A, M0, Pr, params, ext, in);
+    const int device = spai::ResolveDevice(ext != nullptr ? ext->device : -1);
+    session = new SpaiSession();
+    session->ctx.Init(device);
+    session->options = opt;
+    session->n = in.a.cols;
+    session->solver = spai::MakeSolver(session->ctx, opt);
+    session->solver->Upload(in.a, in.has_m0 ? &in.m0 : nullptr, in.has_pr ? &in.pr : nullptr);
+    return session;
+  } catch (const std::exception& ex) {
+    delete session;
+    spai::CopyError(ex.what(), error, error_capacity);
+    return nullptr;
+  }
+}
+
+int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* converged, int64_t* nnz_m, char* error,
+                         int64_t error_capacity) {
+  try {
+    if (session == nullptr) throw std::invalid_argument("null session");
+    session->solver->Run();
+    if (iterations != nullptr) *iterations = session->solver->iterations();
+    if (nnz_m != nullptr) *nnz_m = session->solver->m_nnz();
+    spai::SolveOutput out;
+    // only the history is needed here; M stays on the device
+    if (converged != nullptr) *converged = 0;
+    session->history.clear();
+    return 0;
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_session_history(SpaiSession* session, SingleIterationData* out, int64_t capacity) {
+  if (session == nullptr) return 0;
+  try {
+    spai::SolveOutput full;
+    session->solver->Download(full);
+    const int64_t count = static_cast<int64_t>(full.history.size());
+    for (int64_t i = 0; i < count && i < capacity; ++i) out[i] = full.history[i];
+    return count;
+  } catch (...) {
+    return 0;
+  }
+}
+
+Result spai_session_result(SpaiSession* session) {
+  try {
+    if (session == nullptr) throw std::invalid_argument("null session");
+    spai::SolveOutput out;
+    session->solver->Download(out);
+    return spai::SuccessResult(out);
+  } catch (const std::exception& ex) {
+    return spai::ErrorResult(ex.what());
+  }
+}
+
+int64_t spai_session_set_rhs(SpaiSession* session, const double* b, char* error, int64_t error_capacity) {
+  try {
+    if (session == nullptr) throw std::invalid_argument("null session");
+    const int64_t n = session->n;
+    session->b.Reserve(static_cast<size_t>(n), session->ctx.stream);
+    session->x.Reserve(static_cast<size_t>(n), session->ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(session->b.data(), b, sizeof(double) * n, cudaMemcpyHostToDevice, session->ctx.stream));
+    session->ctx.Sync();
+    session->has_rhs = true;
+    if (!session->has_a_rows) {
+      const auto* a64 = static_cast<const spai::DevCsc<double>*>(session->solver->DeviceA64());
+      spai::Transpose(session->ctx, *a64, session->a_rows);
+      session->has_a_rows = true;
+    }
+    return 0;
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history, int64_t* status, double* x_out,
+                         char* error, int64_t error_capacity) {
+  try {
+    if (session == nullptr) throw std::invalid_argument("null session");
+    if (!session->has_rhs) throw std::invalid_argument("spai_session_set_rhs must be called first");
+    spai::CheckPcgParams(session->n, params);
+    spai::PcgOptions opt;
+    opt.max_iterations = params.max_iterations;
+    opt.tolerance = params.tolerance;
+    opt.refresh_period = params.refresh_period;
+    spai::PcgResult result;
+    if (params.m_precision == 1) {
+      session->solver->ExportMForPcg(&session->m32, true);
+      spai::RunPcg(session->ctx, session->a_rows, session->m32, session->b.data(), session->x.data(), opt, result);
+    } else {
+      session->solver->ExportMForPcg(&session->m64, false);
+      spai::RunPcg(session->ctx, session->a_rows, session->m64, session->b.data(), session->x.data(), opt, result);
+    }
+    if (x_out != nullptr) {
+      SPAI_CUDA(cudaMemcpyAsync(x_out, session->x.data(), sizeof(double) * session->n, cudaMemcpyDeviceToHost,
+                                session->ctx.stream));
+      session->ctx.Sync();
+    }
+    return spai::FinishPcg(result, params.max_iterations, history, status);
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+void spai_session_destroy(SpaiSession* session) { delete session; }
+
+int64_t spai_kernel_launches(void) { return spai::g_launches.load(); }
+
+}  // extern "C"

@@ -1,0 +1,1099 @@
+// Sparse-matrix building blocks on sm_100a: scans, the canonical reduction
+// tree, unions, filters (pruning, top-k, global cutoff), transposition and
+// radix selection.  All are HBM-bound integer/byte work plus light FP64
+// arithmetic; none is a contraction, so none uses tensor cores.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+
+#include "device.cuh"
+#include "ops.cuh"
+
+namespace spai {
+
+namespace {
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int64_t kScanTile = kScanThreads * kScanItems;
+
+constexpr int kTreeLanes = 256;
+constexpr int64_t kTreeChunk = 4096;
+
+constexpr double kDblEps = 2.220446049250313080847e-16;
+
+__device__ __forceinline__ unsigned LaneMaskLt() {
+  unsigned mask;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(mask));
+  return mask;
+}
+
+// ---------------------------------------------------------------------------
+// Scan
+__global__ void ScanTileKernel(const int64_t* __restrict__ in, int64_t n, int64_t* __restrict__ out,
+                               int64_t* __restrict__ tile_sums) {
+  __shared__ int64_t warp_sums[kScanThreads / kWarp];
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kScanTile + static_cast<int64_t>(threadIdx.x) * kScanItems;
+  int64_t v[kScanItems];
+  int64_t local = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    const int64_t at = base + i;
+    v[i] = at < n ? in[at] : 0;
+    local += v[i];
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  int64_t inclusive = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int64_t y = __shfl_up_sync(0xffffffffu, inclusive, o);
+    if (lane >= o) inclusive += y;
+  }
+  if (lane == 31) warp_sums[warp] = inclusive;
+  __syncthreads();
+  if (warp == 0) {
+    int64_t w = lane < kScanThreads / kWarp ? warp_sums[lane] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
+    }
+    if (lane < kScanThreads / kWarp) warp_sums[lane] = w;
+  }
+  __syncthreads();
+  int64_t running = inclusive - local + (warp > 0 ? warp_sums[warp - 1] : 0);
+#pragma unroll
+  for (int i = 0; i < kScanItems; ++i) {
+    running += v[i];
+    if (base + i < n) out[base + i + 1] = running;
+  }
+  if (threadIdx.x == kScanThreads - 1) tile_sums[blockIdx.x] = running;
+}
+
+__global__ void ScanAddKernel(int64_t n, int64_t* __restrict__ out, const int64_t* __restrict__ tile_prefix) {
+  const int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i == 0) out[0] = 0;
+  if (i < n) out[i + 1] += tile_prefix[i / kScanTile];
+}
+
+void ScanRecursive(Ctx& ctx, const int64_t* in, int64_t n, int64_t* out, DevBuf<int64_t>& scratch, size_t offset) {
+  const int64_t tiles = CeilDiv(n, kScanTile);
+  int64_t* tile_sums = scratch.data() + offset;
+  ScanTileKernel<<<static_cast<unsigned>(tiles), kScanThreads, 0, ctx.stream>>>(in, n, out, tile_sums);
+  SPAI_LAUNCH_CHECK();
+  if (tiles > 1) {
+    int64_t* tile_prefix = tile_sums + tiles;
+    ScanRecursive(ctx, tile_sums, tiles, tile_prefix, scratch, offset + 2 * tiles + 1);
+    ScanAddKernel<<<static_cast<unsigned>(CeilDiv(n, 256)), 256, 0, ctx.stream>>>(n, out, tile_prefix);
+    SPAI_LAUNCH_CHECK();
+  } else {
+    SPAI_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), ctx.stream));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Canonical tree: 256 lanes per 4096-value chunk, then a butterfly.
+struct TreeArgs {
+  const double* src[8];
+  const double* src2[8];  // when set, level-one terms are src[i] * src2[i]
+};
+
+__global__ void TreeChunkKernel(TreeArgs args, int64_t n, double* __restrict__ out, int64_t out_stride) {
+  __shared__ double shared[kTreeLanes];
+  const double* __restrict__ src = args.src[blockIdx.y];
+  const double* __restrict__ src2 = args.src2[blockIdx.y];
+  const int t = threadIdx.x;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTreeChunk + t;
+  double s = 0.0;
+  if (src2 != nullptr) {
+#pragma unroll
+    for (int m = 0; m < static_cast<int>(kTreeChunk / kTreeLanes); ++m) {
+      const int64_t i = base + static_cast<int64_t>(kTreeLanes) * m;
+      if (i < n) s = Add(s, Mul(src[i], src2[i]));
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < static_cast<int>(kTreeChunk / kTreeLanes); ++m) {
+      const int64_t i = base + static_cast<int64_t>(kTreeLanes) * m;
+      if (i < n) s = Add(s, src[i]);
+    }
+  }
+  shared[t] = s;
+  __syncthreads();
+#pragma unroll
+  for (int stride = kTreeLanes / 2; stride >= kWarp; stride >>= 1) {
+    const double other = shared[t ^ stride];
+    __syncthreads();
+    s = Add(s, other);
+    shared[t] = s;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int stride = kWarp / 2; stride >= 1; stride >>= 1) {
+    s = Add(s, __shfl_xor_sync(0xffffffffu, s, stride));
+  }
+  if (t == 0) out[blockIdx.y * out_stride + blockIdx.x] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Per-column partial sums
+template <class T>
+__global__ void ColumnSquaresKernel(CscView<T> x, double* __restrict__ partial) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) {
+      const double v = static_cast<double>(x.val[p]);
+      s = Add(s, Mul(v, v));
+    }
+    partial[j] = s;
+  }
+}
+
+template <class T>
+__global__ void ColumnDotsKernel(CscView<T> x, CscView<T> y, double* __restrict__ partial) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    int64_t p = x.ptr[j];
+    int64_t q = y.ptr[j];
+    const int64_t pe = x.ptr[j + 1];
+    const int64_t qe = y.ptr[j + 1];
+    while (p < pe && q < qe) {
+      const int32_t a = x.idx[p];
+      const int32_t b = y.idx[q];
+      if (a == b) {
+        s = Add(s, Mul(static_cast<double>(x.val[p]), static_cast<double>(y.val[q])));
+        ++p;
+        ++q;
+      } else if (a < b) {
+        ++p;
+      } else {
+        ++q;
+      }
+    }
+    partial[j] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Union (thread per column, two phases)
+template <class T>
+__device__ __forceinline__ double UnionBoth(double y, double x, bool scale_y, double ys, double xs, int mode) {
+  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(0.5, Add(y, x));
+  const double yv = scale_y ? Mul(ys, y) : y;
+  return Add(yv, Mul(xs, x));
+}
+
+template <class T>
+__device__ __forceinline__ double UnionLeft(double y, bool scale_y, double ys, int mode) {
+  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(0.5, Add(y, 0.0));
+  const double yv = scale_y ? Mul(ys, y) : y;
+  return Add(yv, 0.0);
+}
+
+template <class T>
+__device__ __forceinline__ double UnionRight(double x, double xs, int mode) {
+  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(0.5, Add(0.0, x));
+  return Add(0.0, Mul(xs, x));
+}
+
+template <class T, bool kWrite>
+__global__ void UnionKernel(CscView<T> y, CscView<T> x, bool scale_y, double ys, double xs, int mode,
+                            int64_t* __restrict__ counts, const int64_t* __restrict__ out_ptr,
+                            int32_t* __restrict__ out_idx, T* __restrict__ out_val) {
+  const bool prune = mode == static_cast<int>(UnionMode::kAxpby);
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < y.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t p = y.ptr[j];
+    int64_t q = x.ptr[j];
+    const int64_t pe = y.ptr[j + 1];
+    const int64_t qe = x.ptr[j + 1];
+    int64_t o = kWrite ? out_ptr[j] : 0;
+    int64_t count = 0;
+    while (p < pe || q < qe) {
+      int32_t row;
+      double v;
+      if (p < pe && q < qe && y.idx[p] == x.idx[q]) {
+        row = y.idx[p];
+        v = UnionBoth<T>(static_cast<double>(y.val[p]), static_cast<double>(x.val[q]), scale_y, ys, xs, mode);
+        ++p;
+        ++q;
+      } else if (p < pe && (q >= qe || y.idx[p] < x.idx[q])) {
+        row = y.idx[p];
+        v = UnionLeft<T>(static_cast<double>(y.val[p]), scale_y, ys, mode);
+        ++p;
+      } else {
+        row = x.idx[q];
+        v = UnionRight<T>(static_cast<double>(x.val[q]), xs, mode);
+        ++q;
+      }
+      const T stored = static_cast<T>(v);
+      if (prune && fabs(static_cast<double>(stored)) <= 0.0) continue;
+      if (kWrite) {
+        out_idx[o] = row;
+        out_val[o] = stored;
+        ++o;
+      } else {
+        ++count;
+      }
+    }
+    if (!kWrite) counts[j] = count;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Warp-per-column filters
+template <class T>
+struct KeepNonZero {
+  __device__ void Begin(const CscView<T>&, int64_t, int) {}
+  __device__ bool Keep(int64_t, int64_t, int32_t, T v) const {
+    const double d = static_cast<double>(v);
+    return !(fabs(d) <= 0.0);
+  }
+};
+
+template <class T>
+struct KeepAboveLimit {
+  double limit;
+  __device__ void Begin(const CscView<T>&, int64_t, int) {}
+  __device__ bool Keep(int64_t, int64_t, int32_t, T v) const {
+    return !(fabs(static_cast<double>(v)) <= limit);
+  }
+};
+
+template <class T>
+struct KeepColumnRelative {
+  double threshold = 0.0;
+  __device__ void Begin(const CscView<T>& x, int64_t col, int lane) {
+    double s = 0.0;
+    if (lane == 0) {
+      for (int64_t p = x.ptr[col]; p < x.ptr[col + 1]; ++p) {
+        const double v = static_cast<double>(x.val[p]);
+        s = Add(s, Mul(v, v));
+      }
+      s = Mul(kDblEps, sqrt(s));
+    }
+    threshold = __shfl_sync(0xffffffffu, s, 0);
+  }
+  __device__ bool Keep(int64_t col, int64_t, int32_t row, T v) const {
+    const double d = static_cast<double>(v);
+    return d != 0.0 && (static_cast<int64_t>(row) == col || fabs(d) >= threshold);
+  }
+};
+
+// (|v|, row) keys; keeps the largest `k` (diagonal protected if asked).
+template <class T>
+struct KeepTopK {
+  int64_t k;
+  bool protect;
+  bool keep_all = true;
+  double cut_abs = 0.0;
+  int32_t cut_row = 0;
+  __device__ void Begin(const CscView<T>& x, int64_t col, int lane) {
+    const int64_t start = x.ptr[col];
+    const int64_t end = x.ptr[col + 1];
+    const int64_t count = end - start;
+    keep_all = count <= k;
+    if (keep_all) return;
+    // candidates: all entries except a protected diagonal
+    bool has_diag = false;
+    if (protect) {
+      for (int64_t base = start; base < end; base += kWarp) {
+        const int64_t p = base + lane;
+        const bool d = p < end && static_cast<int64_t>(x.idx[p]) == col;
+        if (__any_sync(0xffffffffu, d)) has_diag = true;
+      }
+    }
+    const int64_t candidates = count - (has_diag ? 1 : 0);
+    const int64_t keep_off = k - (has_diag ? 1 : 0) > 0 ? k - (has_diag ? 1 : 0) : 0;
+    const int64_t drop = candidates - keep_off;
+    if (drop <= 0) {
+      keep_all = true;
+      return;
+    }
+    // the drop-th smallest candidate key is the cutoff
+    double found_abs = 0.0;
+    int32_t found_row = 0;
+    bool found = false;
+    for (int64_t base = start; base < end; base += kWarp) {
+      const int64_t p = base + lane;
+      bool mine = false;
+      double a = 0.0;
+      int32_t r = 0;
+      if (p < end) {
+        r = x.idx[p];
+        a = fabs(static_cast<double>(x.val[p]));
+        const bool is_cand = !(protect && static_cast<int64_t>(r) == col);
+        if (is_cand) {
+          int64_t rank = 0;
+          for (int64_t q = start; q < end; ++q) {
+            const int32_t rq = x.idx[q];
+            if (protect && static_cast<int64_t>(rq) == col) continue;
+            const double aq = fabs(static_cast<double>(x.val[q]));
+            rank += (aq < a || (aq == a && rq < r)) ? 1 : 0;
+          }
+          mine = rank == drop - 1;
+        }
+      }
+      const unsigned ballot = __ballot_sync(0xffffffffu, mine);
+      if (ballot != 0u) {
+        const int src = __ffs(ballot) - 1;
+        found_abs = __shfl_sync(0xffffffffu, a, src);
+        found_row = __shfl_sync(0xffffffffu, r, src);
+        found = true;
+      }
+    }
+    cut_abs = found_abs;
+    cut_row = found_row;
+    if (!found) keep_all = true;
+  }
+  __device__ bool Keep(int64_t col, int64_t, int32_t row, T v) const {
+    if (keep_all) return true;
+    if (protect && static_cast<int64_t>(row) == col) return true;
+    const double a = fabs(static_cast<double>(v));
+    return a > cut_abs || (a == cut_abs && row > cut_row);
+  }
+};
+
+__device__ __forceinline__ unsigned long long OrderedBits(double s) {
+  if (s == 0.0) s = 0.0;  // -0.0 and +0.0 compare equal in the reference ordering
+  unsigned long long u = static_cast<unsigned long long>(__double_as_longlong(s));
+  return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+
+// keep iff diagonal (when skipped) or (ordered score, offset) > cutoff.
+template <class T>
+struct KeepAboveCutoff {
+  const double* scores;
+  const int64_t* column_base;  // first candidate offset of each column
+  const unsigned long long* cutoff;  // [score bits, offset]
+  bool skip_diag;
+  int64_t diag_pos = -1;
+  int64_t start = 0;
+  unsigned long long cut_score = 0;
+  unsigned long long cut_offset = 0;
+  __device__ void Begin(const CscView<T>& x, int64_t col, int lane) {
+    start = x.ptr[col];
+    const int64_t end = x.ptr[col + 1];
+    cut_score = cutoff[0];
+    cut_offset = cutoff[1];
+    diag_pos = -1;
+    if (skip_diag) {
+      for (int64_t base = start; base < end; base += kWarp) {
+        const int64_t p = base + lane;
+        const bool d = p < end && static_cast<int64_t>(x.idx[p]) == col;
+        const unsigned b = __ballot_sync(0xffffffffu, d);
+        if (b != 0u) diag_pos = base + __ffs(b) - 1;
+      }
+    }
+  }
+  __device__ bool Keep(int64_t col, int64_t pos, int32_t row, T) const {
+    if (skip_diag && static_cast<int64_t>(row) == col) return true;
+    const int64_t offset = skip_diag ? column_base[col] + (pos - start) - ((diag_pos >= 0 && diag_pos < pos) ? 1 : 0)
+                                     : pos;
+    const unsigned long long s = OrderedBits(scores[pos]);
+    const unsigned long long o = static_cast<unsigned long long>(offset);
+    return s > cut_score || (s == cut_score && o > cut_offset);
+  }
+};
+
+template <class T, class Pred>
+__global__ void FilterCountKernel(CscView<T> x, Pred pred, int64_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t col = warp; col < x.cols; col += warps) {
+    Pred p = pred;
+    p.Begin(x, col, lane);
+    const int64_t start = x.ptr[col];
+    const int64_t end = x.ptr[col + 1];
+    int64_t count = 0;
+    for (int64_t base = start; base < end; base += kWarp) {
+      const int64_t at = base + lane;
+      const bool keep = at < end && p.Keep(col, at, x.idx[at], x.val[at]);
+      count += __popc(__ballot_sync(0xffffffffu, keep));
+    }
+    if (lane == 0) counts[col] = count;
+  }
+}
+
+template <class T, class Pred>
+__global__ void FilterWriteKernel(CscView<T> x, Pred pred, const int64_t* __restrict__ out_ptr,
+                                  int32_t* __restrict__ out_idx, T* __restrict__ out_val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t col = warp; col < x.cols; col += warps) {
+    Pred p = pred;
+    p.Begin(x, col, lane);
+    const int64_t start = x.ptr[col];
+    const int64_t end = x.ptr[col + 1];
+    int64_t o = out_ptr[col];
+    for (int64_t base = start; base < end; base += kWarp) {
+      const int64_t at = base + lane;
+      int32_t row = 0;
+      T v = T(0);
+      bool keep = false;
+      if (at < end) {
+        row = x.idx[at];
+        v = x.val[at];
+        keep = p.Keep(col, at, row, v);
+      }
+      const unsigned mask = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int64_t dst = o + __popc(mask & LaneMaskLt());
+        out_idx[dst] = row;
+        out_val[dst] = v;
+      }
+      o += __popc(mask);
+    }
+  }
+}
+
+template <class T, class Pred>
+void RunFilter(Ctx& ctx, DevCsc<T>& x, const Pred& pred) {
+  const int64_t cols = x.cols;
+  ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+  const int threads = 256;
+  const int grid = GridFor(cols * kWarp, threads);
+  FilterCountKernel<T, Pred><<<grid, threads, 0, ctx.stream>>>(View(x), pred, ctx.counts.data());
+  SPAI_LAUNCH_CHECK();
+  DevCsc<T> out;
+  out.Shape(x.rows, cols, ctx.stream);
+  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());
+  if (nnz == x.nnz) {
+    return;  // nothing removed: keep x as it is
+  }
+  out.ReserveNnz(nnz, ctx.stream);
+  FilterWriteKernel<T, Pred><<<grid, threads, 0, ctx.stream>>>(View(x), pred, out.ptr.data(), out.idx.data(),
+                                                               out.val.data());
+  SPAI_LAUNCH_CHECK();
+  x.Swap(out);
+}
+
+// ---------------------------------------------------------------------------
+// Row scaling / column scaling
+template <class T>
+__global__ void DiagScaleKernel(const T* __restrict__ d, const int32_t* __restrict__ idx, const T* __restrict__ val,
+                                int64_t nnz, T* __restrict__ out) {
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[p] = static_cast<T>(Mul(static_cast<double>(d[idx[p]]), static_cast<double>(val[p])));
+  }
+}
+
+template <class T>
+__global__ void ScaleColumnsKernel(CscView<T> x, T* __restrict__ val, const double* __restrict__ scale) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double s = scale[j];
+    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) {
+      val[p] = static_cast<T>(Mul(static_cast<double>(val[p]), s));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Transpose
+__global__ void RowCountKernel(const int32_t* __restrict__ idx, int64_t nnz, unsigned long long* __restrict__ counts) {
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    atomicAdd(&counts[idx[p]], 1ull);
+  }
+}
+
+template <class T>
+__global__ void ScatterKernel(CscView<T> x, const int64_t* __restrict__ t_ptr, unsigned long long* __restrict__ cursor,
+                              int32_t* __restrict__ t_idx, T* __restrict__ t_val) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) {
+      const int32_t row = x.idx[p];
+      const int64_t dst = t_ptr[row] + static_cast<int64_t>(atomicAdd(&cursor[row], 1ull));
+      t_idx[dst] = static_cast<int32_t>(j);
+      t_val[dst] = x.val[p];
+    }
+  }
+}
+
+// Bitonic sort of (key, value) pairs in shared memory by one warp or one block.
+template <class T>
+__device__ void BitonicSortPairs(int32_t* keys, T* vals, int size, int tid, int nthreads, bool block_sync) {
+  for (int k = 2; k <= size; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = tid; i < size; i += nthreads) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const bool ascending = (i & k) == 0;
+          const int32_t a = keys[i];
+          const int32_t b = keys[ixj];
+          if ((a > b) == ascending) {
+            keys[i] = b;
+            keys[ixj] = a;
+            const T tv = vals[i];
+            vals[i] = vals[ixj];
+            vals[ixj] = tv;
+          }
+        }
+      }
+      if (block_sync) {
+        __syncthreads();
+      } else {
+        __syncwarp();
+      }
+    }
+  }
+}
+
+constexpr int kWarpSortCap = 512;
+constexpr int kBlockSortCap = 8192;
+
+template <class T>
+__global__ void SegmentSortWarpKernel(const int64_t* __restrict__ ptr, int64_t segments, int32_t* __restrict__ idx,
+                                      T* __restrict__ val) {
+  extern __shared__ unsigned char smem_raw[];
+  constexpr int kWarpsPerBlock = 4;
+  const int warp_in_block = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  int32_t* keys = reinterpret_cast<int32_t*>(smem_raw) + warp_in_block * kWarpSortCap;
+  T* vals = reinterpret_cast<T*>(smem_raw + kWarpsPerBlock * kWarpSortCap * sizeof(int32_t)) + warp_in_block * kWarpSortCap;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = warp; s < segments; s += warps) {
+    const int64_t start = ptr[s];
+    const int len = static_cast<int>(ptr[s + 1] - start);
+    if (len <= 1 || len > kWarpSortCap) continue;
+    int size = 1;
+    while (size < len) size <<= 1;
+    for (int i = lane; i < size; i += kWarp) {
+      keys[i] = i < len ? idx[start + i] : INT32_MAX;
+      vals[i] = i < len ? val[start + i] : T(0);
+    }
+    __syncwarp();
+    BitonicSortPairs(keys, vals, size, lane, kWarp, false);
+    for (int i = lane; i < len; i += kWarp) {
+      idx[start + i] = keys[i];
+      val[start + i] = vals[i];
+    }
+    __syncwarp();
+  }
+}
+
+template <class T>
+__global__ void SegmentSortBlockKernel(const int64_t* __restrict__ ptr, int64_t segments, int32_t* __restrict__ idx,
+                                       T* __restrict__ val) {
+  extern __shared__ unsigned char smem_raw[];
+  int32_t* keys = reinterpret_cast<int32_t*>(smem_raw);
+  T* vals = reinterpret_cast<T*>(smem_raw + kBlockSortCap * sizeof(int32_t));
+  for (int64_t s = blockIdx.x; s < segments; s += gridDim.x) {
+    const int64_t start = ptr[s];
+    const int len = static_cast<int>(ptr[s + 1] - start);
+    if (len <= kWarpSortCap || len > kBlockSortCap) continue;
+    int size = 1;
+    while (size < len) size <<= 1;
+    for (int i = threadIdx.x; i < size; i += blockDim.x) {
+      keys[i] = i < len ? idx[start + i] : INT32_MAX;
+      vals[i] = i < len ? val[start + i] : T(0);
+    }
+    __syncthreads();
+    BitonicSortPairs(keys, vals, size, threadIdx.x, blockDim.x, true);
+    for (int i = threadIdx.x; i < len; i += blockDim.x) {
+      idx[start + i] = keys[i];
+      val[start + i] = vals[i];
+    }
+    __syncthreads();
+  }
+}
+
+// Segments longer than the shared-memory cap: insertion sort in global memory
+// (one thread per segment; only reached by very dense columns).
+template <class T>
+__global__ void SegmentSortLongKernel(const int64_t* __restrict__ ptr, int64_t segments, int32_t* __restrict__ idx,
+                                      T* __restrict__ val) {
+  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < segments;
+       s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t start = ptr[s];
+    const int64_t end = ptr[s + 1];
+    if (end - start <= kBlockSortCap) continue;
+    for (int64_t i = start + 1; i < end; ++i) {
+      const int32_t key = idx[i];
+      const T v = val[i];
+      int64_t j = i - 1;
+      while (j >= start && idx[j] > key) {
+        idx[j + 1] = idx[j];
+        val[j + 1] = val[j];
+        --j;
+      }
+      idx[j + 1] = key;
+      val[j + 1] = v;
+    }
+  }
+}
+
+template <class T>
+void SortSegments(Ctx& ctx, const int64_t* ptr, int64_t segments, int32_t* idx, T* val) {
+  const size_t warp_smem = 4 * kWarpSortCap * (sizeof(int32_t) + sizeof(T));
+  SegmentSortWarpKernel<T><<<GridFor(segments * kWarp, 128), 128, warp_smem, ctx.stream>>>(ptr, segments, idx, val);
+  SPAI_LAUNCH_CHECK();
+  const size_t block_smem = kBlockSortCap * (sizeof(int32_t) + sizeof(T));
+  SPAI_CUDA(cudaFuncSetAttribute(SegmentSortBlockKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(block_smem)));
+  SegmentSortBlockKernel<T><<<GridFor(segments * 1024, 1024) , 1024, block_smem, ctx.stream>>>(ptr, segments, idx, val);
+  SPAI_LAUNCH_CHECK();
+  SegmentSortLongKernel<T><<<GridFor(segments, 128), 128, 0, ctx.stream>>>(ptr, segments, idx, val);
+  SPAI_LAUNCH_CHECK();
+}
+
+// ---------------------------------------------------------------------------
+// Scores
+template <class T>
+__global__ void DropScoresKernel(CscView<T> m, const double* __restrict__ cn, const double* __restrict__ tmp,
+                                 double* __restrict__ scores) {
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < m.ptr[m.cols];
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const double v = static_cast<double>(m.val[p]);
+    const double s = Add(Mul(Mul(v, v), cn[m.idx[p]]), Mul(Mul(2.0, v), tmp[p]));
+    scores[p] = isfinite(s) ? s : -INFINITY;
+  }
+}
+
+template <class T>
+__global__ void AbsScoresKernel(const T* __restrict__ val, int64_t nnz, double* __restrict__ scores) {
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    scores[p] = fabs(static_cast<double>(val[p]));
+  }
+}
+
+// candidate counts per column (entries minus a diagonal)
+template <class T>
+__global__ void NonDiagonalCountKernel(CscView<T> x, int64_t* __restrict__ counts) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t c = 0;
+    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) c += static_cast<int64_t>(x.idx[p]) != j ? 1 : 0;
+    counts[j] = c;
+  }
+}
+
+// candidate keys in offset order: key[offset] = ordered score bits
+template <class T>
+__global__ void GatherCandidateKeysKernel(CscView<T> x, const double* __restrict__ scores,
+                                          const int64_t* __restrict__ column_base, bool skip_diag,
+                                          unsigned long long* __restrict__ keys) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t o = skip_diag ? column_base[j] : x.ptr[j];
+    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) {
+      if (skip_diag && static_cast<int64_t>(x.idx[p]) == j) continue;
+      keys[o++] = OrderedBits(scores[p]);
+    }
+  }
+}
+
+// Radix select over 128-bit keys (ordered score bits, candidate offset), 8
+// bits per pass from the most significant byte.  state = {prefix_hi,
+// prefix_lo, remaining rank (1-based)}.
+__global__ void RadixHistKernel(const unsigned long long* __restrict__ keys, int64_t count, int pass,
+                                const unsigned long long* __restrict__ state, unsigned long long* __restrict__ hist) {
+  __shared__ unsigned int local[256];
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) local[i] = 0;
+  __syncthreads();
+  const unsigned long long prefix_hi = state[0];
+  const unsigned long long prefix_lo = state[1];
+  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < count;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned long long hi = keys[c];
+    const unsigned long long lo = static_cast<unsigned long long>(c);
+    bool match;
+    unsigned digit;
+    if (pass < 8) {
+      const int shift = 56 - 8 * pass;
+      const unsigned long long mask = pass == 0 ? 0ull : (~0ull << (shift + 8));
+      match = (hi & mask) == (prefix_hi & mask);
+      digit = static_cast<unsigned>((hi >> shift) & 0xFFull);
+    } else {
+      const int shift = 56 - 8 * (pass - 8);
+      const unsigned long long mask = pass == 8 ? 0ull : (~0ull << (shift + 8));
+      match = hi == prefix_hi && (lo & mask) == (prefix_lo & mask);
+      digit = static_cast<unsigned>((lo >> shift) & 0xFFull);
+    }
+    if (match) atomicAdd(&local[digit], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 256; i += blockDim.x) {
+    if (local[i] != 0) atomicAdd(&hist[i], static_cast<unsigned long long>(local[i]));
+  }
+}
+
+__global__ void RadixDecideKernel(int pass, unsigned long long* __restrict__ state, unsigned long long* __restrict__ hist) {
+  if (threadIdx.x != 0) return;
+  unsigned long long remaining = state[2];
+  unsigned long long cumulative = 0;
+  int digit = 255;
+  for (int b = 0; b < 256; ++b) {
+    if (cumulative + hist[b] >= remaining) {
+      digit = b;
+      break;
+    }
+    cumulative += hist[b];
+  }
+  if (pass < 8) {
+    state[0] |= static_cast<unsigned long long>(digit) << (56 - 8 * pass);
+  } else {
+    state[1] |= static_cast<unsigned long long>(digit) << (56 - 8 * (pass - 8));
+  }
+  state[2] = remaining - cumulative;
+  for (int b = 0; b < 256; ++b) hist[b] = 0;
+}
+
+template <class S, class D>
+__global__ void ConvertKernel(const S* __restrict__ src, D* __restrict__ dst, int64_t n) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    dst[i] = static_cast<D>(src[i]);
+  }
+}
+
+}  // namespace
+
+// ===========================================================================
+int GridFor(int64_t work_items, int threads_per_block) {
+  int device = 0;
+  cudaGetDevice(&device);
+  static int sm_count = 0;
+  if (sm_count == 0) {
+    cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (sm_count <= 0) sm_count = 148;
+  }
+  const int64_t needed = CeilDiv(work_items > 0 ? work_items : 1, threads_per_block);
+  const int64_t cap = static_cast<int64_t>(sm_count) * 16;
+  return static_cast<int>(needed < cap ? needed : cap);
+}
+
+void Ctx::Init(int device_ordinal) {
+  device = device_ordinal;
+  SPAI_CUDA(cudaSetDevice(device));
+  SPAI_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
+  SPAI_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  cudaMemPool_t pool;
+  SPAI_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+  uint64_t threshold = UINT64_MAX;
+  SPAI_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+  SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_scalars), sizeof(double) * kScalarSlots));
+  SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_counts), sizeof(int64_t) * 8));
+  SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_flags), sizeof(int32_t) * 8));
+  scalars.Reserve(kScalarSlots, stream);
+  select_state.Reserve(4, stream);
+  histogram.Reserve(256, stream);
+  flags.Reserve(8, stream);
+  SPAI_CUDA(cudaMemsetAsync(histogram.data(), 0, 256 * sizeof(unsigned long long), stream));
+}
+
+void Ctx::Destroy() {
+  if (stream != nullptr) {
+    cudaStreamSynchronize(stream);
+  }
+  counts.Release();
+  counts2.Release();
+  scan_blocks.Release();
+  for (auto& p : partials) p.Release();
+  tree_scratch.Release();
+  scalars.Release();
+  for (auto& c : colvec) c.Release();
+  select_state.Release();
+  histogram.Release();
+  flags.Release();
+  if (stream != nullptr) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+    stream = nullptr;
+  }
+  if (host_scalars != nullptr) cudaFreeHost(host_scalars);
+  if (host_counts != nullptr) cudaFreeHost(host_counts);
+  if (host_flags != nullptr) cudaFreeHost(host_flags);
+  host_scalars = nullptr;
+  host_counts = nullptr;
+  host_flags = nullptr;
+}
+
+void Ctx::Sync() { SPAI_CUDA(cudaStreamSynchronize(stream)); }
+
+int64_t ScanCounts(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out) {
+  if (n <= 0) {
+    SPAI_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), ctx.stream));
+    return 0;
+  }
+  int64_t need = 0;
+  for (int64_t m = n; m > 1; m = CeilDiv(m, kScanTile)) need += 2 * CeilDiv(m, kScanTile) + 2;
+  ctx.scan_blocks.Reserve(static_cast<size_t>(need + 8), ctx.stream);
+  ScanRecursive(ctx, counts, n, out, ctx.scan_blocks, 0);
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_counts, out + n, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.Sync();
+  return ctx.host_counts[0];
+}
+
+void TreeSums(Ctx& ctx, const double* const* partials, int arrays, int64_t n, int slot) {
+  TreeDots(ctx, partials, nullptr, arrays, n, slot);
+}
+
+void TreeDots(Ctx& ctx, const double* const* x, const double* const* y, int arrays, int64_t n, int slot) {
+  if (n <= 0) {
+    SPAI_CUDA(cudaMemsetAsync(ctx.scalars.data() + slot, 0, sizeof(double) * arrays, ctx.stream));
+    return;
+  }
+  TreeArgs args{};
+  for (int a = 0; a < arrays; ++a) {
+    args.src[a] = x[a];
+    args.src2[a] = y != nullptr ? y[a] : nullptr;
+  }
+  int64_t count = n;
+  size_t scratch_need = 0;
+  for (int64_t m = n; m > kTreeChunk; m = CeilDiv(m, kTreeChunk)) scratch_need += static_cast<size_t>(arrays) * CeilDiv(m, kTreeChunk);
+  ctx.tree_scratch.Reserve(scratch_need + 8, ctx.stream);
+  size_t scratch_at = 0;
+  while (true) {
+    const int64_t chunks = CeilDiv(count, kTreeChunk);
+    double* dst;
+    int64_t stride;
+    if (chunks == 1) {
+      dst = ctx.scalars.data() + slot;
+      stride = 1;
+    } else {
+      dst = ctx.tree_scratch.data() + scratch_at;
+      stride = chunks;
+    }
+    dim3 grid(static_cast<unsigned>(chunks), static_cast<unsigned>(arrays));
+    TreeChunkKernel<<<grid, kTreeLanes, 0, ctx.stream>>>(args, count, dst, stride);
+    SPAI_LAUNCH_CHECK();
+    if (chunks == 1) break;
+    for (int a = 0; a < arrays; ++a) {
+      args.src[a] = dst + a * chunks;
+      args.src2[a] = nullptr;
+    }
+    scratch_at += static_cast<size_t>(arrays) * chunks;
+    count = chunks;
+  }
+}
+
+void FetchScalars(Ctx& ctx, int first_slot, int count, double* out) {
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_scalars, ctx.scalars.data() + first_slot, sizeof(double) * count,
+                            cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.Sync();
+  std::memcpy(out, ctx.host_scalars, sizeof(double) * count);
+}
+
+template <class T>
+void ColumnSquares(Ctx& ctx, CscView<T> x, double* partial) {
+  ColumnSquaresKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(x, partial);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+void ColumnDots(Ctx& ctx, CscView<T> x, CscView<T> y, double* partial) {
+  ColumnDotsKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(x, y, partial);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T>& x, double xs, DevCsc<T>& out,
+           UnionMode mode) {
+  const int64_t cols = y.cols;
+  ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+  const int grid = GridFor(cols, 128);
+  UnionKernel<T, false><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode),
+                                                      ctx.counts.data(), nullptr, nullptr, nullptr);
+  SPAI_LAUNCH_CHECK();
+  DevCsc<T> result;
+  result.Shape(y.rows, cols, ctx.stream);
+  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, result.ptr.data());
+  result.ReserveNnz(nnz, ctx.stream);
+  UnionKernel<T, true><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode),
+                                                     nullptr, result.ptr.data(), result.idx.data(), result.val.data());
+  SPAI_LAUNCH_CHECK();
+  out.Swap(result);
+}
+
+template <class T>
+void DiagScale(Ctx& ctx, const T* d, const DevCsc<T>& b, DevCsc<T>& out, bool prune_zeros) {
+  DevCsc<T> result;
+  result.Shape(b.rows, b.cols, ctx.stream);
+  result.ReserveNnz(b.nnz, ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(result.ptr.data(), b.ptr.data(), sizeof(int64_t) * (b.cols + 1), cudaMemcpyDeviceToDevice,
+                            ctx.stream));
+  if (b.nnz > 0) {
+    SPAI_CUDA(cudaMemcpyAsync(result.idx.data(), b.idx.data(), sizeof(int32_t) * b.nnz, cudaMemcpyDeviceToDevice,
+                              ctx.stream));
+    DiagScaleKernel<T><<<GridFor(b.nnz, 256), 256, 0, ctx.stream>>>(d, b.idx.data(), b.val.data(), b.nnz,
+                                                                   result.val.data());
+    SPAI_LAUNCH_CHECK();
+  }
+  out.Swap(result);
+  if (prune_zeros) DropZeros(ctx, out);
+}
+
+template <class T>
+void ScaleColumns(Ctx& ctx, DevCsc<T>& x, const double* scale) {
+  ScaleColumnsKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(View(x), x.val.data(), scale);
+  SPAI_LAUNCH_CHECK();
+  DropZeros(ctx, x);
+}
+
+template <class T>
+void DropZeros(Ctx& ctx, DevCsc<T>& x) {
+  RunFilter(ctx, x, KeepNonZero<T>{});
+}
+
+template <class T>
+void PruneColumnRelative(Ctx& ctx, DevCsc<T>& m) {
+  RunFilter(ctx, m, KeepColumnRelative<T>{});
+}
+
+template <class T>
+void PruneAbsAtMost(Ctx& ctx, DevCsc<T>& x, double limit) {
+  RunFilter(ctx, x, KeepAboveLimit<T>{limit});
+}
+
+template <class T>
+void KeepTopKPerColumn(Ctx& ctx, DevCsc<T>& x, int64_t k, bool protect_diagonal) {
+  KeepTopK<T> pred;
+  pred.k = k;
+  pred.protect = protect_diagonal;
+  RunFilter(ctx, x, pred);
+}
+
+template <class T>
+void GlobalDropByScore(Ctx& ctx, DevCsc<T>& x, const double* entry_scores, bool skip_diagonal, int64_t drop) {
+  const int64_t cols = x.cols;
+  ctx.counts2.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+  int64_t candidates = x.nnz;
+  const int64_t* column_base = nullptr;
+  if (skip_diagonal) {
+    ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+    NonDiagonalCountKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(View(x), ctx.counts.data());
+    SPAI_LAUNCH_CHECK();
+    candidates = ScanCounts(ctx, ctx.counts.data(), cols, ctx.counts2.data());
+    column_base = ctx.counts2.data();
+  }
+  if (drop <= 0 || drop > candidates) {
+    throw std::invalid_argument("Invalid global sparse dropping count");
+  }
+  DevBuf<unsigned long long> keys;
+  keys.Reserve(static_cast<size_t>(candidates), ctx.stream);
+  GatherCandidateKeysKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(View(x), entry_scores, column_base,
+                                                                          skip_diagonal, keys.data());
+  SPAI_LAUNCH_CHECK();
+  unsigned long long init[3] = {0ull, 0ull, static_cast<unsigned long long>(drop)};
+  SPAI_CUDA(cudaMemcpyAsync(ctx.select_state.data(), init, sizeof(init), cudaMemcpyHostToDevice, ctx.stream));
+  SPAI_CUDA(cudaMemsetAsync(ctx.histogram.data(), 0, 256 * sizeof(unsigned long long), ctx.stream));
+  const int grid = GridFor(candidates, 256);
+  for (int pass = 0; pass < 16; ++pass) {
+    RadixHistKernel<<<grid, 256, 0, ctx.stream>>>(keys.data(), candidates, pass, ctx.select_state.data(),
+                                                  ctx.histogram.data());
+    SPAI_LAUNCH_CHECK();
+    RadixDecideKernel<<<1, 32, 0, ctx.stream>>>(pass, ctx.select_state.data(), ctx.histogram.data());
+    SPAI_LAUNCH_CHECK();
+  }
+  KeepAboveCutoff<T> pred;
+  pred.scores = entry_scores;
+  pred.column_base = column_base;
+  pred.cutoff = ctx.select_state.data();
+  pred.skip_diag = skip_diagonal;
+  RunFilter(ctx, x, pred);
+  keys.Release();
+}
+
+template <class T>
+void Transpose(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& t) {
+  DevCsc<T> result;
+  result.Shape(x.cols, x.rows, ctx.stream);
+  ctx.counts.Reserve(static_cast<size_t>(x.rows + 1), ctx.stream);
+  unsigned long long* row_counts = reinterpret_cast<unsigned long long*>(ctx.counts.data());
+  SPAI_CUDA(cudaMemsetAsync(row_counts, 0, sizeof(int64_t) * (x.rows + 1), ctx.stream));
+  if (x.nnz > 0) {
+    RowCountKernel<<<GridFor(x.nnz, 256), 256, 0, ctx.stream>>>(x.idx.data(), x.nnz, row_counts);
+    SPAI_LAUNCH_CHECK();
+  }
+  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), x.rows, result.ptr.data());
+  result.ReserveNnz(nnz, ctx.stream);
+  SPAI_CUDA(cudaMemsetAsync(row_counts, 0, sizeof(int64_t) * (x.rows + 1), ctx.stream));
+  if (nnz > 0) {
+    ScatterKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(View(x), result.ptr.data(), row_counts,
+                                                                  result.idx.data(), result.val.data());
+    SPAI_LAUNCH_CHECK();
+    SortSegments<T>(ctx, result.ptr.data(), x.rows, result.idx.data(), result.val.data());
+  }
+  t.Swap(result);
+}
+
+template <class T>
+void Copy(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& out) {
+  DevCsc<T> result;
+  result.Shape(x.rows, x.cols, ctx.stream);
+  result.ReserveNnz(x.nnz, ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(result.ptr.data(), x.ptr.data(), sizeof(int64_t) * (x.cols + 1), cudaMemcpyDeviceToDevice,
+                            ctx.stream));
+  if (x.nnz > 0) {
+    SPAI_CUDA(cudaMemcpyAsync(result.idx.data(), x.idx.data(), sizeof(int32_t) * x.nnz, cudaMemcpyDeviceToDevice,
+                              ctx.stream));
+    SPAI_CUDA(cudaMemcpyAsync(result.val.data(), x.val.data(), sizeof(T) * x.nnz, cudaMemcpyDeviceToDevice,
+                              ctx.stream));
+  }
+  out.Swap(result);
+}
+
+template <class T>
+void DropScores(Ctx& ctx, const DevCsc<T>& m, const double* col_norm2, const double* tmp, double* scores) {
+  if (m.nnz == 0) return;
+  DropScoresKernel<T><<<GridFor(m.nnz, 256), 256, 0, ctx.stream>>>(View(m), col_norm2, tmp, scores);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+void AbsScores(Ctx& ctx, const DevCsc<T>& x, double* scores) {
+  if (x.nnz == 0) return;
+  AbsScoresKernel<T><<<GridFor(x.nnz, 256), 256, 0, ctx.stream>>>(x.val.data(), x.nnz, scores);
+  SPAI_LAUNCH_CHECK();
+}
+
+void FillZero(Ctx& ctx, int64_t* ptr, int64_t n) {
+  SPAI_CUDA(cudaMemsetAsync(ptr, 0, sizeof(int64_t) * n, ctx.stream));
+}
+
+template <class S, class D>
+void ConvertValues(Ctx& ctx, const S* src, D* dst, int64_t n) {
+  if (n <= 0) return;
+  ConvertKernel<S, D><<<GridFor(n, 256), 256, 0, ctx.stream>>>(src, dst, n);
+  SPAI_LAUNCH_CHECK();
+}
+
+#define SPAI_INSTANTIATE(T)                                                                                   \
+  template void ColumnSquares<T>(Ctx&, CscView<T>, double*);                                                  \
+  template void ColumnDots<T>(Ctx&, CscView<T>, CscView<T>, double*);                                         \
+  template void Union<T>(Ctx&, const DevCsc<T>&, bool, double, const DevCsc<T>&, double, DevCsc<T>&, UnionMode); \
+  template void DiagScale<T>(Ctx&, const T*, const DevCsc<T>&, DevCsc<T>&, bool);                             \
+  template void ScaleColumns<T>(Ctx&, DevCsc<T>&, const double*);                                             \
+  template void DropZeros<T>(Ctx&, DevCsc<T>&);                                                               \
+  template void PruneColumnRelative<T>(Ctx&, DevCsc<T>&);                                                     \
+  template void PruneAbsAtMost<T>(Ctx&, DevCsc<T>&, double);                                                  \
+  template void KeepTopKPerColumn<T>(Ctx&, DevCsc<T>&, int64_t, bool);                                        \
+  template void GlobalDropByScore<T>(Ctx&, DevCsc<T>&, const double*, bool, int64_t);                         \
+  template void Transpose<T>(Ctx&, const DevCsc<T>&, DevCsc<T>&);                                             \
+  template void Copy<T>(Ctx&, const DevCsc<T>&, DevCsc<T>&);                                                  \
+  template void DropScores<T>(Ctx&, const DevCsc<T>&, const double*, const double*, double*);                 \
+  template void AbsScores<T>(Ctx&, const DevCsc<T>&, double*);
+
+SPAI_INSTANTIATE(double)
+SPAI_INSTANTIATE(float)
+
+template void ConvertValues<double, float>(Ctx&, const double*, float*, int64_t);
+template void ConvertValues<float, double>(Ctx&, const float*, double*, int64_t);
+template void ConvertValues<double, double>(Ctx&, const double*, double*, int64_t);
+
+}  // namespace spai

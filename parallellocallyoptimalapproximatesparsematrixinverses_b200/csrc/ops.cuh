@@ -1,0 +1,126 @@
+#pragma once
+// Host-callable device operations on sparse matrices in HBM.  Each operation
+// is stream-ordered on Ctx::stream.  Functions that must size an output read
+// one int64 back from the device (ScanCounts); everything else is
+// asynchronous.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <vector>
+
+#include "device.cuh"
+
+namespace spai {
+
+// Per-call device context: stream, scratch buffers and pinned readback slots.
+struct Ctx {
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int sm_count = 148;
+  DevBuf<int64_t> counts;       // per-column counts, n + 1
+  DevBuf<int64_t> counts2;      // second per-column count array
+  DevBuf<int64_t> scan_blocks;  // scan tile sums
+  DevBuf<double> partials[8];   // per-column partial sums of the canonical reductions
+  DevBuf<double> tree_scratch;  // tree-sum chunk sums
+  DevBuf<double> scalars;       // device-resident reduction results (kScalarSlots)
+  DevBuf<double> colvec[6];     // per-column coefficient vectors (inner-outer)
+  DevBuf<unsigned long long> select_state;  // radix-select state
+  DevBuf<unsigned long long> histogram;     // radix-select histogram
+  DevBuf<int32_t> flags;        // device flags (zero pruning happened, overflow)
+  double* host_scalars = nullptr;   // pinned, kScalarSlots
+  int64_t* host_counts = nullptr;   // pinned, 8
+  int32_t* host_flags = nullptr;    // pinned, 8
+
+  static constexpr int kScalarSlots = 64;
+
+  void Init(int device_ordinal);
+  void Destroy();
+  void Sync();
+  double* Partial(int i, int64_t n) {
+    partials[i].Reserve(static_cast<size_t>(n), stream);
+    return partials[i].data();
+  }
+};
+
+// out[0] = 0, out[i + 1] = counts[0] + ... + counts[i]; returns out[n] (one
+// device-to-host read).  counts and out may alias.
+int64_t ScanCounts(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out);
+
+// Canonical reduction: the fixed 4096-wide tree over `n` partial sums.
+// Results land in ctx.scalars[slot + i] for i < arrays; read them with
+// FetchScalars.
+void TreeSums(Ctx& ctx, const double* const* partials, int arrays, int64_t n, int slot);
+// Same tree over the products x[a][i] * y[a][i] (dot products of vectors).
+void TreeDots(Ctx& ctx, const double* const* x, const double* const* y, int arrays, int64_t n, int slot);
+void FetchScalars(Ctx& ctx, int first_slot, int count, double* out);
+
+// Per-column sequential partial sums (storage order, as Eigen within a column).
+template <class T>
+void ColumnSquares(Ctx& ctx, CscView<T> x, double* partial);
+// sum over rows present in both columns of x*y, ascending rows.
+template <class T>
+void ColumnDots(Ctx& ctx, CscView<T> x, CscView<T> y, double* partial);
+
+// Union combination: out = ys*Y (+) xs*X (sparse_operations.cpp:22-49).
+// kAxpby prunes exact zeros; kHalfSum computes 0.5*(y + x) and keeps zeros
+// (the symmetrisation of dropping.cpp:115-117).
+enum class UnionMode { kAxpby = 0, kHalfSum = 1 };
+template <class T>
+void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T>& x, double xs, DevCsc<T>& out,
+           UnionMode mode);
+
+// Row scaling out = diag(d) * b (Pr * X with a diagonal Pr); optional zero pruning.
+template <class T>
+void DiagScale(Ctx& ctx, const T* d, const DevCsc<T>& b, DevCsc<T>& out, bool prune_zeros);
+
+// x(:, j) *= scale[j] (device array), then exact zeros pruned (sparse_operations.cpp:28-39).
+template <class T>
+void ScaleColumns(Ctx& ctx, DevCsc<T>& x, const double* scale);
+
+// Filters (each writes a compacted copy and swaps it in).
+template <class T>
+void DropZeros(Ctx& ctx, DevCsc<T>& x);
+// keep iff v != 0 and (diagonal or |v| >= eps * ||column||_2)   (dropping.cpp:124-133)
+template <class T>
+void PruneColumnRelative(Ctx& ctx, DevCsc<T>& m);
+// keep iff !(|v| <= limit)   (dropping.cpp:182-185 with limit = ||X||_F * eps)
+template <class T>
+void PruneAbsAtMost(Ctx& ctx, DevCsc<T>& x, double limit);
+// keep the k largest (|v|, row) per column; the diagonal is always kept (and
+// counts toward k) when protect_diagonal.
+template <class T>
+void KeepTopKPerColumn(Ctx& ctx, DevCsc<T>& x, int64_t k, bool protect_diagonal);
+
+// Global budget selection (dropping.cpp:64-93,145-171,192-222).
+// scores: one key per candidate, candidates enumerated in column-major order
+// (for M the diagonal is excluded); drops the `drop` smallest (score, offset).
+template <class T>
+void GlobalDropByScore(Ctx& ctx, DevCsc<T>& x, const double* entry_scores, bool skip_diagonal, int64_t drop);
+
+// Transpose with rows sorted inside every output column.
+template <class T>
+void Transpose(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& t);
+
+// Copies.
+template <class T>
+void Copy(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& out);
+
+// Residual-aware drop score for every entry of M (dropping.cpp:19-29):
+// s = v*v*cn[row] + 2*v*tmp, non-finite -> -inf; tmp aligned with M entries.
+template <class T>
+void DropScores(Ctx& ctx, const DevCsc<T>& m, const double* col_norm2, const double* tmp, double* scores);
+
+// |v| for every entry (direction budget key).
+template <class T>
+void AbsScores(Ctx& ctx, const DevCsc<T>& x, double* scores);
+
+// Number of structural nonzeros (host value already known) -- helper to set
+// every column pointer of an empty matrix.
+void FillZero(Ctx& ctx, int64_t* ptr, int64_t n);
+
+// Convert values between storage precisions (identical pattern).
+template <class S, class D>
+void ConvertValues(Ctx& ctx, const S* src, D* dst, int64_t n);
+
+}  // namespace spai

@@ -1,0 +1,763 @@
+// Device implementation of Global SPAI CG / MR / LOMR and Inner-Outer MR /
+// LOMR.  Each method follows the reference's control flow line for line
+// (file:line given at each method); the arithmetic of every step runs in the
+// kernels of ops.cu and spgemm.cu.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <limits>
+#include <stdexcept>
+#include <type_traits>
+#include <vector>
+
+#include "cod2x2.cuh"
+#include "device.cuh"
+#include "ops.cuh"
+#include "solver.cuh"
+#include "spgemm.cuh"
+
+namespace spai {
+
+namespace {
+
+constexpr double kEpsilon = std::numeric_limits<double>::epsilon();  // methods_common.hpp:32
+constexpr double kMinDensity = 1e-9;                                 // include/methods.hpp:15
+
+__device__ __forceinline__ bool FiniteNonZero(double v) { return isfinite(v) && fabs(v) > 0.0; }
+
+__device__ __forceinline__ double SafeQuotient(double num, double den) {
+  if (!FiniteNonZero(den)) return 0.0;
+  const double q = __ddiv_rn(num, den);
+  return isfinite(q) ? q : 0.0;
+}
+
+// Per-column Inner-Outer step lengths (inner_outer_common.hpp:50-69).
+__global__ void InnerOuterStepKernel(int64_t n, const double* __restrict__ r_az, const double* __restrict__ az_az,
+                                     const double* __restrict__ az_aq, const double* __restrict__ aq_aq,
+                                     const double* __restrict__ r_aq, bool locally_optimal, bool first,
+                                     double* __restrict__ delta, double* __restrict__ gamma,
+                                     double* __restrict__ normalization) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double d;
+    double g;
+    if (!locally_optimal || first) {
+      d = SafeQuotient(r_az[j], az_az[j]);
+      g = locally_optimal ? 1.0 : 0.0;
+    } else {
+      const double gram[4] = {az_az[j], az_aq[j], az_aq[j], aq_aq[j]};
+      const double rhs[2] = {r_az[j], r_aq[j]};
+      double coef[2];
+      SolveLeastSquares2x2(gram, rhs, coef);
+      d = coef[0];
+      g = coef[1];
+    }
+    delta[j] = d;
+    gamma[j] = g;
+    const double inverse = d != 0.0 ? __ddiv_rn(1.0, d) : 1.0;
+    normalization[j] = isfinite(inverse) ? inverse : 1.0;
+  }
+}
+
+__global__ void SafeQuotientKernel(int64_t n, const double* __restrict__ num, const double* __restrict__ den,
+                                   double* __restrict__ out) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[j] = SafeQuotient(num[j], den[j]);
+  }
+}
+
+__global__ void IdentityKernel(int64_t n, int64_t* __restrict__ ptr, int32_t* __restrict__ idx) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j <= n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    ptr[j] = j;
+    if (j < n) idx[j] = static_cast<int32_t>(j);
+  }
+}
+
+template <class T>
+__global__ void FillKernel(T* __restrict__ out, int64_t n, T value) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[i] = value;
+  }
+}
+
+__global__ void NarrowIndexKernel(const int64_t* __restrict__ src, int32_t* __restrict__ dst, int64_t n) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    dst[i] = static_cast<int32_t>(src[i]);
+  }
+}
+
+__global__ void WidenIndexKernel(const int32_t* __restrict__ src, int64_t* __restrict__ dst, int64_t n) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    dst[i] = static_cast<int64_t>(src[i]);
+  }
+}
+
+// Uploads a host CSC (int64 indices, f64 values) as DevCsc<T>.
+template <class T>
+void UploadCsc(Ctx& ctx, const HostCsc& h, DevCsc<T>& d, DevBuf<int64_t>& stage_idx, DevBuf<double>& stage_val) {
+  d.Shape(h.rows, h.cols, ctx.stream);
+  // column offsets are rebased so the device matrix starts at 0
+  std::vector<int64_t> ptr(h.cols + 1);
+  const int64_t base = h.ptr[0];
+  for (int64_t j = 0; j <= h.cols; ++j) ptr[j] = h.ptr[j] - base;
+  const int64_t nnz = ptr[h.cols];
+  d.ReserveNnz(nnz, ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(d.ptr.data(), ptr.data(), sizeof(int64_t) * (h.cols + 1), cudaMemcpyHostToDevice,
+                            ctx.stream));
+  if (nnz > 0) {
+    stage_idx.Reserve(static_cast<size_t>(nnz), ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(stage_idx.data(), h.idx + base, sizeof(int64_t) * nnz, cudaMemcpyHostToDevice,
+                              ctx.stream));
+    NarrowIndexKernel<<<GridFor(nnz, 256), 256, 0, ctx.stream>>>(stage_idx.data(), d.idx.data(), nnz);
+    SPAI_LAUNCH_CHECK();
+    if (std::is_same<T, double>::value) {
+      SPAI_CUDA(cudaMemcpyAsync(d.val.data(), h.val + base, sizeof(double) * nnz, cudaMemcpyHostToDevice,
+                                ctx.stream));
+    } else {
+      stage_val.Reserve(static_cast<size_t>(nnz), ctx.stream);
+      SPAI_CUDA(cudaMemcpyAsync(stage_val.data(), h.val + base, sizeof(double) * nnz, cudaMemcpyHostToDevice,
+                                ctx.stream));
+      ConvertValues<double, T>(ctx, stage_val.data(), d.val.data(), nnz);
+    }
+  }
+  // the pageable host arrays must stay valid until the copies finish
+  ctx.Sync();
+}
+
+template <class T>
+class Solver final : public SolverBase {
+ public:
+  Solver(Ctx& ctx, const SolveOptions& options) : ctx_(ctx), opt_(options) {}
+
+  void Upload(const HostCsc& a, const HostCsc* m0, const HostCsc* pr) override {
+    n_ = a.cols;
+    DevBuf<int64_t> stage_idx;
+    DevBuf<double> stage_val;
+    UploadCsc(ctx_, a, a64_, stage_idx, stage_val);
+    if constexpr (!std::is_same<T, double>::value) {
+      UploadCsc(ctx_, a, a_, stage_idx, stage_val);
+    }
+    Transpose(ctx_, A(), a_csr_);
+    // ||A e_k||^2 per column (methods_common.cpp:65-76)
+    col_norm2_.Reserve(static_cast<size_t>(n_), ctx_.stream);
+    if (opt_.dropping) {
+      ColumnSquares(ctx_, View(a64_), col_norm2_.data());
+    } else {
+      SPAI_CUDA(cudaMemsetAsync(col_norm2_.data(), 0, sizeof(double) * n_, ctx_.stream));
+    }
+    // preconditioner (methods_common.cpp:105-110)
+    pr_diagonal_ = true;
+    std::vector<double> diag(n_);
+    if (pr != nullptr) {
+      pr_diagonal_ = IsFullDiagonal(*pr);
+      if (pr_diagonal_) {
+        for (int64_t j = 0; j < n_; ++j) diag[j] = pr->val[pr->ptr[j]];
+      } else {
+        UploadCsc(ctx_, *pr, pr_, stage_idx, stage_val);
+        Transpose(ctx_, pr_, pr_csr_);
+      }
+    } else {
+      for (int64_t j = 0; j < n_; ++j) diag[j] = DiagonalEntry(a, j);
+      for (int64_t j = 0; j < n_; ++j) {
+        if (!std::isfinite(diag[j]) || diag[j] <= 0.0) {
+          throw std::invalid_argument("A has an invalid diagonal entry; provide Pr explicitly");
+        }
+      }
+      for (int64_t j = 0; j < n_; ++j) {
+        const double inverse = 1.0 / diag[j];
+        if (!std::isfinite(inverse)) {
+          throw std::invalid_argument("A diagonal cannot be inverted safely; provide Pr explicitly");
+        }
+        diag[j] = inverse;
+      }
+    }
+    if (pr_diagonal_) {
+      std::vector<T> host(n_);
+      for (int64_t j = 0; j < n_; ++j) host[j] = static_cast<T>(diag[j]);
+      pr_vec_.Reserve(static_cast<size_t>(n_), ctx_.stream);
+      SPAI_CUDA(cudaMemcpyAsync(pr_vec_.data(), host.data(), sizeof(T) * n_, cudaMemcpyHostToDevice, ctx_.stream));
+      ctx_.Sync();
+    }
+    // M0 (methods_common.cpp:78-103): given, or the identity
+    if (m0 != nullptr) {
+      UploadCsc(ctx_, *m0, m0_, stage_idx, stage_val);
+    } else {
+      m0_.Shape(n_, n_, ctx_.stream);
+      m0_.ReserveNnz(n_, ctx_.stream);
+      IdentityKernel<<<GridFor(n_ + 1, 256), 256, 0, ctx_.stream>>>(n_, m0_.ptr.data(), m0_.idx.data());
+      SPAI_LAUNCH_CHECK();
+      FillKernel<T><<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(m0_.val.data(), n_, T(1));
+      SPAI_LAUNCH_CHECK();
+    }
+    ctx_.Sync();
+  }
+
+  void Run() override {
+    history_.clear();
+    converged_ = false;
+    iterations_ = 0;
+    Copy(ctx_, m0_, m_);
+    for (DevCsc<T>* x : {&r_, &z_, &p_, &ap_, &az_, &tmp_, &q_}) Empty(*x);
+    const bool inner_outer = opt_.method == Method::kInnerOuterMr || opt_.method == Method::kInnerOuterLomr;
+    symmetric_ = !inner_outer;
+    // PrepareStateManager (methods_common.cpp:126-157)
+    if (opt_.dropping) {
+      ApplyDroppingStrategy();
+    } else {
+      Residual();
+    }
+    initial_residual_ = std::sqrt(SquaredNorm(r_));
+    switch (opt_.method) {
+      case Method::kGlobalCg: RunCg(); break;
+      case Method::kGlobalMr: RunMr(); break;
+      case Method::kGlobalLomr: RunLomr(); break;
+      case Method::kInnerOuterMr: RunInnerOuter(false); break;
+      case Method::kInnerOuterLomr: RunInnerOuter(true); break;
+    }
+    ctx_.Sync();
+  }
+
+  void Download(SolveOutput& out) override {
+    out.rows = m_.rows;
+    out.cols = m_.cols;
+    out.ptr.resize(m_.cols + 1);
+    out.idx.resize(m_.nnz);
+    out.val.resize(m_.nnz);
+    SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), m_.ptr.data(), sizeof(int64_t) * (m_.cols + 1), cudaMemcpyDeviceToHost,
+                              ctx_.stream));
+    if (m_.nnz > 0) {
+      DevBuf<int64_t> wide;
+      wide.Reserve(static_cast<size_t>(m_.nnz), ctx_.stream);
+      WidenIndexKernel<<<GridFor(m_.nnz, 256), 256, 0, ctx_.stream>>>(m_.idx.data(), wide.data(), m_.nnz);
+      SPAI_LAUNCH_CHECK();
+      SPAI_CUDA(cudaMemcpyAsync(out.idx.data(), wide.data(), sizeof(int64_t) * m_.nnz, cudaMemcpyDeviceToHost,
+                                ctx_.stream));
+      if constexpr (std::is_same<T, double>::value) {
+        SPAI_CUDA(cudaMemcpyAsync(out.val.data(), m_.val.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost,
+                                  ctx_.stream));
+        ctx_.Sync();
+      } else {
+        DevBuf<double> widev;
+        widev.Reserve(static_cast<size_t>(m_.nnz), ctx_.stream);
+        ConvertValues<T, double>(ctx_, m_.val.data(), widev.data(), m_.nnz);
+        SPAI_CUDA(cudaMemcpyAsync(out.val.data(), widev.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost,
+                                  ctx_.stream));
+        ctx_.Sync();
+      }
+    }
+    ctx_.Sync();
+    out.history = history_;
+    out.iterations = iterations_;
+    out.converged = converged_;
+  }
+
+  int64_t iterations() const override { return iterations_; }
+  int64_t m_nnz() const override { return m_.nnz; }
+  int64_t n() const override { return n_; }
+  const void* DeviceA() const override { return &A(); }
+  const void* DeviceA64() const override { return &a64_; }
+
+  void ExportMForPcg(void* csr_out, bool want_fp32) override {
+    DevCsc<T> mt;
+    Transpose(ctx_, m_, mt);
+    if (want_fp32) {
+      auto* out = static_cast<DevCsc<float>*>(csr_out);
+      if constexpr (std::is_same<T, float>::value) {
+        out->Swap(mt);
+      } else {
+        ConvertCsc(mt, *out);
+      }
+    } else {
+      auto* out = static_cast<DevCsc<double>*>(csr_out);
+      if constexpr (std::is_same<T, double>::value) {
+        out->Swap(mt);
+      } else {
+        ConvertCsc(mt, *out);
+      }
+    }
+  }
+
+ private:
+  template <class D>
+  void ConvertCsc(const DevCsc<T>& src, DevCsc<D>& dst) {
+    dst.Shape(src.rows, src.cols, ctx_.stream);
+    dst.ReserveNnz(src.nnz, ctx_.stream);
+    SPAI_CUDA(cudaMemcpyAsync(dst.ptr.data(), src.ptr.data(), sizeof(int64_t) * (src.cols + 1),
+                              cudaMemcpyDeviceToDevice, ctx_.stream));
+    if (src.nnz > 0) {
+      SPAI_CUDA(cudaMemcpyAsync(dst.idx.data(), src.idx.data(), sizeof(int32_t) * src.nnz, cudaMemcpyDeviceToDevice,
+                                ctx_.stream));
+      ConvertValues<T, D>(ctx_, src.val.data(), dst.val.data(), src.nnz);
+    }
+  }
+
+  const DevCsc<T>& A() const {
+    if constexpr (std::is_same<T, double>::value) {
+      return a64_;
+    } else {
+      return a_;
+    }
+  }
+
+  static bool IsFullDiagonal(const HostCsc& pr) {
+    if (pr.nnz != pr.cols) return false;
+    for (int64_t j = 0; j < pr.cols; ++j) {
+      if (pr.ptr[j + 1] - pr.ptr[j] != 1 || pr.idx[pr.ptr[j]] != j) return false;
+    }
+    return true;
+  }
+
+  static double DiagonalEntry(const HostCsc& a, int64_t j) {
+    const int64_t* begin = a.idx + a.ptr[j];
+    const int64_t* end = a.idx + a.ptr[j + 1];
+    const int64_t* it = std::lower_bound(begin, end, j);
+    if (it != end && *it == j) return a.val[it - a.idx];
+    return 0.0;
+  }
+
+  void Empty(DevCsc<T>& x) {
+    x.Shape(n_, n_, ctx_.stream);
+    x.ReserveNnz(0, ctx_.stream);
+    FillZero(ctx_, x.ptr.data(), n_ + 1);
+  }
+
+  // ---- products (state_manager.cpp:47-66; dropping.cpp:97-104) ------------
+  void MulA(const DevCsc<T>& in, DevCsc<T>& out) {
+    Spgemm(ctx_, A(), a_csr_, in, out, opt_.dropping ? Epilogue::kPlain : Epilogue::kPruneZeros);
+  }
+
+  void MulPr(const DevCsc<T>& in, DevCsc<T>& out) {
+    if (pr_diagonal_) {
+      DiagScale(ctx_, pr_vec_.data(), in, out, !opt_.dropping);
+    } else {
+      Spgemm(ctx_, pr_, pr_csr_, in, out, opt_.dropping ? Epilogue::kPlain : Epilogue::kPruneZeros);
+    }
+  }
+
+  void Residual() { Spgemm(ctx_, A(), a_csr_, m_, r_, Epilogue::kResidual); }
+
+  // ---- reductions ----------------------------------------------------------
+  double Dot(const DevCsc<T>& x, const DevCsc<T>& y) {
+    double* part = ctx_.Partial(0, n_);
+    ColumnDots(ctx_, View(x), View(y), part);
+    const double* parts[1] = {part};
+    TreeSums(ctx_, parts, 1, n_, 0);
+    double out;
+    FetchScalars(ctx_, 0, 1, &out);
+    return out;
+  }
+
+  double SquaredNorm(const DevCsc<T>& x) {
+    double* part = ctx_.Partial(0, n_);
+    ColumnSquares(ctx_, View(x), part);
+    const double* parts[1] = {part};
+    TreeSums(ctx_, parts, 1, n_, 0);
+    double out;
+    FetchScalars(ctx_, 0, 1, &out);
+    return out;
+  }
+
+  // ---- sparse updates (sparse_operations.cpp:22-49) ------------------------
+  void AddScaled(DevCsc<T>& t, const DevCsc<T>& d, double c) {
+    if (c != 0.0) {
+      Union(ctx_, t, false, 1.0, d, c, t, UnionMode::kAxpby);
+    } else {
+      DropZeros(ctx_, t);
+    }
+  }
+
+  void LinComb(const DevCsc<T>& x, double a, DevCsc<T>& y, double b) {
+    Union(ctx_, y, true, b, x, a, y, UnionMode::kAxpby);
+  }
+
+  // state_manager.cpp:68-71
+  int64_t MaxNonZeros() const {
+    const double limit = opt_.max_density * static_cast<double>(n_) * static_cast<double>(n_);
+    return std::max(n_, static_cast<int64_t>(std::floor(limit)));
+  }
+
+  // dropping.cpp:106-120
+  void EnsureSymmetry() {
+    if (!symmetric_) return;
+    DevCsc<T> mt;
+    Transpose(ctx_, m_, mt);
+    Union(ctx_, m_, false, 1.0, mt, 1.0, m_, UnionMode::kHalfSum);
+  }
+
+  // dropping.cpp:122-175 (or the per-column top-k variant)
+  void ApplyDroppingStrategy() {
+    EnsureSymmetry();
+    PruneColumnRelative(ctx_, m_);
+    if (opt_.topk > 0) {
+      KeepTopKPerColumn(ctx_, m_, opt_.topk, true);
+      Residual();
+      return;
+    }
+    Residual();
+    const int64_t budget = MaxNonZeros();
+    const int64_t nonzeros = m_.nnz;
+    if (nonzeros <= budget) return;
+    DevBuf<double> tmp_values;
+    DevBuf<double> scores;
+    tmp_values.Reserve(static_cast<size_t>(nonzeros), ctx_.stream);
+    scores.Reserve(static_cast<size_t>(nonzeros), ctx_.stream);
+    // (A*R)(k, l) at every entry (k, l) of M: the masked product
+    SpgemmMasked(ctx_, a_csr_, r_, m_, tmp_values.data());
+    DropScores(ctx_, m_, col_norm2_.data(), tmp_values.data(), scores.data());
+    GlobalDropByScore(ctx_, m_, scores.data(), true, nonzeros - budget);
+    Residual();
+  }
+
+  // dropping.cpp:177-224 (or the per-column top-k variant)
+  bool DropForMatrixType(DevCsc<T>& x) {
+    if (!opt_.dropping) return false;
+    const int64_t original = x.nnz;
+    const double limit = std::sqrt(SquaredNorm(x)) * kEpsilon;
+    PruneAbsAtMost(ctx_, x, limit);
+    if (opt_.topk > 0) {
+      KeepTopKPerColumn(ctx_, x, opt_.topk, false);
+      return x.nnz != original;
+    }
+    const int64_t budget = MaxNonZeros();
+    if (x.nnz <= budget) return x.nnz != original;
+    DevBuf<double> scores;
+    scores.Reserve(static_cast<size_t>(x.nnz), ctx_.stream);
+    AbsScores(ctx_, x, scores.data());
+    GlobalDropByScore(ctx_, x, scores.data(), false, x.nnz - budget);
+    return true;
+  }
+
+  // state_manager.cpp:81-95
+  void StabilizeResiduals() {
+    const double norm = std::sqrt(SquaredNorm(r_));
+    const double floor = 64.0 * kEpsilon * std::sqrt(static_cast<double>(n_));
+    const double limit = std::max(10.0 * opt_.tolerance, floor);
+    if (std::isfinite(norm) && norm > limit) return;
+    Residual();
+  }
+
+  // methods_common.hpp:83-93
+  template <class F>
+  void UpdateResiduals(F recursive_update, bool stabilize) {
+    if (opt_.dropping) {
+      ApplyDroppingStrategy();
+      return;
+    }
+    recursive_update();
+    if (stabilize) StabilizeResiduals();
+  }
+
+  // result_operations.cpp:53-67
+  bool AppendIteration(const DevCsc<T>& direction) {
+    const int64_t iter = static_cast<int64_t>(history_.size());
+    iterations_ = iter;
+    const double residual = history_.empty() ? initial_residual_ : std::sqrt(SquaredNorm(r_));
+    const double entries = static_cast<double>(n_) * static_cast<double>(n_);
+    SingleIterationData row;
+    row.iteration = iter;
+    row.residual_norm = residual;
+    row.density_m = static_cast<double>(m_.nnz) / entries;
+    row.density_direction = static_cast<double>(direction.nnz) / entries;
+    history_.push_back(row);
+    if (row.residual_norm < opt_.tolerance) {
+      converged_ = true;
+      return true;
+    }
+    return !opt_.dropping && opt_.max_density < 1.0 && row.density_m >= opt_.max_density;
+  }
+
+  static bool FiniteNonZeroHost(double v) { return std::isfinite(v) && std::fabs(v) > 0.0; }
+
+  // ---- Global CG (conjugate_gradient.cpp:15-83) ----------------------------
+  void RunCg() {
+    MulPr(r_, z_);
+    Copy(ctx_, z_, p_);
+    double r_z = Dot(r_, z_);
+    DropForMatrixType(p_);
+    if (AppendIteration(p_)) return;
+    MulA(p_, ap_);
+    for (int64_t i = 1; i <= opt_.max_iterations; ++i) {
+      const double den = Dot(p_, ap_);
+      if (!FiniteNonZeroHost(r_z) || !FiniteNonZeroHost(den)) break;
+      const double alpha = r_z / den;
+      if (!std::isfinite(alpha)) break;
+      const double previous = r_z;
+      AddScaled(m_, p_, alpha);
+      UpdateResiduals([&] { AddScaled(r_, ap_, -alpha); }, false);
+      if (AppendIteration(p_)) break;
+      MulPr(r_, z_);
+      r_z = Dot(r_, z_);
+      const double beta = r_z / previous;
+      if (!std::isfinite(beta)) break;
+      LinComb(z_, 1.0, p_, beta);
+      DropForMatrixType(p_);
+      MulA(p_, ap_);
+    }
+  }
+
+  // num = <Z, Pr A Z>, den = ||Pr A Z||^2 (minimal_residual.cpp:44-52,78-88)
+  void MrProjection(double& num, double& den) {
+    if (pr_diagonal_) {
+      double* tt = ctx_.Partial(0, n_);
+      double* bt = ctx_.Partial(1, n_);
+      SpgemmExtras extras;
+      extras.row_scale = pr_vec_.data();
+      extras.proj_tt = tt;
+      extras.proj_bt = bt;
+      DevCsc<T> unused;
+      Spgemm(ctx_, A(), a_csr_, z_, unused, Epilogue::kProjection, extras);
+      const double* parts[2] = {bt, tt};
+      TreeSums(ctx_, parts, 2, n_, 0);
+      double out[2];
+      FetchScalars(ctx_, 0, 2, out);
+      num = out[0];
+      den = out[1];
+      return;
+    }
+    MulA(z_, az_);
+    MulPr(az_, tmp_);
+    num = Dot(z_, tmp_);
+    den = SquaredNorm(tmp_);
+  }
+
+  // ---- Global MR (minimal_residual.cpp:31-93) ------------------------------
+  void RunMr() {
+    MulPr(r_, z_);
+    if (AppendIteration(z_)) return;
+    double num = 0.0;
+    double den = 0.0;
+    MrProjection(num, den);
+    for (int64_t i = 1; i <= opt_.max_iterations; ++i) {
+      if (!FiniteNonZeroHost(den)) break;
+      const double alpha = num / den;
+      if (!std::isfinite(alpha)) break;
+      AddScaled(m_, z_, alpha);
+      UpdateResiduals([&] { Residual(); }, false);
+      if (AppendIteration(z_)) break;
+      MulPr(r_, z_);
+      MrProjection(num, den);
+    }
+  }
+
+  // ---- Global LOMR (locally_minimal_residual.cpp:54-118) -------------------
+  void RunLomr() {
+    MulPr(r_, z_);
+    if (AppendIteration(z_)) return;
+    for (int64_t i = 1; i <= opt_.max_iterations; ++i) {
+      MulA(p_, ap_);
+      MulA(z_, az_);
+      MulPr(az_, tmp_);
+      double* parts_buf[5];
+      for (int k = 0; k < 5; ++k) parts_buf[k] = ctx_.Partial(k, n_);
+      ColumnDots(ctx_, View(az_), View(tmp_), parts_buf[0]);
+      ColumnDots(ctx_, View(z_), View(az_), parts_buf[1]);
+      int arrays = 2;
+      if (i > 1) {
+        MulPr(ap_, tmp_);
+        ColumnDots(ctx_, View(ap_), View(tmp_), parts_buf[2]);
+        ColumnDots(ctx_, View(az_), View(tmp_), parts_buf[3]);
+        ColumnDots(ctx_, View(z_), View(ap_), parts_buf[4]);
+        arrays = 5;
+      }
+      const double* parts[5] = {parts_buf[0], parts_buf[1], parts_buf[2], parts_buf[3], parts_buf[4]};
+      TreeSums(ctx_, parts, arrays, n_, 0);
+      double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+      FetchScalars(ctx_, 0, arrays, s);
+      const double az_praz = s[0];
+      const double z_az = s[1];
+      const double ap_prap = s[2];
+      const double az_prap = s[3];
+      const double z_ap = s[4];
+      double delta;
+      double gamma;
+      if (i == 1) {
+        if (!FiniteNonZeroHost(az_praz)) break;
+        delta = z_az / az_praz;
+        gamma = 1.0;
+      } else {
+        const double gram[4] = {az_praz, az_prap, az_prap, ap_prap};
+        const double rhs[2] = {z_az, z_ap};
+        double coef[2];
+        SolveLeastSquares2x2(gram, rhs, coef);
+        delta = coef[0];
+        gamma = coef[1];
+      }
+      if (!std::isfinite(delta) || !std::isfinite(gamma)) break;
+      AddScaled(m_, z_, delta);
+      AddScaled(m_, p_, gamma);
+      UpdateResiduals(
+          [&] {
+            AddScaled(r_, az_, -delta);
+            AddScaled(r_, ap_, -gamma);
+          },
+          false);
+      const double ratio = delta != 0.0 ? gamma / delta : 0.0;
+      LinComb(z_, 1.0, p_, std::isfinite(ratio) ? ratio : 0.0);
+      DropForMatrixType(p_);
+      if (AppendIteration(p_)) break;
+      MulPr(r_, z_);
+    }
+  }
+
+  // ---- Inner-Outer (inner_outer_common.hpp:14-107) -------------------------
+  void RunInnerOuter(bool locally_optimal) {
+    if (AppendIteration(p_)) return;
+    double* normalization = ColVec(5);
+    const int grid = GridFor(n_, 128);
+    FillKernel<double><<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(normalization, n_, 1.0);
+    SPAI_LAUNCH_CHECK();
+    DevCsc<T> outer;
+    DevCsc<T> outer_csr;
+    for (int64_t iteration = 0; iteration < opt_.max_iterations;) {
+      Copy(ctx_, m_, outer);
+      Transpose(ctx_, outer, outer_csr);
+      Residual();
+      Empty(q_);
+      const int64_t inner_count = std::min(opt_.inner_iterations, opt_.max_iterations - iteration);
+      for (int64_t inner = 0; inner < inner_count; ++inner, ++iteration) {
+        Spgemm(ctx_, outer, outer_csr, r_, z_, opt_.dropping ? Epilogue::kPlain : Epilogue::kPruneZeros);
+        MulA(z_, az_);
+        if (locally_optimal) {
+          Spgemm(ctx_, A(), a_csr_, q_, ap_, Epilogue::kPlain);
+        }
+        double* r_az = ctx_.Partial(0, n_);
+        double* az_az = ctx_.Partial(1, n_);
+        double* az_aq = ctx_.Partial(2, n_);
+        double* aq_aq = ctx_.Partial(3, n_);
+        double* r_aq = ctx_.Partial(4, n_);
+        ColumnDots(ctx_, View(r_), View(az_), r_az);
+        ColumnSquares(ctx_, View(az_), az_az);
+        const bool first = !locally_optimal || inner == 0;
+        if (!first) {
+          ColumnDots(ctx_, View(az_), View(ap_), az_aq);
+          ColumnSquares(ctx_, View(ap_), aq_aq);
+          ColumnDots(ctx_, View(r_), View(ap_), r_aq);
+        }
+        double* delta = ColVec(0);
+        double* gamma = ColVec(1);
+        InnerOuterStepKernel<<<grid, 128, 0, ctx_.stream>>>(n_, r_az, az_az, az_aq, aq_aq, r_aq, locally_optimal,
+                                                            first, delta, gamma, normalization);
+        SPAI_LAUNCH_CHECK();
+        Copy(ctx_, z_, p_);
+        ScaleColumns(ctx_, p_, delta);
+        if (locally_optimal) {
+          ScaleColumns(ctx_, q_, gamma);
+          AddScaled(p_, q_, 1.0);
+        }
+        const bool dropped = DropForMatrixType(p_);
+        MulA(p_, ap_);
+        if (dropped) {
+          double* num = ctx_.Partial(0, n_);
+          double* den = ctx_.Partial(1, n_);
+          double* correction = ColVec(2);
+          ColumnDots(ctx_, View(r_), View(ap_), num);
+          ColumnSquares(ctx_, View(ap_), den);
+          SafeQuotientKernel<<<grid, 128, 0, ctx_.stream>>>(n_, num, den, correction);
+          SPAI_LAUNCH_CHECK();
+          ScaleColumns(ctx_, p_, correction);
+          ScaleColumns(ctx_, ap_, correction);
+        }
+        AddScaled(m_, p_, 1.0);
+        if (locally_optimal) {
+          Copy(ctx_, p_, q_);
+          ScaleColumns(ctx_, q_, normalization);
+        }
+        UpdateResiduals([&] { AddScaled(r_, ap_, -1.0); }, true);
+        if (AppendIteration(p_)) return;
+      }
+    }
+  }
+
+  double* ColVec(int i) {
+    ctx_.colvec[i].Reserve(static_cast<size_t>(n_), ctx_.stream);
+    return ctx_.colvec[i].data();
+  }
+
+  Ctx& ctx_;
+  SolveOptions opt_;
+  int64_t n_ = 0;
+  bool symmetric_ = true;
+  DevCsc<double> a64_;
+  DevCsc<T> a_;  // FP32 copy of A in mixed precision (unused in FP64)
+  DevCsc<T> a_csr_;
+  DevBuf<double> col_norm2_;
+  bool pr_diagonal_ = true;
+  DevBuf<T> pr_vec_;
+  DevCsc<T> pr_;
+  DevCsc<T> pr_csr_;
+  DevCsc<T> m0_;
+  DevCsc<T> m_, r_, z_, p_, ap_, az_, tmp_, q_;
+  std::vector<SingleIterationData> history_;
+  double initial_residual_ = 0.0;
+  int64_t iterations_ = 0;
+  bool converged_ = false;
+};
+
+}  // namespace
+
+std::unique_ptr<SolverBase> MakeSolver(Ctx& ctx, const SolveOptions& options) {
+  if (options.precision == 0) return std::unique_ptr<SolverBase>(new Solver<double>(ctx, options));
+  return std::unique_ptr<SolverBase>(new Solver<float>(ctx, options));
+}
+
+HostCsc CheckedMatrix(const MatrixData& data) {
+  // GetCompressedSparseMatrix (methods_c_api.cpp:16-40)
+  if (data.rows <= 0 || data.cols <= 0 || data.nnz <= 0) {
+    throw std::invalid_argument("Sparse matrix dimensions and nnz must be positive");
+  }
+  for (int64_t i = 0; i < data.cols; ++i) {
+    if (data.col_offsets[i] > data.col_offsets[i + 1]) {
+      throw std::invalid_argument("Sparse matrix column offsets must be non-decreasing");
+    }
+  }
+  for (int64_t i = 0; i < data.nnz; ++i) {
+    if (data.row_indices[i] < 0 || data.row_indices[i] >= data.rows) {
+      throw std::invalid_argument("Sparse matrix row idx is out of range");
+    }
+  }
+  if (data.rows > static_cast<int64_t>(std::numeric_limits<int32_t>::max()) ||
+      data.cols > static_cast<int64_t>(std::numeric_limits<int32_t>::max())) {
+    throw std::invalid_argument("Sparse matrix dimensions exceed the 32-bit row index range of the device layout");
+  }
+  HostCsc h;
+  h.rows = data.rows;
+  h.cols = data.cols;
+  h.nnz = data.nnz;
+  h.ptr = data.col_offsets;
+  h.idx = data.row_indices;
+  h.val = data.values;
+  return h;
+}
+
+void ValidateProblem(const HostCsc& a, const HostCsc* m0, const HostCsc* pr, const MethodParams& p) {
+  // methods_common.cpp:12-36
+  if (a.rows != a.cols || a.rows == 0) throw std::invalid_argument("A must be a non-empty square matrix");
+  if (m0 != nullptr && (m0->rows != a.rows || m0->cols != a.cols)) {
+    throw std::invalid_argument("Initial preconditioner M0 must have the same shape as A");
+  }
+  if (pr != nullptr && (pr->rows != a.rows || pr->cols != a.cols)) {
+    throw std::invalid_argument("Pr must have the same shape as A");
+  }
+  if (p.max_iterations <= 0) throw std::invalid_argument("max_iterations must be positive");
+  if (!std::isfinite(p.tolerance) || p.tolerance < 0.0) {
+    throw std::invalid_argument("tolerance must be finite and non-negative");
+  }
+  if (!std::isfinite(p.max_density) || p.max_density <= kMinDensity || p.max_density > 1.0) {
+    throw std::invalid_argument("max_density must be finite and in the interval (0, 1]");
+  }
+  const double entries = p.max_density * static_cast<double>(a.rows) * static_cast<double>(a.rows);
+  if (p.enable_dropping != 0 && entries < static_cast<double>(a.rows)) {
+    throw std::invalid_argument("max_density is too small to preserve the diagonal of M");
+  }
+  // methods_common.cpp:38-48
+  if (p.num_threads <= 0) throw std::invalid_argument("Invalid threads count value");
+}
+
+}  // namespace spai

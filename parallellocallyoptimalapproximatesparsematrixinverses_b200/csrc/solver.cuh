@@ -1,0 +1,94 @@
+#pragma once
+// Device solver for the five SPAI methods.  One Solver owns every matrix of
+// the iteration in HBM (A and its row-compressed copy, M, R, Z, P, AP, AZ,
+// Tmp, Q) and runs the reference's control flow with device kernels; the
+// host only reads back the global scalars each iteration needs for its
+// branch decisions (step lengths, convergence, sizes of new patterns).
+//
+// Global reductions use the device's canonical order: sequential inside a
+// column (as Eigen sums a column), then the fixed 4096-wide tree across
+// columns.  The CPU oracle reproduces that order bit for bit.
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/methods_c_api.h"
+#include "device.cuh"
+#include "ops.cuh"
+
+namespace spai {
+
+struct HostCsc {
+  int64_t rows = 0;
+  int64_t cols = 0;
+  int64_t nnz = 0;
+  const int64_t* ptr = nullptr;
+  const int64_t* idx = nullptr;
+  const double* val = nullptr;
+};
+
+enum class Method : int64_t {
+  kGlobalCg = 0,
+  kGlobalMr = 1,
+  kGlobalLomr = 2,
+  kInnerOuterMr = 3,
+  kInnerOuterLomr = 4,
+};
+
+struct SolveOptions {
+  Method method = Method::kGlobalMr;
+  int64_t max_iterations = 100;
+  double tolerance = 1e-9;
+  double max_density = 0.03;
+  bool dropping = true;
+  int64_t inner_iterations = 2;
+  int64_t topk = 0;       // 0: reference global budget; K > 0: per-column top-K by magnitude
+  int precision = 0;      // 0: FP64 storage, 1: FP32 storage with FP64 reductions
+};
+
+struct SolveOutput {
+  int64_t rows = 0;
+  int64_t cols = 0;
+  std::vector<int64_t> ptr;
+  std::vector<int64_t> idx;
+  std::vector<double> val;
+  std::vector<SingleIterationData> history;
+  int64_t iterations = 0;
+  bool converged = false;
+};
+
+struct IterationTimes {
+  double setup_ms = 0.0;
+  double iterate_ms = 0.0;
+};
+
+class SolverBase {
+ public:
+  virtual ~SolverBase() = default;
+  // Host-to-device upload and one-time setup (row-compressed A, column norms,
+  // preconditioner).  m0 / pr may be null (identity / diag(A)^-1).
+  virtual void Upload(const HostCsc& a, const HostCsc* m0, const HostCsc* pr) = 0;
+  // Runs the method from M0; may be called repeatedly.
+  virtual void Run() = 0;
+  // Copies M (as FP64, int64 indices) and the history to the host.
+  virtual void Download(SolveOutput& out) = 0;
+  virtual int64_t iterations() const = 0;
+  virtual int64_t m_nnz() const = 0;
+  // Device CSR copy of the current M (rows as major), values widened to FP64
+  // or kept in FP32 depending on want_fp32; used by the PCG evaluator.
+  virtual void ExportMForPcg(void* csr_out, bool want_fp32) = 0;
+  virtual const void* DeviceA() const = 0;  // DevCsc<double>* when precision == 0, else DevCsc<float>*
+  virtual const void* DeviceA64() const = 0;  // DevCsc<double>* (always)
+  virtual int64_t n() const = 0;
+};
+
+std::unique_ptr<SolverBase> MakeSolver(Ctx& ctx, const SolveOptions& options);
+
+// Validation shared by the C entry points (reference methods_c_api.cpp:16-40,
+// methods_common.cpp:12-48); throws std::invalid_argument with the reference's messages.
+HostCsc CheckedMatrix(const MatrixData& data);
+void ValidateProblem(const HostCsc& a, const HostCsc* m0, const HostCsc* pr, const MethodParams& p);
+
+}  // namespace spai

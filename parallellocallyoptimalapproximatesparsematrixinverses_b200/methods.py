@@ -1,0 +1,249 @@
+"""Python surface of the SPAI methods, mirroring the reference's
+methods_cython/methods.pyx (GlobalSpaiMethods / InnerOuterMethods,
+methods.pyx:182-258) on top of libspai_b200.so.
+
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import global_spai
+    result = global_spai.mr(A, M0=M0, Pr=Pr, max_iterations=20, max_density=10 / n)
+    result.M, result.iterations, result.converged, result.history
+
+Same arguments, defaults, conversions (scipy -> canonical int64 CSC, methods.pyx:74-98)
+and error behaviour (RuntimeError with the library's message, methods.pyx:128-130)
+as the reference.  Extra keyword arguments select the device-only forms:
+precision ("fp64" | "mixed"), topk_per_column (0 = the reference's global budget)
+and device (CUDA ordinal, -1 = current).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+from scipy import sparse
+
+from . import _lib
+
+HISTORY_DTYPE = np.dtype([
+    ("iteration", np.int64),
+    ("residual_norm", np.float64),
+    ("density_m", np.float64),
+    ("density_direction", np.float64),
+])
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
+
+
+class OutputResult:
+    """Reference methods_cython/methods.pyx:61-67."""
+
+    def __init__(self, M, iterations, converged, history):
+        self.M = M
+        self.iterations = iterations
+        self.converged = converged
+        self.history = history
+        self.residual_norms = history["residual_norm"]
+
+
+def _empty_csc():
+    return sparse.csc_matrix((0, 0), dtype=np.float64)
+
+
+def as_csc(matrix, shape=None):
+    """scipy matrix -> canonical CSC with int64 indices (methods.pyx:74-87)."""
+    if matrix is None:
+        return _empty_csc()
+    csc = sparse.csc_matrix(matrix, dtype=np.float64, copy=False)
+    if shape is not None and csc.shape != tuple(shape):
+        raise ValueError("matrix shape does not match A")
+    csc.sum_duplicates()
+    csc.sort_indices()
+    csc.indptr = np.ascontiguousarray(csc.indptr, dtype=np.int64)
+    csc.indices = np.ascontiguousarray(csc.indices, dtype=np.int64)
+    csc.data = np.ascontiguousarray(csc.data, dtype=np.float64)
+    return csc
+
+
+def matrix_data(csc) -> _lib.MatrixData:
+    """Borrowed pointers into a canonical CSC (methods.pyx:90-98)."""
+    return _lib.MatrixData(
+        csc.shape[0], csc.shape[1], csc.nnz,
+        csc.indptr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        csc.indices.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+        csc.data.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+    )
+
+
+def history_array(rows, count) -> np.ndarray:
+    history = np.empty(count, dtype=HISTORY_DTYPE)
+    for i in range(count):
+        h = rows[i]
+        history[i] = (h.iteration, h.residual_norm, h.density_m, h.density_direction)
+    return history
+
+
+def result_to_python(result: _lib.Result) -> OutputResult:
+    """Copies a Result into numpy/scipy and always frees it (methods.pyx:119-144)."""
+    lib = _lib.load()
+    try:
+        if result.error_message:
+            raise RuntimeError(result.error_message.decode("utf-8", "replace"))
+        indptr = np.ctypeslib.as_array(result.col_offsets, shape=(result.cols + 1,)).copy()
+        if result.nnz:
+            indices = np.ctypeslib.as_array(result.row_indices, shape=(result.nnz,)).copy()
+            values = np.ctypeslib.as_array(result.values, shape=(result.nnz,)).copy()
+        else:
+            indices = np.empty(0, dtype=np.int64)
+            values = np.empty(0, dtype=np.float64)
+        M = sparse.csc_matrix((values, indices, indptr), shape=(result.rows, result.cols))
+        history = history_array(result.history, result.history_size)
+        return OutputResult(M, result.iterations, bool(result.converged), history)
+    finally:
+        lib.free_mem(ctypes.byref(result))
+
+
+def method_params(A_csc, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
+                  inner_iterations) -> _lib.MethodParams:
+    return _lib.MethodParams(max_iterations, tolerance, max_density, 1 if enable_dropping else 0, num_threads,
+                             1 if M0 is not None else 0, 1 if Pr is not None else 0, inner_iterations)
+
+
+def ext_params(precision="fp64", topk_per_column=0, device=-1) -> _lib.SpaiExtParams:
+    if precision not in PRECISIONS:
+        raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
+    return _lib.SpaiExtParams(PRECISIONS[precision], int(topk_per_column), int(device), 0)
+
+
+def _call_method(family, name, A, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
+                 inner_iterations=2, precision="fp64", topk_per_column=0, device=-1) -> OutputResult:
+    """methods.pyx:147-179 plus the extension knobs."""
+    lib = _lib.load()
+    A_csc = as_csc(A)
+    M0_csc = as_csc(M0, A_csc.shape) if M0 is not None else _empty_csc()
+    Pr_csc = as_csc(Pr, A_csc.shape) if Pr is not None else _empty_csc()
+    params = method_params(A_csc, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
+                           inner_iterations)
+    method_id = _lib.METHOD_IDS[(family, name)]
+    if precision == "fp64" and not topk_per_column and device == -1:
+        # the reference's own entry points (methods_c_api.h:48-56)
+        entry = {0: lib.spai_global_cg, 1: lib.spai_global_mr, 2: lib.spai_global_lomr,
+                 3: lib.inner_outer_mr, 4: lib.inner_outer_lomr}[method_id]
+        result = entry(matrix_data(A_csc), matrix_data(M0_csc), matrix_data(Pr_csc), params)
+    else:
+        ext = ext_params(precision, topk_per_column, device)
+        result = lib.spai_run_ex(method_id, matrix_data(A_csc), matrix_data(M0_csc), matrix_data(Pr_csc), params,
+                                 ctypes.byref(ext))
+    return result_to_python(result)
+
+
+class GlobalSpaiMethods:
+    """Reference methods.pyx:182-222."""
+    available_methods = ("cg", "mr", "lomr")
+
+    def cg(self, A, M0=None, Pr=None, max_iterations=100, tolerance=1e-9, max_density=0.03, enable_dropping=True,
+           num_threads=1, **ext):
+        return _call_method("global_spai", "cg", A, M0, Pr, max_iterations, tolerance, max_density,
+                            enable_dropping, num_threads, **ext)
+
+    def mr(self, A, M0=None, Pr=None, max_iterations=100, tolerance=1e-9, max_density=0.03, enable_dropping=True,
+           num_threads=1, **ext):
+        return _call_method("global_spai", "mr", A, M0, Pr, max_iterations, tolerance, max_density,
+                            enable_dropping, num_threads, **ext)
+
+    def lomr(self, A, M0=None, Pr=None, max_iterations=100, tolerance=1e-9, max_density=0.03, enable_dropping=True,
+             num_threads=1, **ext):
+        return _call_method("global_spai", "lomr", A, M0, Pr, max_iterations, tolerance, max_density,
+                            enable_dropping, num_threads, **ext)
+
+
+class InnerOuterMethods:
+    """Reference methods.pyx:225-254."""
+    available_methods = ("mr", "lomr")
+
+    def mr(self, A, M0=None, Pr=None, max_iterations=100, tolerance=1e-9, max_density=0.03, enable_dropping=True,
+           num_threads=1, inner_iterations=2, **ext):
+        return _call_method("inner_outer", "mr", A, M0, Pr, max_iterations, tolerance, max_density,
+                            enable_dropping, num_threads, inner_iterations, **ext)
+
+    def lomr(self, A, M0=None, Pr=None, max_iterations=100, tolerance=1e-9, max_density=0.03, enable_dropping=True,
+             num_threads=1, inner_iterations=2, **ext):
+        return _call_method("inner_outer", "lomr", A, M0, Pr, max_iterations, tolerance, max_density,
+                            enable_dropping, num_threads, inner_iterations, **ext)
+
+
+global_spai = GlobalSpaiMethods()
+inner_outer = InnerOuterMethods()
+
+
+class Session:
+    """A problem resident in HBM (include/spai_b200.h sessions): repeated SPAI
+    runs and PCG solves without re-uploading A."""
+
+    def __init__(self, family, name, A, M0=None, Pr=None, max_iterations=100, tolerance=1e-9, max_density=0.03,
+                 enable_dropping=True, num_threads=1, inner_iterations=2, precision="fp64", topk_per_column=0,
+                 device=-1):
+        self._lib = _lib.load()
+        self._A = as_csc(A)
+        self._M0 = as_csc(M0, self._A.shape) if M0 is not None else _empty_csc()
+        self._Pr = as_csc(Pr, self._A.shape) if Pr is not None else _empty_csc()
+        params = method_params(self._A, M0, Pr, max_iterations, tolerance, max_density, enable_dropping,
+                               num_threads, inner_iterations)
+        ext = ext_params(precision, topk_per_column, device)
+        err = _lib.error_buffer()
+        handle = self._lib.spai_session_create(_lib.METHOD_IDS[(family, name)], matrix_data(self._A),
+                                               matrix_data(self._M0), matrix_data(self._Pr), params,
+                                               ctypes.byref(ext), err, len(err))
+        if not handle:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        self._handle = ctypes.c_void_p(handle)
+        self.n = self._A.shape[0]
+
+    def run(self):
+        it = ctypes.c_int64(0)
+        conv = ctypes.c_int64(0)
+        nnz = ctypes.c_int64(0)
+        err = _lib.error_buffer()
+        if self._lib.spai_session_run(self._handle, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(nnz), err,
+                                      len(err)) != 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        return it.value, nnz.value
+
+    def history(self):
+        cap = 1 << 16
+        rows = (_lib.SingleIterationData * cap)()
+        count = self._lib.spai_session_history(self._handle, rows, cap)
+        return history_array(rows, min(count, cap))
+
+    def result(self) -> OutputResult:
+        return result_to_python(self._lib.spai_session_result(self._handle))
+
+    def set_rhs(self, b):
+        self._b = np.ascontiguousarray(b, dtype=np.float64)
+        err = _lib.error_buffer()
+        if self._lib.spai_session_set_rhs(self._handle, self._b.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), err,
+                                          len(err)) != 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+
+    def pcg(self, max_iterations, tolerance, refresh_period=0, m_precision="fp64", return_x=False, device=-1):
+        params = _lib.PcgParams(max_iterations, tolerance, refresh_period, PRECISIONS[m_precision], device)
+        history = np.zeros(max_iterations, dtype=np.float64)
+        status = ctypes.c_int64(0)
+        x = np.zeros(self.n, dtype=np.float64) if return_x else None
+        err = _lib.error_buffer()
+        count = self._lib.spai_session_pcg(self._handle, params,
+                                           history.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                           ctypes.byref(status),
+                                           x.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if x is not None else None,
+                                           err, len(err))
+        if count < 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        out = (history[:count].copy(), int(status.value))
+        return out + (x,) if return_x else out
+
+    def close(self):
+        if getattr(self, "_handle", None):
+            self._lib.spai_session_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
