@@ -1,0 +1,491 @@
+#!/usr/bin/env python
+"""Benchmark: Global SPAI MR + PCG to 1e-8 on the 64^3 7-point log-normal
+diffusion operator, mixed precision vs FP64, on one B200 per rank.
+
+Workload (synthetic, seeded; no public data set is involved):
+  A      7-point variable-coefficient diffusion on a 64^3 grid, face
+         coefficients exp(N(0,1)) (numpy default_rng(0)), Dirichlet boundary:
+         n = 262,144, nnz = 1,810,432.
+  SPAI   Global MR (reference src/global_spai/minimal_residual.cpp), 30
+         iterations, M0 = diag(A)^-1, Pr = diag(A)^-1 (the reference default),
+         dropping on with at most 16 entries per column by magnitude.
+  PCG    b = A x*, x* ~ N(0,1) (default_rng(0)), x0 = 0, relative tolerance
+         1e-8, true-residual refresh every 50 iterations, preconditioned with
+         the symmetric part (M + M^T)/2 of the SPAI result (PCG needs a
+         symmetric preconditioner; MR iterates are not symmetric).
+  step   one SPAI build followed by one PCG solve.
+
+`value` is SPAI iterations per second of the mixed-precision step (FP32
+storage of M, R, Z, A; FP64 reductions; PCG in FP64 with FP32 M-apply), timed
+with CUDA events on the library's stream, inputs resident in HBM, L2 flushed
+before every step.  The same line carries the PCG time to 1e-8, the FP64 step
+for comparison, the end-to-end figure through the C ABI with host buffers,
+the roofline of the dominant kernel and the CPU baseline.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+if str(ROOT) not in sys.path:
+    sys.path.insert(0, str(ROOT))
+
+METRIC = "SPAI iters/s + PCG time to 1e-8, mixed vs FP64 on one B200, 64³ 7-pt"
+UNIT = "SPAI iters/s"
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    p.add_argument("--grid", type=int, default=64, help="grid edge of the 7-point operator (64 -> 64^3)")
+    p.add_argument("--spai-iterations", type=int, default=30)
+    p.add_argument("--topk", type=int, default=16)
+    p.add_argument("--pcg-tolerance", type=float, default=1e-8)
+    p.add_argument("--pcg-refresh", type=int, default=50)
+    p.add_argument("--pcg-max-iterations", type=int, default=5000)
+    p.add_argument("--skip-cpu-baseline", action="store_true")
+    p.add_argument("--skip-e2e", action="store_true")
+    return p.parse_args()
+
+
+def workload(args):
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import problems
+    A = problems.diffusion_3d(args.grid, 1.0, 0)
+    M0 = problems.diagonal_inverse(A)
+    b, _ = problems.solution_rhs(A, seed=0)
+    return A, M0, b
+
+
+def config_dict(args, A):
+    n = A.shape[0]
+    return {
+        "workload": f"Global SPAI MR ({args.spai_iterations} it, top-{args.topk}/column) + PCG to "
+                    f"{args.pcg_tolerance:g} on 7-pt log-normal diffusion {args.grid}^3",
+        "grid": args.grid, "n": n, "nnz": int(A.nnz),
+        "spai_method": "global_spai.mr", "spai_iterations": args.spai_iterations,
+        "dropping": f"top-{args.topk} per column by magnitude (diagonal kept)",
+        "m0": "diag(A)^-1", "pr": "diag(A)^-1",
+        "pcg_tolerance": args.pcg_tolerance, "pcg_refresh_period": args.pcg_refresh,
+        "pcg_preconditioner": "(M + M^T)/2 of the SPAI result",
+        "precision": "mixed: FP32 storage of A, M, R, Z; FP64 reductions; PCG FP64 with FP32 M-apply",
+        "l2": "flushed (256 MiB write) before every timed step",
+    }
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.device_index)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, sm_max, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                sm_max = max(sm_max, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": sm_max or None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def measured_peak_hbm():
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        data = json.loads(path.read_text())
+        return float(data["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel: str):
+    path = ROOT / "profiles" / "roofline_traffic.json"
+    try:
+        data = json.loads(path.read_text())
+        return data.get(kernel, {}).get("dram_bytes_per_launch")
+    except (OSError, ValueError):
+        return None
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    group = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        group = dist
+    return world, rank, local, group
+
+
+def barrier(group, device):
+    """All ranks meet here (an all-reduce of one element), device drained."""
+    if group is not None:
+        import torch
+        t = torch.zeros(1, device=device)
+        group.all_reduce(t)
+        if torch.device(device).type == "cuda":
+            torch.cuda.synchronize(device)
+
+
+def max_over_ranks(group, value, device):
+    if group is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    group.all_reduce(t, op=group.ReduceOp.MAX)
+    return float(t.item())
+
+
+def run_ours(args):
+    import torch
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import Session, _lib, backward_error, global_spai
+
+    world, rank, local, group = dist_setup(args)
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    lib = _lib.load()
+    A, M0, b = workload(args)
+    n = A.shape[0]
+    sessions = {}
+    for prec in ("mixed", "fp64"):
+        s = Session("global_spai", "mr", A, M0=M0, max_iterations=args.spai_iterations, tolerance=1e-12,
+                    max_density=float(args.topk) / n, precision=prec, topk_per_column=args.topk, device=local)
+        s.set_rhs(b)
+        sessions[prec] = s
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=device)  # 256 MiB > 126 MB L2
+
+    def one_step(prec, record):
+        s = sessions[prec]
+        stream = torch.cuda.ExternalStream(s.stream, device=device)
+        flush.zero_()
+        torch.cuda.synchronize(device)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e2 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        iterations, nnz_m = s.run()
+        e1.record(stream)
+        hist, status = s.pcg(args.pcg_max_iterations, args.pcg_tolerance, refresh_period=args.pcg_refresh,
+                             m_precision=prec, symmetric_part=True)
+        e2.record(stream)
+        e2.synchronize()
+        spai_ms = e0.elapsed_time(e1)
+        pcg_ms = e1.elapsed_time(e2)
+        if record is not None:
+            record.append({"spai_ms": spai_ms, "pcg_ms": pcg_ms, "iterations": iterations, "nnz_m": nnz_m,
+                           "pcg_iterations": len(hist) - 1, "pcg_status": status, "pcg_final": float(hist[-1])})
+
+    for _ in range(args.warmup):
+        one_step("mixed", None)
+        one_step("fp64", None)
+
+    results = {"mixed": [], "fp64": []}
+    launches0 = lib.spai_kernel_launches()
+    lib.spai_profile_reset()
+    lib.spai_profile_enable(1)
+    barrier(group, device)
+    torch.cuda.synchronize(device)
+    with ClockSampler(local) as clocks:
+        for _ in range(args.steps):
+            one_step("mixed", results["mixed"])
+        lib.spai_profile_enable(0)
+        for _ in range(args.steps):
+            one_step("fp64", results["fp64"])
+    torch.cuda.synchronize(device)
+    barrier(group, device)
+    launches = lib.spai_kernel_launches() - launches0
+
+    def agg(rows):
+        spai = sum(r["spai_ms"] for r in rows)
+        pcg = sum(r["pcg_ms"] for r in rows)
+        its = sum(r["iterations"] for r in rows)
+        return spai, pcg, its
+
+    spai_ms, pcg_ms, its = agg(results["mixed"])
+    spai_ms_max = max_over_ranks(group, spai_ms, device)
+    step_ms_max = max_over_ranks(group, spai_ms + pcg_ms, device)
+    f_spai, f_pcg, f_its = agg(results["fp64"])
+    f_spai = max_over_ranks(group, f_spai, device)
+    f_step = max_over_ranks(group, f_spai + f_pcg, device)
+
+    # dominant kernel: the SpGEMM numeric pass (residual R = I - A M and the fused MR projection)
+    import ctypes
+    ms = ctypes.c_double(0.0)
+    cnt = ctypes.c_int64(0)
+    byt = ctypes.c_double(0.0)
+    lib.spai_profile_read(b"spgemm_numeric", ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(byt))
+    peak, peak_kind = measured_peak_hbm()
+    kernel_table = {}
+    for name in (b"spgemm_numeric", b"spgemm_symbolic", b"union", b"transpose", b"filter", b"pcg_spmv"):
+        m2, c2, b2 = ctypes.c_double(0.0), ctypes.c_int64(0), ctypes.c_double(0.0)
+        lib.spai_profile_read(name, ctypes.byref(m2), ctypes.byref(c2), ctypes.byref(b2))
+        kernel_table[name.decode()] = {"ms": round(m2.value, 3), "launches": c2.value,
+                                       "gbs": round(b2.value / (m2.value * 1e6), 1) if m2.value > 0 and b2.value > 0 else None}
+    achieved = (byt.value / cnt.value) / ((ms.value / cnt.value) * 1e-3) / 1e9 if cnt.value else 0.0
+    traffic = ncu_traffic("spgemm_numeric")
+
+    line = None
+    if rank == 0:
+        rows = results["mixed"]
+        line = {
+            "metric": METRIC,
+            "value": round(world * its / (spai_ms_max * 1e-3), 3),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(step_ms_max / args.steps, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32-storage/f64-reductions",
+            "data": "synthetic (seeded 64^3 log-normal diffusion operator; no public data set)",
+            "config": config_dict(args, A),
+            "spai_ms_per_build": round(spai_ms_max / args.steps, 3),
+            "pcg_ms_to_tolerance": round((step_ms_max - spai_ms_max) / args.steps, 3),
+            "pcg_iterations": rows[-1]["pcg_iterations"],
+            "pcg_status": rows[-1]["pcg_status"],
+            "pcg_final_relative_residual": rows[-1]["pcg_final"],
+            "nnz_m": rows[-1]["nnz_m"],
+            "fp64": {
+                "spai_iters_per_s": round(world * f_its / (f_spai * 1e-3), 3),
+                "spai_ms_per_build": round(f_spai / args.steps, 3),
+                "pcg_ms_to_tolerance": round((f_step - f_spai) / args.steps, 3),
+                "pcg_iterations": results["fp64"][-1]["pcg_iterations"],
+                "ms_per_step": round(f_step / args.steps, 3),
+            },
+            "speedup_mixed_vs_fp64": round(f_step / step_ms_max, 3),
+            "roofline": {
+                "kernel": "spgemm_numeric (NumericKernel: R = I - A*M and the fused MR projection)",
+                "bound": "hbm",
+                "achieved": round(achieved, 1),
+                "peak": peak,
+                "unit": "GB/s",
+                "frac": round(achieved / peak, 4) if peak else None,
+                "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "traffic": traffic,
+                "launches": cnt.value,
+                "ms_per_launch": round(ms.value / cnt.value, 4) if cnt.value else None,
+                "algorithmic_bytes_per_launch": round(byt.value / cnt.value) if cnt.value else None,
+            },
+            "kernel_classes_mixed": kernel_table,
+            "clocks": clocks.summary(),
+            "gpu_launches": launches,
+        }
+    for s in sessions.values():
+        s.close()
+
+    if rank == 0 and world == 1:
+        if not args.skip_e2e:
+            line["e2e"] = e2e(args, A, M0, b)
+        if not args.skip_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(args, A, M0, b)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if group is not None:
+        group.destroy_process_group()
+
+
+def e2e(args, A, M0, b):
+    """The same step through the public API with host buffers (pinned), copies included."""
+    import torch
+    from scipy import sparse
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import backward_error, global_spai
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200.methods import as_csc
+
+    def pinned(arr):
+        t = torch.empty(arr.shape, dtype=getattr(torch, str(arr.dtype)), pin_memory=True)
+        out = t.numpy()
+        out[...] = arr
+        return out, t
+
+    keep = []
+    A_csc = as_csc(A)
+    M0_csc = as_csc(M0)
+    for m in (A_csc, M0_csc):
+        for attr in ("indptr", "indices", "data"):
+            arr, t = pinned(getattr(m, attr))
+            keep.append(t)
+            setattr(m, attr, arr)
+    A_csr = sparse.csr_matrix(A)
+    A_csr.sort_indices()
+    a_arrays = []
+    for arr in (A_csr.data.astype(np.float64), A_csr.indices.astype(np.int64), A_csr.indptr.astype(np.int64)):
+        p, t = pinned(arr)
+        keep.append(t)
+        a_arrays.append(p)
+    b_pinned, t = pinned(np.ascontiguousarray(b))
+    keep.append(t)
+    n = A.shape[0]
+    times_spai, times_pcg = [], []
+    h2d = d2h = 0
+    for rep in range(max(1, min(args.steps, 3)) + 1):
+        t0 = time.perf_counter()
+        r = global_spai.mr(A_csc, M0=M0_csc, max_iterations=args.spai_iterations, tolerance=1e-12,
+                           max_density=float(args.topk) / n, precision="mixed", topk_per_column=args.topk)
+        t1 = time.perf_counter()
+        M_csr = sparse.csr_matrix(r.M)
+        hist, status = backward_error.pcg(a_arrays[0], a_arrays[1], a_arrays[2], M_csr.data, M_csr.indices,
+                                          M_csr.indptr, b_pinned, args.pcg_max_iterations, 1, args.pcg_tolerance,
+                                          refresh_period=args.pcg_refresh, m_precision="mixed", symmetric_part=True)
+        t2 = time.perf_counter()
+        if rep == 0:
+            continue  # first call pays context creation
+        times_spai.append(t1 - t0)
+        times_pcg.append(t2 - t1)
+        h2d = (A_csc.indptr.nbytes + A_csc.indices.nbytes + A_csc.data.nbytes + M0_csc.indptr.nbytes
+               + M0_csc.indices.nbytes + M0_csc.data.nbytes + sum(x.nbytes for x in a_arrays)
+               + M_csr.data.nbytes + M_csr.indices.nbytes + M_csr.indptr.nbytes + b_pinned.nbytes)
+        d2h = (r.M.indptr.nbytes + r.M.indices.nbytes + r.M.data.nbytes + r.history.nbytes
+               + 8 * args.pcg_max_iterations)
+    spai_s = statistics.median(times_spai)
+    pcg_s = statistics.median(times_pcg)
+    return {"value": round(args.spai_iterations / spai_s, 3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h), "spai_ms_per_build": round(spai_s * 1e3, 3),
+            "pcg_ms_to_tolerance": round(pcg_s * 1e3, 3), "ms_per_step": round((spai_s + pcg_s) * 1e3, 3),
+            "timing": "time.perf_counter around global_spai.mr and backward_error.pcg (host buffers, synchronous)",
+            "api": "global_spai.mr(..., precision='mixed', topk_per_column=K) -> spai_run_ex; "
+                   "backward_error.pcg(..., symmetric_part=True) -> spai_pcg"}
+
+
+def cpu_baseline(args, A, M0, b, threads=None):
+    """CPU oracle SPAI (the FP64 restatement, OpenMP over column batches) on a
+    bounded sample, plus the reference's own compiled PCG (oracle/_ref) to 1e-8."""
+    from scipy import sparse
+    from oracle import pyoracle
+    threads = threads or os.cpu_count() or 1
+    n = A.shape[0]
+    sample = 3
+    t_start = time.perf_counter()
+    r1 = pyoracle.run("global_spai", "mr", A, M0=M0, max_iterations=1, tolerance=1e-12,
+                      max_density=float(args.topk) / n, num_threads=threads, omp_threads=threads,
+                      topk_per_column=args.topk, order=pyoracle.ORDER_REFERENCE)
+    t1 = time.perf_counter()
+    r3 = pyoracle.run("global_spai", "mr", A, M0=M0, max_iterations=sample, tolerance=1e-12,
+                      max_density=float(args.topk) / n, num_threads=threads, omp_threads=threads,
+                      topk_per_column=args.topk, order=pyoracle.ORDER_REFERENCE)
+    t3 = time.perf_counter()
+    per_iteration = ((t3 - t1) - (t1 - t_start)) / (sample - 1)
+    its_per_s = 1.0 / per_iteration if per_iteration > 0 else None
+    # PCG: the reference's compiled backward_error.pcg when present, else the oracle port
+    M = r3.M
+    msym = sparse.csr_matrix((M + M.T) * 0.5)
+    msym.sort_indices()
+    A_csr = sparse.csr_matrix(A)
+    A_csr.sort_indices()
+    ref = pyoracle.reference_pcg_module()
+    t0 = time.perf_counter()
+    if ref is not None:
+        hist, status = ref.pcg(A_csr.data, A_csr.indices.astype(np.int64), A_csr.indptr.astype(np.int64),
+                               msym.data, msym.indices.astype(np.int64), msym.indptr.astype(np.int64), b,
+                               args.pcg_max_iterations, threads, args.pcg_tolerance)
+        pcg_kind = "reference (methods_cython/backward_error.pyx compiled from the reference source)"
+    else:
+        hist, status = pyoracle.pcg(A_csr, msym, b, args.pcg_max_iterations, args.pcg_tolerance)
+        pcg_kind = "port"
+    pcg_s = time.perf_counter() - t0
+    return {"value": round(its_per_s, 4) if its_per_s else None, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{sample} Global MR iterations minus 1 (setup excluded) on the same 64^3 operator, "
+                      f"FP64 CPU oracle, {threads} OpenMP threads over {threads} column batches",
+            "pcg_ms_to_tolerance": round(pcg_s * 1e3, 3), "pcg_iterations": len(hist) - 1, "pcg_status": int(status),
+            "pcg_kind": pcg_kind,
+            "pcg_note": f"preconditioner = (M+M^T)/2 of the CPU {sample}-iteration M"}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU implementation of the path (the
+    oracle port for SPAI, the reference's compiled PCG) on the host cores."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    A, M0, b = workload(args)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        pass  # the CPU path has no warm-up state; each step is a fresh bounded sample
+    rows = []
+    for _ in range(args.steps):
+        rows.append(cpu_baseline(args, A, M0, b, threads))
+    value = statistics.median(r["value"] for r in rows)
+    pcg_ms = statistics.median(r["pcg_ms_to_tolerance"] for r in rows)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(1e3 * args.spai_iterations / value + pcg_ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded 64^3 log-normal diffusion operator; no public data set)",
+        "config": config_dict(args, A), "impl": "reference",
+        "pcg_ms_to_tolerance": pcg_ms,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": rows[0]["sample"], "pcg_kind": rows[0]["pcg_kind"]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -90,6 +90,8 @@ typedef struct PcgParams {
   int64_t refresh_period; /* 0: the reference's refresh at convergence only; K > 0: also r = b - A x every K steps */
   int64_t m_precision;    /* 0: M applied in FP64; 1: M stored in FP32, vectors and dots in FP64 */
   int64_t device;         /* CUDA device ordinal; -1: current device */
+  int64_t symmetric_part; /* 0: precondition with M as given (the reference); 1: with (M + M^T)/2, formed on the
+                             device (PCG assumes a symmetric preconditioner; SPAI iterates are not symmetric) */
 } PcgParams;
 
 /* PCG with x0 = 0 on CSR A and CSR M (int64 indices), the device form of the
@@ -133,8 +135,20 @@ int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history
                          char* error, int64_t error_capacity);
 void spai_session_destroy(SpaiSession* session);
 
+/* The CUDA stream (cudaStream_t) every kernel of the session runs on, for
+ * callers that time the session with their own CUDA events. */
+void* spai_session_stream(SpaiSession* session);
+
 /* Number of kernels this library has launched since load (diagnostics). */
 int64_t spai_kernel_launches(void);
+
+/* Opt-in per-kernel-class accounting with CUDA events: enable (1) / disable (0),
+ * reset, and read the totals of one class ("spgemm_numeric", "spgemm_symbolic",
+ * "union", "transpose", "filter", "pcg_spmv"): elapsed ms, launches and the
+ * algorithmic bytes those launches must move.  Returns 1 if the class was seen. */
+void spai_profile_enable(int64_t on);
+void spai_profile_reset(void);
+int64_t spai_profile_read(const char* name, double* ms, int64_t* launches, double* bytes);
 
 #ifdef __cplusplus
 }

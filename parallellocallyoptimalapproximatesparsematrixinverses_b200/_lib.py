@@ -55,7 +55,7 @@ class SpaiExtParams(ctypes.Structure):
 class PcgParams(ctypes.Structure):
     """include/spai_b200.h PcgParams."""
     _fields_ = [("max_iterations", _i64), ("tolerance", _f64), ("refresh_period", _i64),
-                ("m_precision", _i64), ("device", _i64)]
+                ("m_precision", _i64), ("device", _i64), ("symmetric_part", _i64)]
 
 
 METHOD_IDS = {
@@ -80,7 +80,8 @@ EXPORTED_SYMBOLS = (
     "spai_global_cg", "spai_global_mr", "spai_global_lomr", "inner_outer_mr", "inner_outer_lomr", "free_mem",
     "spai_run_ex", "spai_pcg", "spai_matvec", "spai_session_create", "spai_session_run", "spai_session_history",
     "spai_session_result", "spai_session_set_rhs", "spai_session_pcg", "spai_session_destroy",
-    "spai_kernel_launches",
+    "spai_kernel_launches", "spai_session_stream", "spai_profile_enable", "spai_profile_reset",
+    "spai_profile_read",
 )
 
 _lib = None
@@ -119,6 +120,14 @@ def _declare(lib) -> None:
     lib.spai_session_destroy.argtypes = [ctypes.c_void_p]
     lib.spai_kernel_launches.restype = _i64
     lib.spai_kernel_launches.argtypes = []
+    lib.spai_session_stream.restype = ctypes.c_void_p
+    lib.spai_session_stream.argtypes = [ctypes.c_void_p]
+    lib.spai_profile_enable.restype = None
+    lib.spai_profile_enable.argtypes = [_i64]
+    lib.spai_profile_reset.restype = None
+    lib.spai_profile_reset.argtypes = []
+    lib.spai_profile_read.restype = _i64
+    lib.spai_profile_read.argtypes = [ctypes.c_char_p, _pf64, _pi64, _pf64]
 
 
 def load():

@@ -55,7 +55,7 @@ def matvec(values, indices, offsets, x, threads, device=-1):
 
 
 def pcg(a_values, a_indices, a_offsets, m_values, m_indices, m_offsets, b, max_iterations, threads, tolerance,
-        refresh_period=0, m_precision="fp64", device=-1, return_x=False):
+        refresh_period=0, m_precision="fp64", device=-1, return_x=False, symmetric_part=False):
     """PCG with x0 = 0 (backward_error.pyx:69-144); returns (history, status)."""
     b = _f64(b)
     n = b.shape[0]
@@ -64,7 +64,7 @@ def pcg(a_values, a_indices, a_offsets, m_values, m_indices, m_offsets, b, max_i
     av, ai, ao = _f64(a_values), _i64(a_indices), _i64(a_offsets)
     mv, mi, mo = _f64(m_values), _i64(m_indices), _i64(m_offsets)
     params = _lib.PcgParams(int(max_iterations), float(tolerance), int(refresh_period), M_PRECISIONS[m_precision],
-                            int(device))
+                            int(device), 1 if symmetric_part else 0)
     history = np.zeros(int(max_iterations), dtype=np.float64)
     status = ctypes.c_int64(0)
     x = np.zeros(n, dtype=np.float64) if return_x else None

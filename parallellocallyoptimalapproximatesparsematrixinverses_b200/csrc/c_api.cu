@@ -18,6 +18,7 @@
 #include "device.cuh"
 #include "ops.cuh"
 #include "pcg.cuh"
+#include "profile.cuh"
 #include "solver.cuh"
 
 namespace spai {
@@ -184,7 +185,16 @@ void UploadCsr(Ctx& ctx, int64_t n, const double* values, const int64_t* indices
   ctx.Sync();
 }
 
+// (M + M^T) / 2 of a row- or column-compressed M, in place.
+template <class T>
+void SymmetricPart(Ctx& ctx, DevCsc<T>& m) {
+  DevCsc<T> mt;
+  Transpose(ctx, m, mt);
+  Union(ctx, m, false, 1.0, mt, 1.0, m, UnionMode::kHalfSum);
+}
+
 void CheckPcgParams(int64_t n, const PcgParams& p) {
+  if (p.symmetric_part != 0 && p.symmetric_part != 1) throw std::invalid_argument("symmetric_part must be 0 or 1");
   if (n <= 0 || p.max_iterations <= 0) throw std::invalid_argument("n, max_iterations and threads must be positive");
   if (!(p.tolerance >= 0.0)) throw std::invalid_argument("tolerance must be non-negative");
   if (p.m_precision != 0 && p.m_precision != 1) throw std::invalid_argument("m_precision must be 0 or 1");
@@ -290,10 +300,12 @@ int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, co
     if (params.m_precision == 1) {
       spai::DevCsc<float> m;
       spai::UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
+      if (params.symmetric_part) spai::SymmetricPart(ctx, m);
       spai::RunPcg(ctx, a, m, bd.data(), xd.data(), opt, result);
     } else {
       spai::DevCsc<double> m;
       spai::UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
+      if (params.symmetric_part) spai::SymmetricPart(ctx, m);
       spai::RunPcg(ctx, a, m, bd.data(), xd.data(), opt, result);
     }
     if (x_out != nullptr) {
@@ -427,9 +439,11 @@ int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history
     spai::PcgResult result;
     if (params.m_precision == 1) {
       session->solver->ExportMForPcg(&session->m32, true);
+      if (params.symmetric_part) spai::SymmetricPart(session->ctx, session->m32);
       spai::RunPcg(session->ctx, session->a_rows, session->m32, session->b.data(), session->x.data(), opt, result);
     } else {
       session->solver->ExportMForPcg(&session->m64, false);
+      if (params.symmetric_part) spai::SymmetricPart(session->ctx, session->m64);
       spai::RunPcg(session->ctx, session->a_rows, session->m64, session->b.data(), session->x.data(), opt, result);
     }
     if (x_out != nullptr) {
@@ -445,6 +459,25 @@ int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history
 }
 
 void spai_session_destroy(SpaiSession* session) { delete session; }
+
+void* spai_session_stream(SpaiSession* session) {
+  return session != nullptr ? static_cast<void*>(session->ctx.stream) : nullptr;
+}
+
+void spai_profile_enable(int64_t on) { spai::prof::SetEnabled(on != 0); }
+
+void spai_profile_reset(void) { spai::prof::Reset(); }
+
+int64_t spai_profile_read(const char* name, double* ms, int64_t* launches, double* bytes) {
+  double t = 0.0;
+  double b = 0.0;
+  int64_t c = 0;
+  const bool seen = spai::prof::Read(name != nullptr ? name : "", &t, &c, &b);
+  if (ms != nullptr) *ms = t;
+  if (launches != nullptr) *launches = c;
+  if (bytes != nullptr) *bytes = b;
+  return seen ? 1 : 0;
+}
 
 int64_t spai_kernel_launches(void) { return spai::g_launches.load(); }
 

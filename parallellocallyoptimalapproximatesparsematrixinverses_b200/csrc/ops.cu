@@ -12,6 +12,7 @@
 
 #include "device.cuh"
 #include "ops.cuh"
+#include "profile.cuh"
 
 namespace spai {
 
@@ -459,6 +460,7 @@ __global__ void FilterWriteKernel(CscView<T> x, Pred pred, const int64_t* __rest
 template <class T, class Pred>
 void RunFilter(Ctx& ctx, DevCsc<T>& x, const Pred& pred) {
   const int64_t cols = x.cols;
+  prof::Scope scope(ctx.stream, "filter", 0.0);
   ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
   const int threads = 256;
   const int grid = GridFor(cols * kWarp, threads);
@@ -907,6 +909,7 @@ void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T
   const int64_t cols = y.cols;
   ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
   const int grid = GridFor(cols, 128);
+  prof::Scope scope(ctx.stream, "union", 0.0);
   UnionKernel<T, false><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode),
                                                       ctx.counts.data(), nullptr, nullptr, nullptr);
   SPAI_LAUNCH_CHECK();
@@ -1011,6 +1014,7 @@ void GlobalDropByScore(Ctx& ctx, DevCsc<T>& x, const double* entry_scores, bool 
 
 template <class T>
 void Transpose(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& t) {
+  prof::Scope scope(ctx.stream, "transpose", 0.0);
   DevCsc<T> result;
   result.Shape(x.cols, x.rows, ctx.stream);
   ctx.counts.Reserve(static_cast<size_t>(x.rows + 1), ctx.stream);

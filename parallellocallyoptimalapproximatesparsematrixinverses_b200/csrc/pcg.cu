@@ -11,6 +11,7 @@
 #include "device.cuh"
 #include "ops.cuh"
 #include "pcg.cuh"
+#include "profile.cuh"
 
 namespace spai {
 
@@ -69,6 +70,10 @@ double DotProduct(Ctx& ctx, const double* x, const double* y, int64_t n) {
 
 template <class TM>
 void Spmv(Ctx& ctx, const DevCsc<TM>& a_rows, const double* x, double* y) {
+  // algorithmic bytes: the matrix once, x once, y written once
+  const double bytes = static_cast<double>(a_rows.nnz) * (sizeof(TM) + sizeof(int32_t)) +
+                       static_cast<double>(a_rows.cols + 1) * sizeof(int64_t) + 16.0 * static_cast<double>(a_rows.cols);
+  prof::Scope scope(ctx.stream, "pcg_spmv", bytes);
   SpmvKernel<TM><<<GridFor(a_rows.cols, 128), 128, 0, ctx.stream>>>(View(a_rows), x, y);
   SPAI_LAUNCH_CHECK();
 }

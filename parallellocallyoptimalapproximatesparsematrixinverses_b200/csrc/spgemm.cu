@@ -19,6 +19,7 @@
 
 #include "device.cuh"
 #include "ops.cuh"
+#include "profile.cuh"
 #include "spgemm.cuh"
 
 namespace spai {
@@ -451,6 +452,16 @@ __global__ void MaskedKernel(MaskedArgs<T> a, int slots, int64_t lo_need, int64_
   }
 }
 
+// One atomicMax per warp instead of one per thread.
+__device__ __forceinline__ void WarpAtomicMax(unsigned long long* target, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, v, o);
+    v = other > v ? other : v;
+  }
+  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicMax(target, v);
+}
+
 // upper bound on distinct rows and the B column length, plus the maxima.
 template <class T>
 __global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ ub,
@@ -468,8 +479,8 @@ __global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* _
     local_ub = max(local_ub, static_cast<unsigned long long>(u));
     local_nb = max(local_nb, static_cast<unsigned long long>(b.ptr[j + 1] - b.ptr[j]));
   }
-  atomicMax(&maxima[0], local_ub);
-  atomicMax(&maxima[1], local_nb);
+  WarpAtomicMax(&maxima[0], local_ub);
+  WarpAtomicMax(&maxima[1], local_nb);
 }
 
 // symbolic need = 2 * ub; numeric need = max(2 * count, 4 * nb)
@@ -492,7 +503,7 @@ __global__ void NumericNeedKernel(const int64_t* __restrict__ counts, const int6
     need[j] = v;
     local = max(local, static_cast<unsigned long long>(v));
   }
-  atomicMax(&maxima[2], local);
+  WarpAtomicMax(&maxima[2], local);
 }
 
 __global__ void MaskedNeedKernel(const int64_t* __restrict__ bptr, int64_t cols, int64_t* __restrict__ need) {
@@ -568,6 +579,12 @@ void LaunchBins(Ctx& ctx, Kernel kernel, Args args, int64_t cols, int64_t max_ne
   }
 }
 
+template <class T>
+double MatrixBytes(int64_t nnz, int64_t major) {
+  return static_cast<double>(nnz) * static_cast<double>(sizeof(T) + sizeof(int32_t)) +
+         static_cast<double>(major + 1) * static_cast<double>(sizeof(int64_t));
+}
+
 }  // namespace
 
 template <class T>
@@ -597,7 +614,10 @@ void Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   const int64_t max_sym_need = 2 * static_cast<int64_t>(host_max[0]);
 
   SymbolicArgs<T> sargs{View(x_csc), View(b), need.data(), residual, counts.data(), nullptr};
-  LaunchBins(ctx, SymbolicKernel<T>, sargs, cols, max_sym_need, false, sizeof(T), fallback);
+  {
+    prof::Scope scope(ctx.stream, "spgemm_symbolic", 0.0);
+    LaunchBins(ctx, SymbolicKernel<T>, sargs, cols, max_sym_need, false, sizeof(T), fallback);
+  }
 
   NumericNeedKernel<<<GridFor(cols, 256), 256, 0, ctx.stream>>>(counts.data(), b.ptr.data(), cols, need.data(),
                                                                 maxima.data());
@@ -636,7 +656,18 @@ void Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   SPAI_CUDA(cudaMemcpyAsync(host_max, maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
   ctx.Sync();
   const int64_t max_num_need = static_cast<int64_t>(host_max[2]);
-  LaunchBins(ctx, NumericKernel<T>, nargs, cols, max_num_need, true, sizeof(T), fallback);
+  {
+    // algorithmic bytes: |X| + |B| + |C| (C written; the projection writes two per-column sums instead)
+    double bytes = MatrixBytes<T>(x_csr.nnz, x_csr.cols) + MatrixBytes<T>(b.nnz, b.cols);
+    if (projection) {
+      bytes += static_cast<double>(cols) * (sizeof(T) + 2 * sizeof(double));
+    } else {
+      bytes += MatrixBytes<T>(nnz, cols);
+      if (nargs.z_val != nullptr) bytes += static_cast<double>(nnz) * sizeof(T);
+    }
+    prof::Scope scope(ctx.stream, "spgemm_numeric", bytes);
+    LaunchBins(ctx, NumericKernel<T>, nargs, cols, max_num_need, true, sizeof(T), fallback);
+  }
   if (projection) {
     return;
   }

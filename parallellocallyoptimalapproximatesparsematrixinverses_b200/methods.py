@@ -221,8 +221,10 @@ class Session:
                                           len(err)) != 0:
             raise RuntimeError(err.value.decode("utf-8", "replace"))
 
-    def pcg(self, max_iterations, tolerance, refresh_period=0, m_precision="fp64", return_x=False, device=-1):
-        params = _lib.PcgParams(max_iterations, tolerance, refresh_period, PRECISIONS[m_precision], device)
+    def pcg(self, max_iterations, tolerance, refresh_period=0, m_precision="fp64", return_x=False, device=-1,
+            symmetric_part=False):
+        params = _lib.PcgParams(max_iterations, tolerance, refresh_period, PRECISIONS[m_precision], device,
+                                1 if symmetric_part else 0)
         history = np.zeros(max_iterations, dtype=np.float64)
         status = ctypes.c_int64(0)
         x = np.zeros(self.n, dtype=np.float64) if return_x else None
@@ -236,6 +238,11 @@ class Session:
             raise RuntimeError(err.value.decode("utf-8", "replace"))
         out = (history[:count].copy(), int(status.value))
         return out + (x,) if return_x else out
+
+    @property
+    def stream(self) -> int:
+        """cudaStream_t of the session (for CUDA events recorded by the caller)."""
+        return int(self._lib.spai_session_stream(self._handle) or 0)
 
     def close(self):
         if getattr(self, "_handle", None):

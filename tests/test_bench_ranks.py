@@ -1,0 +1,37 @@
+"""bench.py's multi-rank plumbing (barrier, max over ranks) on 2 gloo ranks."""
+import os
+import socket
+
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, out):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import bench
+    bench.barrier(dist, "cpu")
+    value = bench.max_over_ranks(dist, 10.0 * (rank + 1), "cpu")
+    out[rank] = value
+    dist.destroy_process_group()
+
+
+def test_max_over_two_gloo_ranks():
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, out)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert out[0] == out[1] == 20.0
