@@ -204,13 +204,16 @@ __device__ __forceinline__ double UnionRight(double x, double xs, int mode) {
   return Add(0.0, Mul(xs, x));
 }
 
+// One thread per column: used for columns whose X part is longer than the
+// warp kernels' cap (min_nx); prunes exact zeros inline.
 template <class T, bool kWrite>
-__global__ void UnionKernel(CscView<T> y, CscView<T> x, bool scale_y, double ys, double xs, int mode,
+__global__ void UnionKernel(CscView<T> y, CscView<T> x, bool scale_y, double ys, double xs, int mode, int64_t min_nx,
                             int64_t* __restrict__ counts, const int64_t* __restrict__ out_ptr,
                             int32_t* __restrict__ out_idx, T* __restrict__ out_val) {
   const bool prune = mode == static_cast<int>(UnionMode::kAxpby);
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < y.cols;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    if (x.ptr[j + 1] - x.ptr[j] <= min_nx) continue;
     int64_t p = y.ptr[j];
     int64_t q = x.ptr[j];
     const int64_t pe = y.ptr[j + 1];
@@ -812,6 +815,16 @@ void Ctx::Destroy() {
   select_state.Release();
   histogram.Release();
   flags.Release();
+  sg_need.Release();
+  sg_counts.Release();
+  sg_proj_ptr.Release();
+  sg_win_lo.Release();
+  sg_win_words.Release();
+  sg_cols.Release();
+  sg_proj_rows.Release();
+  sg_proj_vals.Release();
+  sg_fallback.Release();
+  sg_maxima.Release();
   if (stream != nullptr) {
     cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
@@ -909,17 +922,28 @@ void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T
   const int64_t cols = y.cols;
   ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
   const int grid = GridFor(cols, 128);
+  const int64_t cap = UnionWarpCap();
+  const bool half_sum = mode == UnionMode::kHalfSum;
   prof::Scope scope(ctx.stream, "union", 0.0);
-  UnionKernel<T, false><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode),
+  UnionCountWarp(ctx, y, x, ctx.counts.data());
+  UnionKernel<T, false><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode), cap,
                                                       ctx.counts.data(), nullptr, nullptr, nullptr);
   SPAI_LAUNCH_CHECK();
   DevCsc<T> result;
   result.Shape(y.rows, cols, ctx.stream);
   const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, result.ptr.data());
   result.ReserveNnz(nnz, ctx.stream);
-  UnionKernel<T, true><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode),
+  SPAI_CUDA(cudaMemsetAsync(ctx.flags.data(), 0, sizeof(int32_t), ctx.stream));
+  UnionWriteWarp(ctx, y, x, scale_y, ys, xs, half_sum, !half_sum, result, ctx.flags.data());
+  UnionKernel<T, true><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode), cap,
                                                      nullptr, result.ptr.data(), result.idx.data(), result.val.data());
   SPAI_LAUNCH_CHECK();
+  if (!half_sum) {
+    // exact zeros from y + a*x (rare): remove them like Eigen's prune(0.0)
+    SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags, ctx.flags.data(), sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.Sync();
+    if (ctx.host_flags[0] != 0) DropZeros(ctx, result);
+  }
   out.Swap(result);
 }
 

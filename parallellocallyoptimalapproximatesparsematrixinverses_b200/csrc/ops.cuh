@@ -28,6 +28,17 @@ struct Ctx {
   DevBuf<unsigned long long> select_state;  // radix-select state
   DevBuf<unsigned long long> histogram;     // radix-select histogram
   DevBuf<int32_t> flags;        // device flags (zero pruning happened, overflow)
+  // SpGEMM per-call scratch, kept so the iteration loop reaches the allocator only on growth
+  DevBuf<int64_t> sg_need;
+  DevBuf<int64_t> sg_counts;
+  DevBuf<int64_t> sg_proj_ptr;
+  DevBuf<int32_t> sg_win_lo;
+  DevBuf<int32_t> sg_win_words;
+  DevBuf<int32_t> sg_cols;
+  DevBuf<int32_t> sg_proj_rows;
+  DevBuf<unsigned char> sg_proj_vals;
+  DevBuf<unsigned char> sg_fallback;
+  DevBuf<unsigned long long> sg_maxima;
   double* host_scalars = nullptr;   // pinned, kScalarSlots
   int64_t* host_counts = nullptr;   // pinned, 8
   int32_t* host_flags = nullptr;    // pinned, 8
@@ -44,7 +55,7 @@ struct Ctx {
 };
 
 // out[0] = 0, out[i + 1] = counts[0] + ... + counts[i]; returns out[n] (one
-// device-to-host read).  counts and out may alias.
+// device-to-host read).  counts and out must not alias.
 int64_t ScanCounts(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out);
 
 // Canonical reduction: the fixed 4096-wide tree over `n` partial sums.
@@ -69,6 +80,21 @@ enum class UnionMode { kAxpby = 0, kHalfSum = 1 };
 template <class T>
 void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T>& x, double xs, DevCsc<T>& out,
            UnionMode mode);
+
+// Fused drop step of M (dropping.cpp:106-135 and the per-column top-k rule):
+// M := 0.5 (M + M^T) when symmetric, relative threshold prune, then at most
+// topk entries per column (topk == 0: no cap).  Returns false, leaving M
+// untouched, when a column is too long for the shared-memory kernel.
+template <class T>
+bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk);
+
+// Warp-per-column union kernels (update.cu), used by Union().
+template <class T>
+void UnionCountWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, int64_t* counts);
+template <class T>
+void UnionWriteWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, bool scale_y, double ys, double xs, bool half_sum,
+                    bool prune, DevCsc<T>& out, int32_t* flag);
+int UnionWarpCap();
 
 // Row scaling out = diag(d) * b (Pr * X with a diagonal Pr); optional zero pruning.
 template <class T>

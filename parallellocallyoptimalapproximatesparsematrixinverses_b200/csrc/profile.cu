@@ -27,6 +27,21 @@ std::atomic<bool> g_enabled{false};
 std::mutex g_mutex;
 std::vector<Pending> g_pending;
 std::map<std::string, Totals> g_totals;
+std::vector<cudaEvent_t> g_free_events;  // recycled so a scope never creates events in steady state
+
+cudaEvent_t TakeEvent() {
+  {
+    std::lock_guard<std::mutex> lock(g_mutex);
+    if (!g_free_events.empty()) {
+      cudaEvent_t e = g_free_events.back();
+      g_free_events.pop_back();
+      return e;
+    }
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+  return e;
+}
 
 void Drain() {
   for (Pending& p : g_pending) {
@@ -37,8 +52,8 @@ void Drain() {
       t.count += 1;
       t.bytes += p.bytes;
     }
-    cudaEventDestroy(p.start);
-    cudaEventDestroy(p.stop);
+    g_free_events.push_back(p.start);
+    g_free_events.push_back(p.stop);
   }
   g_pending.clear();
 }
@@ -73,21 +88,37 @@ bool Read(const std::string& name, double* ms, int64_t* count, double* bytes) {
 
 Scope::Scope(cudaStream_t stream, const char* name, double bytes) : stream_(stream), name_(name), bytes_(bytes) {
   if (!Enabled()) return;
-  if (cudaEventCreate(&start_) != cudaSuccess) return;
+  start_ = TakeEvent();
+  if (start_ == nullptr) return;
   cudaEventRecord(start_, stream_);
   active_ = true;
 }
 
 Scope::~Scope() {
   if (!active_) return;
-  cudaEvent_t stop = nullptr;
-  if (cudaEventCreate(&stop) != cudaSuccess) {
-    cudaEventDestroy(start_);
-    return;
-  }
+  cudaEvent_t stop = TakeEvent();
+  if (stop == nullptr) return;
   cudaEventRecord(stop, stream_);
   std::lock_guard<std::mutex> lock(g_mutex);
   g_pending.push_back(Pending{name_, start_, stop, bytes_});
+  // fold finished pairs into the totals without blocking, so events recycle
+  if (g_pending.size() >= 256) {
+    size_t done = 0;
+    while (done < g_pending.size() && cudaEventQuery(g_pending[done].stop) == cudaSuccess) ++done;
+    for (size_t i = 0; i < done; ++i) {
+      Pending& p = g_pending[i];
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess) {
+        Totals& t = g_totals[p.name];
+        t.ms += ms;
+        t.count += 1;
+        t.bytes += p.bytes;
+      }
+      g_free_events.push_back(p.start);
+      g_free_events.push_back(p.stop);
+    }
+    g_pending.erase(g_pending.begin(), g_pending.begin() + static_cast<std::ptrdiff_t>(done));
+  }
 }
 
 }  // namespace prof

@@ -205,6 +205,7 @@ class Solver final : public SolverBase {
     iterations_ = 0;
     Copy(ctx_, m0_, m_);
     for (DevCsc<T>* x : {&r_, &z_, &p_, &ap_, &az_, &tmp_, &q_}) Empty(*x);
+    InvalidateResidualExtras();
     const bool inner_outer = opt_.method == Method::kInnerOuterMr || opt_.method == Method::kInnerOuterLomr;
     symmetric_ = !inner_outer;
     // PrepareStateManager (methods_common.cpp:126-157)
@@ -341,7 +342,36 @@ class Solver final : public SolverBase {
     }
   }
 
-  void Residual() { Spgemm(ctx_, A(), a_csr_, m_, r_, Epilogue::kResidual); }
+  // R = I - A*M, with the per-column squares of R (for ||R||_F) and, when Pr
+  // is diagonal and the dropping path keeps R's pattern, Z = Pr*R in the same pass.
+  void Residual() {
+    SpgemmExtras extras;
+    extras.col_squares = ctx_.Partial(kResidualPartial, n_);
+    DevCsc<T>* z_out = nullptr;
+    // the global methods (symmetric_) use Z = Pr*R right after every dropping-path residual
+    if (pr_diagonal_ && opt_.dropping && symmetric_) {
+      extras.row_scale = pr_vec_.data();
+      z_out = &z_fused_;
+    }
+    const bool z_written = Spgemm(ctx_, A(), a_csr_, m_, r_, Epilogue::kResidual, extras, z_out);
+    r_squares_ready_ = true;
+    z_fused_ready_ = z_written;
+  }
+
+  void InvalidateResidualExtras() {
+    r_squares_ready_ = false;
+    z_fused_ready_ = false;
+  }
+
+  // Z = Pr*R: the copy fused into the last residual product when it is current.
+  void ComputeZ() {
+    if (z_fused_ready_) {
+      z_.Swap(z_fused_);
+      z_fused_ready_ = false;
+      return;
+    }
+    MulPr(r_, z_);
+  }
 
   // ---- reductions ----------------------------------------------------------
   double Dot(const DevCsc<T>& x, const DevCsc<T>& y) {
@@ -355,6 +385,13 @@ class Solver final : public SolverBase {
   }
 
   double SquaredNorm(const DevCsc<T>& x) {
+    if (&x == &r_ && r_squares_ready_) {
+      const double* ready[1] = {ctx_.Partial(kResidualPartial, n_)};
+      TreeSums(ctx_, ready, 1, n_, 0);
+      double out;
+      FetchScalars(ctx_, 0, 1, &out);
+      return out;
+    }
     double* part = ctx_.Partial(0, n_);
     ColumnSquares(ctx_, View(x), part);
     const double* parts[1] = {part};
@@ -366,6 +403,7 @@ class Solver final : public SolverBase {
 
   // ---- sparse updates (sparse_operations.cpp:22-49) ------------------------
   void AddScaled(DevCsc<T>& t, const DevCsc<T>& d, double c) {
+    if (&t == &r_) InvalidateResidualExtras();
     if (c != 0.0) {
       Union(ctx_, t, false, 1.0, d, c, t, UnionMode::kAxpby);
     } else {
@@ -393,10 +431,13 @@ class Solver final : public SolverBase {
 
   // dropping.cpp:122-175 (or the per-column top-k variant)
   void ApplyDroppingStrategy() {
-    EnsureSymmetry();
-    PruneColumnRelative(ctx_, m_);
+    if (!SymmetrizeAndDrop(ctx_, m_, symmetric_, opt_.topk)) {
+      // a column longer than the fused kernel takes: the same steps one pass each
+      EnsureSymmetry();
+      PruneColumnRelative(ctx_, m_);
+      if (opt_.topk > 0) KeepTopKPerColumn(ctx_, m_, opt_.topk, true);
+    }
     if (opt_.topk > 0) {
-      KeepTopKPerColumn(ctx_, m_, opt_.topk, true);
       Residual();
       return;
     }
@@ -477,7 +518,7 @@ class Solver final : public SolverBase {
 
   // ---- Global CG (conjugate_gradient.cpp:15-83) ----------------------------
   void RunCg() {
-    MulPr(r_, z_);
+    ComputeZ();
     Copy(ctx_, z_, p_);
     double r_z = Dot(r_, z_);
     DropForMatrixType(p_);
@@ -492,7 +533,7 @@ class Solver final : public SolverBase {
       AddScaled(m_, p_, alpha);
       UpdateResiduals([&] { AddScaled(r_, ap_, -alpha); }, false);
       if (AppendIteration(p_)) break;
-      MulPr(r_, z_);
+      ComputeZ();
       r_z = Dot(r_, z_);
       const double beta = r_z / previous;
       if (!std::isfinite(beta)) break;
@@ -529,7 +570,7 @@ class Solver final : public SolverBase {
 
   // ---- Global MR (minimal_residual.cpp:31-93) ------------------------------
   void RunMr() {
-    MulPr(r_, z_);
+    ComputeZ();
     if (AppendIteration(z_)) return;
     double num = 0.0;
     double den = 0.0;
@@ -541,14 +582,14 @@ class Solver final : public SolverBase {
       AddScaled(m_, z_, alpha);
       UpdateResiduals([&] { Residual(); }, false);
       if (AppendIteration(z_)) break;
-      MulPr(r_, z_);
+      ComputeZ();
       MrProjection(num, den);
     }
   }
 
   // ---- Global LOMR (locally_minimal_residual.cpp:54-118) -------------------
   void RunLomr() {
-    MulPr(r_, z_);
+    ComputeZ();
     if (AppendIteration(z_)) return;
     for (int64_t i = 1; i <= opt_.max_iterations; ++i) {
       MulA(p_, ap_);
@@ -602,7 +643,7 @@ class Solver final : public SolverBase {
       LinComb(z_, 1.0, p_, std::isfinite(ratio) ? ratio : 0.0);
       DropForMatrixType(p_);
       if (AppendIteration(p_)) break;
-      MulPr(r_, z_);
+      ComputeZ();
     }
   }
 
@@ -694,6 +735,10 @@ class Solver final : public SolverBase {
   DevCsc<T> pr_csr_;
   DevCsc<T> m0_;
   DevCsc<T> m_, r_, z_, p_, ap_, az_, tmp_, q_;
+  DevCsc<T> z_fused_;             // Pr*R written by the last residual product
+  bool r_squares_ready_ = false;  // Partial(kResidualPartial) holds R's column squares
+  bool z_fused_ready_ = false;
+  static constexpr int kResidualPartial = 7;
   std::vector<SingleIterationData> history_;
   double initial_residual_ = 0.0;
   int64_t iterations_ = 0;

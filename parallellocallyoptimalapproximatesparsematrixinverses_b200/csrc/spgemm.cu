@@ -1,16 +1,26 @@
-// SpGEMM kernels (sm_100a).  One warp owns one output column.
+// SpGEMM C = X * B on sm_100a in four stages.
 //
-//  symbolic : the rows of X(:,k) for every k in B(:,j) are flattened across
-//             the 32 lanes and inserted into a per-warp open-addressing hash
-//             in shared memory; the number of new keys is the column count.
-//  numeric  : the row set is rebuilt, compacted and bitonic-sorted in shared
-//             memory; column j of B is put in a second hash (k -> value); lane
-//             s then computes output entry s by walking row i of X (CSR) in
-//             ascending k and looking each k up in the B hash.
+//  1. row-set count   (one warp per output column) -- the distinct rows of the
+//     union of X(:,k), k in B(:,j):
+//       bitmap: candidates set bits of a shared-memory bitmap over the row
+//               window (all candidate rows within 65,536 rows: every stencil
+//               operator); popcounts give the count;
+//       hash:   otherwise an open-addressing hash in shared memory (global
+//               memory beyond the largest bin).
+//  2. row-set list    (same warps, after the scan of the counts) -- writes the
+//     sorted rows of every column (bitmap: lane-blocked popcount prefix;
+//     hash: compaction + bitonic sort) and the column id of every entry.
+//  3. values          (one thread per output entry) -- entry (i, j) walks row
+//     i of X (CSR copy) in ascending k, finds each k in column j of B by a
+//     binary search (eight searches in flight per thread), and accumulates
+//     the first product x*y then += x*y in ascending k: the reference's
+//     accumulation order (Eigen's conservative sparse product), no FMA.
+//  4. column sums     (one thread per column) -- sequential per-column sums in
+//     row order for the global reductions (||R||^2, the MR projection).
 //
-// Columns are binned by the shared memory they need (hash tables sized at
-// twice the number of keys); columns beyond the largest bin use the same
-// code on a global-memory workspace.
+// Stages 1-2 are latency-bound warp-per-column work on small shared-memory
+// structures; stage 3, where the arithmetic happens, is parallel over all
+// output entries so the memory system sees enough independent loads.
 
 #include <cuda_runtime.h>
 
@@ -27,6 +37,16 @@ namespace spai {
 namespace {
 
 constexpr int32_t kEmpty = -1;
+constexpr int kBitmapMaxWords = 2048;  // 65,536-row window
+// window-word bins of the bitmap row-set kernels
+constexpr int kWordBins[] = {128, 512, 1040, kBitmapMaxWords};
+constexpr int kWordBinCount = 4;
+// maxima[] layout: 0 max upper bound, 1 max nnz(B col), 4.. bitmap bin populations, 8 hash columns
+constexpr int kMaxUb = 0;
+constexpr int kMaxNb = 1;
+constexpr int kPopulation = 4;
+constexpr int kHashColumns = 8;
+constexpr int kMaximaSlots = 16;
 
 __device__ __forceinline__ unsigned LaneMaskBelow() {
   unsigned mask;
@@ -44,61 +64,7 @@ __host__ __device__ inline int Log2(int v) {
   return b;
 }
 
-// Per-warp workspace (shared memory or global memory).
-template <class T>
-struct Space {
-  double* stage0;    // slots/2
-  double* stage1;    // slots/2
-  T* bvals;          // slots/2
-  int64_t* xstart;   // 32
-  int32_t* keys;     // slots
-  int32_t* sorted;   // slots/2
-  int32_t* bkeys;    // slots/2
-  int32_t* prefix;   // 33
-  uint8_t* present;  // slots/2
-};
-
 __host__ __device__ inline size_t Round16(size_t v) { return (v + 15) & ~static_cast<size_t>(15); }
-
-template <class T>
-__host__ __device__ inline size_t SpaceBytes(int slots, bool numeric) {
-  if (!numeric) {
-    return Round16(32 * sizeof(int64_t)) + Round16(static_cast<size_t>(slots) * 4) + Round16(33 * 4);
-  }
-  const size_t half = static_cast<size_t>(slots) / 2;
-  return Round16(half * 8) * 2 + Round16(half * sizeof(T)) + Round16(32 * sizeof(int64_t)) +
-         Round16(static_cast<size_t>(slots) * 4) + Round16(half * 4) * 2 + Round16(33 * 4) + Round16(half);
-}
-
-template <class T>
-__device__ inline Space<T> CarveSpace(unsigned char* base, int slots, bool numeric) {
-  Space<T> s{};
-  const size_t half = static_cast<size_t>(slots) / 2;
-  if (numeric) {
-    s.stage0 = reinterpret_cast<double*>(base);
-    base += Round16(half * 8);
-    s.stage1 = reinterpret_cast<double*>(base);
-    base += Round16(half * 8);
-    s.bvals = reinterpret_cast<T*>(base);
-    base += Round16(half * sizeof(T));
-  }
-  s.xstart = reinterpret_cast<int64_t*>(base);
-  base += Round16(32 * sizeof(int64_t));
-  s.keys = reinterpret_cast<int32_t*>(base);
-  base += Round16(static_cast<size_t>(slots) * 4);
-  if (numeric) {
-    s.sorted = reinterpret_cast<int32_t*>(base);
-    base += Round16(half * 4);
-    s.bkeys = reinterpret_cast<int32_t*>(base);
-    base += Round16(half * 4);
-  }
-  s.prefix = reinterpret_cast<int32_t*>(base);
-  base += Round16(33 * 4);
-  if (numeric) {
-    s.present = reinterpret_cast<uint8_t*>(base);
-  }
-  return s;
-}
 
 // Returns true when `key` was not in the table yet.
 __device__ __forceinline__ bool InsertKey(int32_t* table, int bits, int32_t key) {
@@ -112,47 +78,37 @@ __device__ __forceinline__ bool InsertKey(int32_t* table, int bits, int32_t key)
   }
 }
 
-// Keys are unique: claims a slot and returns it.
-__device__ __forceinline__ uint32_t ClaimSlot(int32_t* table, int bits, int32_t key) {
-  const uint32_t mask = (1u << bits) - 1u;
-  uint32_t h = Slot(key, bits);
-  while (true) {
-    const int32_t old = atomicCAS(&table[h], kEmpty, key);
-    if (old == kEmpty || old == key) return h;
-    h = (h + 1u) & mask;
-  }
-}
-
-template <class T>
-__device__ __forceinline__ bool Lookup(const int32_t* table, const T* vals, int bits, int32_t key, T& out) {
-  const uint32_t mask = (1u << bits) - 1u;
-  uint32_t h = Slot(key, bits);
-  while (true) {
-    const int32_t cur = table[h];
-    if (cur == key) {
-      out = vals[h];
-      return true;
-    }
-    if (cur == kEmpty) return false;
-    h = (h + 1u) & mask;
-  }
-}
-
 __device__ inline void ClearTable(int32_t* table, int size, int lane) {
   for (int i = lane; i < size; i += kWarp) table[i] = kEmpty;
 }
 
-// Inserts every row of X(:,k), k in B(:,col), plus the diagonal when asked;
-// returns the number of new keys (warp-uniform).
-template <class T>
-__device__ int InsertColumnRows(const CscView<T>& x, const CscView<T>& b, int64_t col, bool add_diag,
-                                const Space<T>& s, int bits, int lane) {
-  int added = 0;
-  if (add_diag) {
-    bool fresh = false;
-    if (lane == 0) fresh = InsertKey(s.keys, bits, static_cast<int32_t>(col));
-    added += __popc(__ballot_sync(0xffffffffu, fresh));
+__device__ inline void ClearWords(uint32_t* words, int size, int lane) {
+  for (int i = lane; i < size; i += kWarp) words[i] = 0u;
+}
+
+// One atomic per warp instead of one per thread.
+__device__ __forceinline__ void WarpAtomicAdd(unsigned long long* target, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicAdd(target, v);
+}
+
+__device__ __forceinline__ void WarpAtomicMax(unsigned long long* target, unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, v, o);
+    v = other > v ? other : v;
   }
+  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicMax(target, v);
+}
+
+// Calls f(row) for every candidate row of output column `col`, the rows of
+// X(:,k) for k in B(:,col) flattened across the 32 lanes; f returns true for
+// a new row.  Returns the warp-uniform number of new rows.
+template <class T, class F>
+__device__ int ForEachCandidate(const CscView<T>& x, const CscView<T>& b, int64_t col, int32_t* prefix,
+                                int64_t* xstart, int lane, F f) {
+  int added = 0;
   const int64_t start = b.ptr[col];
   const int64_t end = b.ptr[col + 1];
   for (int64_t base = start; base < end; base += kWarp) {
@@ -171,26 +127,24 @@ __device__ int InsertColumnRows(const CscView<T>& x, const CscView<T>& b, int64_
       if (lane >= o) inclusive += y;
     }
     const int total = __shfl_sync(0xffffffffu, inclusive, 31);
-    s.prefix[lane] = inclusive - len;
-    s.xstart[lane] = xs;
+    prefix[lane] = inclusive - len;
+    xstart[lane] = xs;
     __syncwarp();
     for (int e0 = 0; e0 < total; e0 += kWarp) {
       const int e = e0 + lane;
       bool fresh = false;
       if (e < total) {
-        // largest entry b with prefix[b] <= e
         int lo = 0;
         int hi = 31;
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
-          if (s.prefix[mid] <= e) {
+          if (prefix[mid] <= e) {
             lo = mid;
           } else {
             hi = mid - 1;
           }
         }
-        const int64_t q = s.xstart[lo] + (e - s.prefix[lo]);
-        fresh = InsertKey(s.keys, bits, x.idx[q]);
+        fresh = f(x.idx[xstart[lo] + (e - prefix[lo])]);
       }
       added += __popc(__ballot_sync(0xffffffffu, fresh));
     }
@@ -199,352 +153,417 @@ __device__ int InsertColumnRows(const CscView<T>& x, const CscView<T>& b, int64_
   return added;
 }
 
+// Per-lane variant for narrow windows: lane l walks the X columns of B
+// entries l, l+32, ...; the B indices and X column bounds of up to four
+// rounds are loaded before any row, so the loads overlap.
+template <class T, class F>
+__device__ inline void ForEachCandidateByLane(const CscView<T>& x, const CscView<T>& b, int64_t col, int lane, F f) {
+  constexpr int kRounds = 4;
+  const int64_t start = b.ptr[col];
+  const int64_t end = b.ptr[col + 1];
+  for (int64_t base = start; base < end; base += kRounds * kWarp) {
+    int32_t k[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      const int64_t p = base + lane + r * kWarp;
+      k[r] = p < end ? b.idx[p] : -1;
+    }
+    int64_t xs[kRounds];
+    int64_t xe[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      xs[r] = k[r] >= 0 ? x.ptr[k[r]] : 0;
+      xe[r] = k[r] >= 0 ? x.ptr[k[r] + 1] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+      for (int64_t q0 = xs[r]; q0 < xe[r]; q0 += 8) {
+        int32_t rows[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) rows[u] = q0 + u < xe[r] ? x.idx[q0 + u] : -1;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (rows[u] >= 0) f(rows[u]);
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Stages 1-2: row sets
 template <class T>
-struct SymbolicArgs {
+struct RowSetArgs {
   CscView<T> x;
   CscView<T> b;
-  const int64_t* need;  // per column required slots
+  const int64_t* need;       // hash path: table slots needed (2 * upper bound)
+  const int32_t* win_lo;     // first row of the candidate window
+  const int32_t* win_words;  // window length in 32-row words (0: no candidates)
   bool add_diag;
-  int64_t* counts;
-  unsigned char* global_space;  // fallback workspace (nullptr: shared memory)
+  bool list;                 // false: count rows; true: write them
+  int64_t* counts;           // count mode output
+  const int64_t* c_ptr;      // list mode: output offsets
+  int32_t* rows;             // list mode: sorted rows
+  int32_t* cols;             // list mode: column id of every entry
+  unsigned char* global_space;
 };
 
+__host__ __device__ inline size_t BitmapBytes(int words) { return Round16(static_cast<size_t>(words) * 4); }
+
 template <class T>
-__global__ void SymbolicKernel(SymbolicArgs<T> a, int slots, int64_t lo_need, int64_t hi_need) {
+__global__ void BitmapRowSetKernel(RowSetArgs<T> a, int words_cap, int lo_words, int hi_words) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int warp_in_block = threadIdx.x >> 5;
-  const int warps_per_block = blockDim.x >> 5;
-  const size_t bytes = SpaceBytes<T>(slots, false);
-  unsigned char* base = a.global_space != nullptr
-                            ? a.global_space + (static_cast<size_t>(blockIdx.x) * warps_per_block + warp_in_block) * bytes
-                            : smem + warp_in_block * bytes;
-  const Space<T> s = CarveSpace<T>(base, slots, false);
-  const int bits = Log2(slots);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(smem + warp_in_block * BitmapBytes(words_cap));
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t col = warp; col < a.b.cols; col += warps) {
-    const int64_t need = a.need[col];
-    if (need <= lo_need || need > hi_need) continue;
-    ClearTable(s.keys, slots, lane);
+    const int words = a.win_words[col];
+    if (words <= lo_words || words > hi_words) continue;
+    const int32_t lo = a.win_lo[col];
+    ClearWords(bm, words, lane);
     __syncwarp();
-    const int count = InsertColumnRows(a.x, a.b, col, a.add_diag, s, bits, lane);
-    if (lane == 0) a.counts[col] = count;
+    if (a.add_diag && lane == 0) {
+      const int off = static_cast<int>(col) - lo;
+      atomicOr(&bm[off >> 5], 1u << (off & 31));
+    }
+    ForEachCandidateByLane(a.x, a.b, col, lane, [&](int32_t row) {
+      const int off = row - lo;
+      atomicOr(&bm[off >> 5], 1u << (off & 31));
+    });
+    __syncwarp();
+    if (!a.list) {
+      int count = 0;
+      for (int w = lane; w < words; w += kWarp) count += __popc(bm[w]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) count += __shfl_xor_sync(0xffffffffu, count, o);
+      if (lane == 0) a.counts[col] = count;
+    } else {
+      // lane-blocked prefix over the window words, then each lane writes its rows in order
+      const int per_lane = (words + kWarp - 1) / kWarp;
+      const int w0 = lane * per_lane;
+      const int w1 = min(w0 + per_lane, words);
+      int local = 0;
+      for (int w = w0; w < w1; ++w) local += __popc(bm[w]);
+      int inclusive = local;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inclusive, o);
+        if (lane >= o) inclusive += y;
+      }
+      int64_t out = a.c_ptr[col] + (inclusive - local);
+      const int32_t col32 = static_cast<int32_t>(col);
+      for (int w = w0; w < w1; ++w) {
+        uint32_t bits = bm[w];
+        while (bits != 0u) {
+          const int bit = __ffs(bits) - 1;
+          a.rows[out] = lo + (w << 5) + bit;
+          a.cols[out] = col32;
+          ++out;
+          bits &= bits - 1u;
+        }
+      }
+    }
     __syncwarp();
   }
 }
 
-template <class T>
-struct NumericArgs {
-  CscView<T> x_csc;
-  CscView<T> x_csr;
-  CscView<T> b;
-  const int64_t* need;
-  const int64_t* c_ptr;  // symbolic offsets (nullptr for kProjection)
-  int epilogue;
-  int32_t* c_idx;
-  T* c_val;
-  T* z_val;
-  const T* row_scale;
-  double* col_squares;
-  double* proj_tt;
-  double* proj_bt;
-  int64_t* kept;
-  int32_t* flag;
-  unsigned char* global_space;
-};
+__host__ __device__ inline size_t HashRowSetBytes(int slots) {
+  // keys + sorted (half) + flattening scratch
+  return Round16(static_cast<size_t>(slots) * 4) + Round16(static_cast<size_t>(slots) * 2) +
+         Round16(32 * sizeof(int64_t)) + Round16(33 * 4);
+}
 
 template <class T>
-__global__ void NumericKernel(NumericArgs<T> a, int slots, int64_t lo_need, int64_t hi_need) {
+__global__ void HashRowSetKernel(RowSetArgs<T> a, int slots, int64_t lo_need, int64_t hi_need) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int warp_in_block = threadIdx.x >> 5;
   const int warps_per_block = blockDim.x >> 5;
-  const size_t bytes = SpaceBytes<T>(slots, true);
+  const size_t bytes = HashRowSetBytes(slots);
   unsigned char* base = a.global_space != nullptr
                             ? a.global_space + (static_cast<size_t>(blockIdx.x) * warps_per_block + warp_in_block) * bytes
                             : smem + warp_in_block * bytes;
-  const Space<T> s = CarveSpace<T>(base, slots, true);
+  int32_t* keys = reinterpret_cast<int32_t*>(base);
+  int32_t* sorted = reinterpret_cast<int32_t*>(base + Round16(static_cast<size_t>(slots) * 4));
+  int64_t* xstart = reinterpret_cast<int64_t*>(base + Round16(static_cast<size_t>(slots) * 4) +
+                                               Round16(static_cast<size_t>(slots) * 2));
+  int32_t* prefix = reinterpret_cast<int32_t*>(reinterpret_cast<unsigned char*>(xstart) + Round16(32 * sizeof(int64_t)));
   const int bits = Log2(slots);
-  const int bbits = bits - 1;
-  const int half = slots / 2;
-  const bool residual = a.epilogue == static_cast<int>(Epilogue::kResidual);
-  const bool projection = a.epilogue == static_cast<int>(Epilogue::kProjection);
-  const bool prune = a.epilogue == static_cast<int>(Epilogue::kPruneZeros) || residual;
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t col = warp; col < a.b.cols; col += warps) {
+    if (a.win_words[col] <= kBitmapMaxWords) continue;
     const int64_t need = a.need[col];
     if (need <= lo_need || need > hi_need) continue;
-    ClearTable(s.keys, slots, lane);
-    ClearTable(s.bkeys, half, lane);
+    ClearTable(keys, slots, lane);
     __syncwarp();
-    // hash of B(:, col): k -> value
-    const int64_t bs = a.b.ptr[col];
-    const int64_t be = a.b.ptr[col + 1];
-    for (int64_t p = bs + lane; p < be; p += kWarp) {
-      const uint32_t h = ClaimSlot(s.bkeys, bbits, a.b.idx[p]);
-      s.bvals[h] = a.b.val[p];
-    }
-    InsertColumnRows(a.x_csc, a.b, col, residual, s, bits, lane);
-    __syncwarp();
-    // compact and sort the row set
     int count = 0;
-    for (int base_slot = 0; base_slot < slots; base_slot += kWarp) {
-      const int32_t key = s.keys[base_slot + lane];
+    if (a.add_diag) {
+      bool fresh = false;
+      if (lane == 0) fresh = InsertKey(keys, bits, static_cast<int32_t>(col));
+      count += __popc(__ballot_sync(0xffffffffu, fresh));
+    }
+    count += ForEachCandidate(a.x, a.b, col, prefix, xstart, lane,
+                              [&](int32_t row) { return InsertKey(keys, bits, row); });
+    __syncwarp();
+    if (!a.list) {
+      if (lane == 0) a.counts[col] = count;
+      __syncwarp();
+      continue;
+    }
+    int n = 0;
+    for (int s = 0; s < slots; s += kWarp) {
+      const int32_t key = keys[s + lane];
       const bool occupied = key != kEmpty;
       const unsigned mask = __ballot_sync(0xffffffffu, occupied);
-      if (occupied) s.sorted[count + __popc(mask & LaneMaskBelow())] = key;
-      count += __popc(mask);
+      if (occupied) sorted[n + __popc(mask & LaneMaskBelow())] = key;
+      n += __popc(mask);
     }
     int size = 1;
-    while (size < count) size <<= 1;
-    for (int i = count + lane; i < size; i += kWarp) s.sorted[i] = INT32_MAX;
+    while (size < n) size <<= 1;
+    for (int i = n + lane; i < size; i += kWarp) sorted[i] = INT32_MAX;
     __syncwarp();
     for (int k = 2; k <= size; k <<= 1) {
       for (int j = k >> 1; j > 0; j >>= 1) {
         for (int i = lane; i < size; i += kWarp) {
           const int ixj = i ^ j;
           if (ixj > i) {
-            const int32_t u = s.sorted[i];
-            const int32_t v = s.sorted[ixj];
-            const bool ascending = (i & k) == 0;
-            if ((u > v) == ascending) {
-              s.sorted[i] = v;
-              s.sorted[ixj] = u;
+            const int32_t u = sorted[i];
+            const int32_t v = sorted[ixj];
+            if ((u > v) == ((i & k) == 0)) {
+              sorted[i] = v;
+              sorted[ixj] = u;
             }
           }
         }
         __syncwarp();
       }
     }
-    // numeric values
-    const int64_t out_base = projection ? 0 : a.c_ptr[col];
-    int kept = 0;
-    for (int base_pos = 0; base_pos < count; base_pos += kWarp) {
-      const int pos = base_pos + lane;
-      const bool active = pos < count;
-      int32_t row = 0;
-      double acc = 0.0;
-      bool has = false;
-      if (active) {
-        row = s.sorted[pos];
-        const int64_t rs = a.x_csr.ptr[row];
-        const int64_t re = a.x_csr.ptr[row + 1];
-        for (int64_t q = rs; q < re; ++q) {
-          T bv;
-          if (Lookup(s.bkeys, s.bvals, bbits, a.x_csr.idx[q], bv)) {
-            const double prod = Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv));
-            acc = has ? Add(acc, prod) : prod;
-            has = true;
-          }
-        }
-      }
-      if (projection) {
-        if (active) {
-          const T az = static_cast<T>(acc);
-          const T t = static_cast<T>(Mul(static_cast<double>(a.row_scale[row]), static_cast<double>(az)));
-          const double td = static_cast<double>(t);
-          s.stage0[pos] = Mul(td, td);
-          T zv;
-          const bool in_b = Lookup(s.bkeys, s.bvals, bbits, row, zv);
-          s.present[pos] = in_b ? 1 : 0;
-          s.stage1[pos] = in_b ? Mul(static_cast<double>(zv), td) : 0.0;
-        }
-        continue;
-      }
-      double v = acc;
-      if (residual) {
-        v = has ? -acc : 0.0;
-        if (static_cast<int64_t>(row) == col) v = has ? Add(v, 1.0) : 1.0;
-      }
-      const T stored = static_cast<T>(v);
-      const bool keep = active && !(prune && fabs(static_cast<double>(stored)) <= 0.0);
-      const unsigned mask = __ballot_sync(0xffffffffu, keep);
-      if (keep) {
-        const int slot = kept + __popc(mask & LaneMaskBelow());
-        a.c_idx[out_base + slot] = row;
-        a.c_val[out_base + slot] = stored;
-        if (a.z_val != nullptr) {
-          a.z_val[out_base + slot] =
-              static_cast<T>(Mul(static_cast<double>(a.row_scale[row]), static_cast<double>(stored)));
-        }
-        const double sd = static_cast<double>(stored);
-        s.stage0[slot] = Mul(sd, sd);
-      }
-      kept += __popc(mask);
-    }
-    __syncwarp();
-    if (lane == 0) {
-      if (projection) {
-        double tt = 0.0;
-        double bt = 0.0;
-        for (int i = 0; i < count; ++i) {
-          tt = Add(tt, s.stage0[i]);
-          if (s.present[i]) bt = Add(bt, s.stage1[i]);
-        }
-        a.proj_tt[col] = tt;
-        a.proj_bt[col] = bt;
-      } else {
-        if (a.col_squares != nullptr) {
-          double sq = 0.0;
-          for (int i = 0; i < kept; ++i) sq = Add(sq, s.stage0[i]);
-          a.col_squares[col] = sq;
-        }
-        a.kept[col] = kept;
-        if (kept != count) atomicOr(a.flag, 1);
-      }
+    const int64_t out = a.c_ptr[col];
+    const int32_t col32 = static_cast<int32_t>(col);
+    for (int i = lane; i < n; i += kWarp) {
+      a.rows[out + i] = sorted[i];
+      a.cols[out + i] = col32;
     }
     __syncwarp();
   }
 }
 
+// ---------------------------------------------------------------------------
+// Stage 3: values, one thread per output entry
+enum class ValueMode : int { kStore = 0, kResidual = 1, kProjection = 2, kMasked = 3 };
+
 template <class T>
-struct MaskedArgs {
+struct ValuesArgs {
   CscView<T> x_csr;
   CscView<T> b;
-  CscView<T> mask;
-  const int64_t* need;
-  double* out;
-  unsigned char* global_space;
+  const int32_t* rows;
+  const int32_t* cols;
+  int64_t count;
+  int mode;
+  bool prune;
+  T* out;              // kStore/kResidual: C values; kProjection: t = pr * (X B)
+  T* z_out;            // kResidual: Z = pr * R (optional)
+  const T* row_scale;  // pr
+  double* out_f64;     // kMasked
+  int32_t* flag;       // set when a stored value is an exact zero (pruning needed)
 };
 
 template <class T>
-__global__ void MaskedKernel(MaskedArgs<T> a, int slots, int64_t lo_need, int64_t hi_need) {
-  extern __shared__ __align__(16) unsigned char smem[];
-  const int lane = threadIdx.x & 31;
-  const int warp_in_block = threadIdx.x >> 5;
-  const int warps_per_block = blockDim.x >> 5;
-  const size_t bytes = SpaceBytes<T>(slots, true);
-  unsigned char* base = a.global_space != nullptr
-                            ? a.global_space + (static_cast<size_t>(blockIdx.x) * warps_per_block + warp_in_block) * bytes
-                            : smem + warp_in_block * bytes;
-  const Space<T> s = CarveSpace<T>(base, slots, true);
-  const int bbits = Log2(slots) - 1;
-  const int half = slots / 2;
-  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t col = warp; col < a.b.cols; col += warps) {
-    const int64_t need = a.need[col];
-    if (need <= lo_need || need > hi_need) continue;
-    ClearTable(s.bkeys, half, lane);
-    __syncwarp();
-    for (int64_t p = a.b.ptr[col] + lane; p < a.b.ptr[col + 1]; p += kWarp) {
-      const uint32_t h = ClaimSlot(s.bkeys, bbits, a.b.idx[p]);
-      s.bvals[h] = a.b.val[p];
-    }
-    __syncwarp();
-    for (int64_t p = a.mask.ptr[col] + lane; p < a.mask.ptr[col + 1]; p += kWarp) {
-      const int32_t row = a.mask.idx[p];
-      double acc = 0.0;
-      bool has = false;
-      for (int64_t q = a.x_csr.ptr[row]; q < a.x_csr.ptr[row + 1]; ++q) {
-        T bv;
-        if (Lookup(s.bkeys, s.bvals, bbits, a.x_csr.idx[q], bv)) {
-          const double prod = Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv));
+__global__ void __launch_bounds__(256) ValuesKernel(ValuesArgs<T> a) {
+  bool zero_seen = false;
+  for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < a.count;
+       p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int32_t i = a.rows[p];
+    const int32_t j = a.cols[p];
+    const int64_t bs = a.b.ptr[j];
+    const int blen = static_cast<int>(a.b.ptr[j + 1] - bs);
+    const int64_t xs = a.x_csr.ptr[i];
+    const int64_t xe = a.x_csr.ptr[i + 1];
+    double acc = 0.0;
+    bool has = false;
+    for (int64_t q0 = xs; q0 < xe; q0 += 8) {
+      int32_t kk[8];
+      T xv[8];
+      int64_t at[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t q = q0 + u;
+        kk[u] = q < xe ? a.x_csr.idx[q] : INT32_MAX;
+        xv[u] = q < xe ? a.x_csr.val[q] : T(0);
+        at[u] = bs;
+      }
+      // eight lower-bound searches in column j of B, in lock step
+      int len = blen;
+      while (len > 1) {
+        const int half = len >> 1;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (a.b.idx[at[u] + half] <= kk[u]) at[u] += half;
+        }
+        len -= half;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        if (blen > 0 && q0 + u < xe && a.b.idx[at[u]] == kk[u]) {
+          const double prod = Mul(static_cast<double>(xv[u]), static_cast<double>(a.b.val[at[u]]));
           acc = has ? Add(acc, prod) : prod;
           has = true;
         }
       }
-      a.out[p] = has ? acc : 0.0;
     }
-    __syncwarp();
+    if (a.mode == static_cast<int>(ValueMode::kMasked)) {
+      a.out_f64[p] = has ? acc : 0.0;
+      continue;
+    }
+    if (a.mode == static_cast<int>(ValueMode::kProjection)) {
+      const T az = static_cast<T>(acc);
+      a.out[p] = static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(az)));
+      continue;
+    }
+    double v = acc;
+    if (a.mode == static_cast<int>(ValueMode::kResidual)) {
+      v = has ? -acc : 0.0;
+      if (i == j) v = has ? Add(v, 1.0) : 1.0;
+    }
+    const T stored = static_cast<T>(v);
+    a.out[p] = stored;
+    if (a.z_out != nullptr) {
+      a.z_out[p] = static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(stored)));
+    }
+    if (a.prune && fabs(static_cast<double>(stored)) <= 0.0) zero_seen = true;
   }
+  if (__any_sync(0xffffffffu, zero_seen) && (threadIdx.x & 31) == 0) atomicOr(a.flag, 1);
 }
 
-// One atomicMax per warp instead of one per thread.
-__device__ __forceinline__ void WarpAtomicMax(unsigned long long* target, unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, v, o);
-    v = other > v ? other : v;
-  }
-  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicMax(target, v);
-}
-
-// upper bound on distinct rows and the B column length, plus the maxima.
+// ---------------------------------------------------------------------------
+// Stage 4: per-column sequential sums
 template <class T>
-__global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ ub,
+struct SumsArgs {
+  const int64_t* c_ptr;
+  const int32_t* rows;
+  const T* vals;
+  CscView<T> b;  // projection: B = Z
+  bool projection;
+  double* col_squares;
+  double* proj_tt;
+  double* proj_bt;
+  int64_t cols;
+};
+
+template <class T>
+__global__ void ColumnSumsKernel(SumsArgs<T> a) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < a.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t s = a.c_ptr[j];
+    const int64_t e = a.c_ptr[j + 1];
+    double sq = 0.0;
+    for (int64_t p = s; p < e; ++p) {
+      const double v = static_cast<double>(a.vals[p]);
+      sq = Add(sq, Mul(v, v));
+    }
+    if (!a.projection) {
+      a.col_squares[j] = sq;
+      continue;
+    }
+    a.proj_tt[j] = sq;
+    double bt = 0.0;
+    int64_t p = s;
+    int64_t q = a.b.ptr[j];
+    const int64_t qe = a.b.ptr[j + 1];
+    while (p < e && q < qe) {
+      const int32_t r1 = a.rows[p];
+      const int32_t r2 = a.b.idx[q];
+      if (r1 == r2) {
+        bt = Add(bt, Mul(static_cast<double>(a.b.val[q]), static_cast<double>(a.vals[p])));
+        ++p;
+        ++q;
+      } else if (r1 < r2) {
+        ++p;
+      } else {
+        ++q;
+      }
+    }
+    a.proj_bt[j] = bt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hash need, window and bin populations of every output column.
+template <class T>
+__global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ need,
+                           int32_t* __restrict__ win_lo, int32_t* __restrict__ win_words,
                            unsigned long long* __restrict__ maxima) {
   unsigned long long local_ub = 0;
   unsigned long long local_nb = 0;
+  unsigned long long population[kWordBinCount + 1] = {};
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < b.cols;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
     int64_t u = add_diag ? 1 : 0;
+    int32_t lo = add_diag ? static_cast<int32_t>(j) : INT32_MAX;
+    int32_t hi = add_diag ? static_cast<int32_t>(j) : -1;
     for (int64_t p = b.ptr[j]; p < b.ptr[j + 1]; ++p) {
       const int32_t k = b.idx[p];
-      u += x.ptr[k + 1] - x.ptr[k];
+      const int64_t xs = x.ptr[k];
+      const int64_t xe = x.ptr[k + 1];
+      if (xe > xs) {
+        u += xe - xs;
+        lo = min(lo, x.idx[xs]);
+        hi = max(hi, x.idx[xe - 1]);
+      }
     }
-    ub[j] = u;
+    need[j] = 2 * u;
+    int words = 0;
+    if (hi >= lo) {
+      const int64_t w = (static_cast<int64_t>(hi) - lo) / 32 + 1;
+      words = w > INT32_MAX ? INT32_MAX : static_cast<int>(w);
+    }
+    win_lo[j] = hi >= lo ? lo : 0;
+    win_words[j] = words;
+    // bins: <= 128, 512, 1040, 2048 words (kWordBins), else the hash path
+    if (words <= 128) {
+      ++population[0];
+    } else if (words <= 512) {
+      ++population[1];
+    } else if (words <= 1040) {
+      ++population[2];
+    } else if (words <= kBitmapMaxWords) {
+      ++population[3];
+    } else {
+      ++population[4];
+    }
     local_ub = max(local_ub, static_cast<unsigned long long>(u));
     local_nb = max(local_nb, static_cast<unsigned long long>(b.ptr[j + 1] - b.ptr[j]));
   }
-  WarpAtomicMax(&maxima[0], local_ub);
-  WarpAtomicMax(&maxima[1], local_nb);
-}
-
-// symbolic need = 2 * ub; numeric need = max(2 * count, 4 * nb)
-__global__ void SymbolicNeedKernel(const int64_t* __restrict__ ub, int64_t cols, int64_t* __restrict__ need) {
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < cols;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    need[j] = 2 * ub[j];
-  }
-}
-
-__global__ void NumericNeedKernel(const int64_t* __restrict__ counts, const int64_t* __restrict__ bptr, int64_t cols,
-                                  int64_t* __restrict__ need, unsigned long long* __restrict__ maxima) {
-  unsigned long long local = 0;
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < cols;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t c = counts[j];
-    const int64_t nb = bptr[j + 1] - bptr[j];
-    int64_t v = 2 * c > 4 * nb ? 2 * c : 4 * nb;
-    if (v < 2) v = 2;
-    need[j] = v;
-    local = max(local, static_cast<unsigned long long>(v));
-  }
-  WarpAtomicMax(&maxima[2], local);
-}
-
-__global__ void MaskedNeedKernel(const int64_t* __restrict__ bptr, int64_t cols, int64_t* __restrict__ need) {
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < cols;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    int64_t v = 4 * (bptr[j + 1] - bptr[j]);
-    need[j] = v < 2 ? 2 : v;
-  }
+  WarpAtomicMax(&maxima[kMaxUb], local_ub);
+  WarpAtomicMax(&maxima[kMaxNb], local_nb);
+  for (int i = 0; i < kWordBinCount; ++i) WarpAtomicAdd(&maxima[kPopulation + i], population[i]);
+  WarpAtomicAdd(&maxima[kHashColumns], population[kWordBinCount]);
 }
 
 template <class T>
-__global__ void SqueezeKernel(int64_t cols, const int64_t* __restrict__ old_ptr, const int64_t* __restrict__ new_ptr,
-                              const int32_t* __restrict__ old_idx, const T* __restrict__ old_val,
-                              const T* __restrict__ old_z, int32_t* __restrict__ new_idx, T* __restrict__ new_val,
-                              T* __restrict__ new_z) {
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < cols;
+__global__ void ColumnIdsKernel(CscView<T> m, int32_t* __restrict__ cols) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < m.cols;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t src = old_ptr[j];
-    const int64_t dst = new_ptr[j];
-    const int64_t len = new_ptr[j + 1] - dst;
-    for (int64_t i = 0; i < len; ++i) {
-      new_idx[dst + i] = old_idx[src + i];
-      new_val[dst + i] = old_val[src + i];
-      if (new_z != nullptr) new_z[dst + i] = old_z[src + i];
-    }
+    for (int64_t p = m.ptr[j]; p < m.ptr[j + 1]; ++p) cols[p] = static_cast<int32_t>(j);
   }
 }
 
-struct Bin {
+struct HashBin {
   int slots;
   int warps;
   int64_t lo;
   int64_t hi;
 };
 
-constexpr Bin kBins[] = {
+constexpr HashBin kHashBins[] = {
     {256, 8, -1, 256},
-    {1024, 4, 256, 1024},
-    {4096, 1, 1024, 4096},
+    {1024, 8, 256, 1024},
+    {4096, 4, 1024, 4096},
 };
-constexpr int64_t kLargestBin = 4096;
+constexpr int64_t kLargestHashBin = 4096;
 
 int NextPow2(int64_t v) {
   int64_t p = 1;
@@ -552,29 +571,51 @@ int NextPow2(int64_t v) {
   return static_cast<int>(p);
 }
 
-template <class Kernel, class Args>
-void LaunchBins(Ctx& ctx, Kernel kernel, Args args, int64_t cols, int64_t max_need, bool numeric, size_t tsize,
-                DevBuf<unsigned char>& fallback) {
-  for (const Bin& bin : kBins) {
+int WarpsFor(size_t bytes_per_warp) {
+  const size_t budget = 96 * 1024;
+  int warps = static_cast<int>(budget / (bytes_per_warp > 0 ? bytes_per_warp : 1));
+  return warps < 1 ? 1 : (warps > 16 ? 16 : warps);
+}
+
+// Launches the row-set stage (count or list mode) over every populated bin.
+template <class T>
+void LaunchRowSets(Ctx& ctx, RowSetArgs<T> args, const unsigned long long* host_max) {
+  int lo_words = -1;
+  for (int bin = 0; bin < kWordBinCount; ++bin) {
+    const int words_cap = kWordBins[bin];
+    const int64_t population = static_cast<int64_t>(host_max[kPopulation + bin]);
+    if (population > 0) {
+      const size_t per_warp = BitmapBytes(words_cap);
+      const int warps = WarpsFor(per_warp);
+      const size_t smem = per_warp * warps;
+      SPAI_CUDA(cudaFuncSetAttribute(BitmapRowSetKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+      BitmapRowSetKernel<T><<<GridFor(population * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(
+          args, words_cap, lo_words, words_cap);
+      SPAI_LAUNCH_CHECK();
+    }
+    lo_words = words_cap;
+  }
+  if (host_max[kHashColumns] == 0) return;
+  const int64_t max_need = 2 * static_cast<int64_t>(host_max[kMaxUb]);
+  const int64_t hash_columns = static_cast<int64_t>(host_max[kHashColumns]);
+  for (const HashBin& bin : kHashBins) {
     if (max_need <= bin.lo) break;
-    const size_t per_warp = numeric ? (tsize == 8 ? SpaceBytes<double>(bin.slots, true) : SpaceBytes<float>(bin.slots, true))
-                                    : SpaceBytes<double>(bin.slots, false);
-    const size_t smem = per_warp * bin.warps;
-    SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    const size_t smem = HashRowSetBytes(bin.slots) * bin.warps;
+    SPAI_CUDA(cudaFuncSetAttribute(HashRowSetKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(smem)));
     const int threads = bin.warps * kWarp;
-    const int grid = GridFor(cols * kWarp, threads);
     args.global_space = nullptr;
-    kernel<<<grid, threads, smem, ctx.stream>>>(args, bin.slots, bin.lo, bin.hi);
+    HashRowSetKernel<T><<<GridFor(hash_columns * kWarp, threads), threads, smem, ctx.stream>>>(args, bin.slots, bin.lo,
+                                                                                            bin.hi);
     SPAI_LAUNCH_CHECK();
   }
-  if (max_need > kLargestBin) {
+  if (max_need > kLargestHashBin) {
     const int slots = NextPow2(max_need);
-    const size_t per_warp = numeric ? (tsize == 8 ? SpaceBytes<double>(slots, true) : SpaceBytes<float>(slots, true))
-                                    : SpaceBytes<double>(slots, false);
     const int blocks = ctx.sm_count * 2;
-    fallback.Reserve(per_warp * blocks, ctx.stream);
-    args.global_space = fallback.data();
-    kernel<<<blocks, kWarp, 0, ctx.stream>>>(args, slots, kLargestBin, INT64_MAX);
+    ctx.sg_fallback.Reserve(HashRowSetBytes(slots) * blocks, ctx.stream);
+    args.global_space = ctx.sg_fallback.data();
+    HashRowSetKernel<T><<<blocks, kWarp, 0, ctx.stream>>>(args, slots, kLargestHashBin, INT64_MAX);
     SPAI_LAUNCH_CHECK();
   }
 }
@@ -588,110 +629,120 @@ double MatrixBytes(int64_t nnz, int64_t major) {
 }  // namespace
 
 template <class T>
-void Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevCsc<T>& b, DevCsc<T>& c,
+bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevCsc<T>& b, DevCsc<T>& c,
             Epilogue epilogue, SpgemmExtras extras, DevCsc<T>* c_z) {
   const int64_t cols = b.cols;
   const bool residual = epilogue == Epilogue::kResidual;
   const bool projection = epilogue == Epilogue::kProjection;
-  DevBuf<int64_t> ub;
-  DevBuf<int64_t> need;
-  DevBuf<int64_t> counts;
-  DevBuf<unsigned long long> maxima;
-  DevBuf<unsigned char> fallback;
-  ub.Reserve(static_cast<size_t>(cols), ctx.stream);
-  need.Reserve(static_cast<size_t>(cols), ctx.stream);
-  counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
-  maxima.Reserve(4, ctx.stream);
-  SPAI_CUDA(cudaMemsetAsync(maxima.data(), 0, 4 * sizeof(unsigned long long), ctx.stream));
-
-  NeedKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(View(x_csc), View(b), residual, ub.data(), maxima.data());
+  ctx.sg_need.Reserve(static_cast<size_t>(cols), ctx.stream);
+  ctx.sg_counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+  ctx.sg_win_lo.Reserve(static_cast<size_t>(cols), ctx.stream);
+  ctx.sg_win_words.Reserve(static_cast<size_t>(cols), ctx.stream);
+  ctx.sg_maxima.Reserve(kMaximaSlots, ctx.stream);
+  SPAI_CUDA(cudaMemsetAsync(ctx.sg_maxima.data(), 0, kMaximaSlots * sizeof(unsigned long long), ctx.stream));
+  NeedKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(View(x_csc), View(b), residual, ctx.sg_need.data(),
+                                                           ctx.sg_win_lo.data(), ctx.sg_win_words.data(),
+                                                           ctx.sg_maxima.data());
   SPAI_LAUNCH_CHECK();
-  SymbolicNeedKernel<<<GridFor(cols, 256), 256, 0, ctx.stream>>>(ub.data(), cols, need.data());
-  SPAI_LAUNCH_CHECK();
-  unsigned long long host_max[4];
-  SPAI_CUDA(cudaMemcpyAsync(host_max, maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
+  unsigned long long host_max[kMaximaSlots];
+  SPAI_CUDA(cudaMemcpyAsync(host_max, ctx.sg_maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
   ctx.Sync();
-  const int64_t max_sym_need = 2 * static_cast<int64_t>(host_max[0]);
 
-  SymbolicArgs<T> sargs{View(x_csc), View(b), need.data(), residual, counts.data(), nullptr};
+  RowSetArgs<T> rs{};
+  rs.x = View(x_csc);
+  rs.b = View(b);
+  rs.need = ctx.sg_need.data();
+  rs.win_lo = ctx.sg_win_lo.data();
+  rs.win_words = ctx.sg_win_words.data();
+  rs.add_diag = residual;
+  rs.counts = ctx.sg_counts.data();
   {
     prof::Scope scope(ctx.stream, "spgemm_symbolic", 0.0);
-    LaunchBins(ctx, SymbolicKernel<T>, sargs, cols, max_sym_need, false, sizeof(T), fallback);
+    rs.list = false;
+    LaunchRowSets(ctx, rs, host_max);
   }
 
-  NumericNeedKernel<<<GridFor(cols, 256), 256, 0, ctx.stream>>>(counts.data(), b.ptr.data(), cols, need.data(),
-                                                                maxima.data());
-  SPAI_LAUNCH_CHECK();
-
+  // output layout: C, or the transient row list of the projection
   DevCsc<T> result;
-  DevBuf<T> zbuf;
-  DevBuf<int64_t> kept;
-  NumericArgs<T> nargs{};
-  nargs.x_csc = View(x_csc);
-  nargs.x_csr = View(x_csr);
-  nargs.b = View(b);
-  nargs.need = need.data();
-  nargs.epilogue = static_cast<int>(epilogue);
-  nargs.row_scale = static_cast<const T*>(extras.row_scale);
-  nargs.col_squares = extras.col_squares;
-  nargs.proj_tt = extras.proj_tt;
-  nargs.proj_bt = extras.proj_bt;
-  nargs.flag = ctx.flags.data();
-  SPAI_CUDA(cudaMemsetAsync(ctx.flags.data(), 0, sizeof(int32_t), ctx.stream));
-  int64_t nnz = 0;
-  if (!projection) {
+  int64_t* c_ptr;
+  if (projection) {
+    ctx.sg_proj_ptr.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+    c_ptr = ctx.sg_proj_ptr.data();
+  } else {
     result.Shape(x_csc.rows, cols, ctx.stream);
-    nnz = ScanCounts(ctx, counts.data(), cols, result.ptr.data());
-    result.ReserveNnz(nnz, ctx.stream);
-    kept.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
-    nargs.c_ptr = result.ptr.data();
-    nargs.c_idx = result.idx.data();
-    nargs.c_val = result.val.data();
-    nargs.kept = kept.data();
-    if (extras.z_val != nullptr || c_z != nullptr) {
-      zbuf.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
-      nargs.z_val = zbuf.data();
-    }
+    c_ptr = result.ptr.data();
   }
-  SPAI_CUDA(cudaMemcpyAsync(host_max, maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
-  ctx.Sync();
-  const int64_t max_num_need = static_cast<int64_t>(host_max[2]);
+  const int64_t nnz = ScanCounts(ctx, ctx.sg_counts.data(), cols, c_ptr);
+  int32_t* rows;
+  T* vals;
+  if (projection) {
+    ctx.sg_proj_rows.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
+    ctx.sg_proj_vals.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1) * sizeof(T), ctx.stream);
+    rows = ctx.sg_proj_rows.data();
+    vals = reinterpret_cast<T*>(ctx.sg_proj_vals.data());
+  } else {
+    result.ReserveNnz(nnz, ctx.stream);
+    rows = result.idx.data();
+    vals = result.val.data();
+  }
+  ctx.sg_cols.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
+  DevBuf<T> zbuf;
+  const bool want_z = residual && extras.row_scale != nullptr && c_z != nullptr;
+  if (want_z) zbuf.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
+  const bool prune = epilogue == Epilogue::kPruneZeros || residual;
+  SPAI_CUDA(cudaMemsetAsync(ctx.flags.data(), 0, sizeof(int32_t), ctx.stream));
   {
-    // algorithmic bytes: |X| + |B| + |C| (C written; the projection writes two per-column sums instead)
+    // algorithmic bytes: |X| + |B| + |C| (the projection writes per-column sums instead of C)
     double bytes = MatrixBytes<T>(x_csr.nnz, x_csr.cols) + MatrixBytes<T>(b.nnz, b.cols);
     if (projection) {
       bytes += static_cast<double>(cols) * (sizeof(T) + 2 * sizeof(double));
     } else {
       bytes += MatrixBytes<T>(nnz, cols);
-      if (nargs.z_val != nullptr) bytes += static_cast<double>(nnz) * sizeof(T);
+      if (want_z) bytes += static_cast<double>(nnz) * sizeof(T);
+      if (extras.col_squares != nullptr) bytes += static_cast<double>(cols) * sizeof(double);
     }
     prof::Scope scope(ctx.stream, "spgemm_numeric", bytes);
-    LaunchBins(ctx, NumericKernel<T>, nargs, cols, max_num_need, true, sizeof(T), fallback);
+    rs.list = true;
+    rs.c_ptr = c_ptr;
+    rs.rows = rows;
+    rs.cols = ctx.sg_cols.data();
+    LaunchRowSets(ctx, rs, host_max);
+    ValuesArgs<T> va{};
+    va.x_csr = View(x_csr);
+    va.b = View(b);
+    va.rows = rows;
+    va.cols = ctx.sg_cols.data();
+    va.count = nnz;
+    va.mode = static_cast<int>(residual ? ValueMode::kResidual
+                                        : (projection ? ValueMode::kProjection : ValueMode::kStore));
+    va.prune = prune;
+    va.out = vals;
+    va.z_out = want_z ? zbuf.data() : nullptr;
+    va.row_scale = static_cast<const T*>(extras.row_scale);
+    va.flag = ctx.flags.data();
+    if (nnz > 0) {
+      ValuesKernel<T><<<GridFor(nnz, 256), 256, 0, ctx.stream>>>(va);
+      SPAI_LAUNCH_CHECK();
+    }
+    if (projection || extras.col_squares != nullptr) {
+      SumsArgs<T> sa{c_ptr, rows, vals, View(b), projection, extras.col_squares, extras.proj_tt, extras.proj_bt,
+                     cols};
+      ColumnSumsKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(sa);
+      SPAI_LAUNCH_CHECK();
+    }
   }
-  if (projection) {
-    return;
-  }
-  int32_t squeezed = 0;
-  if (epilogue != Epilogue::kPlain) {
+  if (projection) return false;
+  bool z_written = want_z;
+  if (prune) {
     SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags, ctx.flags.data(), sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
     ctx.Sync();
-    squeezed = ctx.host_flags[0];
+    if (ctx.host_flags[0] != 0) {
+      // an exact zero: prune it (Eigen prune(0.0)); the fused Z is dropped and recomputed by the caller
+      DropZeros(ctx, result);
+      z_written = false;
+    }
   }
-  if (squeezed) {
-    DevCsc<T> packed;
-    packed.Shape(result.rows, cols, ctx.stream);
-    const int64_t packed_nnz = ScanCounts(ctx, kept.data(), cols, packed.ptr.data());
-    packed.ReserveNnz(packed_nnz, ctx.stream);
-    DevBuf<T> packed_z;
-    if (nargs.z_val != nullptr) packed_z.Reserve(static_cast<size_t>(packed_nnz > 0 ? packed_nnz : 1), ctx.stream);
-    SqueezeKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(
-        cols, result.ptr.data(), packed.ptr.data(), result.idx.data(), result.val.data(), zbuf.data(),
-        packed.idx.data(), packed.val.data(), nargs.z_val != nullptr ? packed_z.data() : nullptr);
-    SPAI_LAUNCH_CHECK();
-    result.Swap(packed);
-    zbuf.Swap(packed_z);
-  }
-  if (c_z != nullptr) {
+  if (z_written) {
     DevCsc<T> z;
     z.Shape(result.rows, cols, ctx.stream);
     z.ReserveNnz(result.nnz, ctx.stream);
@@ -705,35 +756,31 @@ void Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
     c_z->Swap(z);
   }
   c.Swap(result);
+  return z_written;
 }
 
 template <class T>
 void SpgemmMasked(Ctx& ctx, const DevCsc<T>& x_csr, const DevCsc<T>& b, const DevCsc<T>& mask, double* out) {
-  const int64_t cols = b.cols;
-  DevBuf<int64_t> need;
-  DevBuf<unsigned char> fallback;
-  need.Reserve(static_cast<size_t>(cols), ctx.stream);
-  MaskedNeedKernel<<<GridFor(cols, 256), 256, 0, ctx.stream>>>(b.ptr.data(), cols, need.data());
+  if (mask.nnz == 0) return;
+  ctx.sg_cols.Reserve(static_cast<size_t>(mask.nnz), ctx.stream);
+  ColumnIdsKernel<T><<<GridFor(mask.cols, 128), 128, 0, ctx.stream>>>(View(mask), ctx.sg_cols.data());
   SPAI_LAUNCH_CHECK();
-  // the largest B column decides whether the global workspace is needed
-  DevBuf<unsigned long long> maxima;
-  maxima.Reserve(4, ctx.stream);
-  SPAI_CUDA(cudaMemsetAsync(maxima.data(), 0, 4 * sizeof(unsigned long long), ctx.stream));
-  DevBuf<int64_t> ub;
-  ub.Reserve(static_cast<size_t>(cols), ctx.stream);
-  NeedKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(View(x_csr), View(b), false, ub.data(), maxima.data());
+  ValuesArgs<T> va{};
+  va.x_csr = View(x_csr);
+  va.b = View(b);
+  va.rows = mask.idx.data();
+  va.cols = ctx.sg_cols.data();
+  va.count = mask.nnz;
+  va.mode = static_cast<int>(ValueMode::kMasked);
+  va.out_f64 = out;
+  va.flag = ctx.flags.data();
+  ValuesKernel<T><<<GridFor(mask.nnz, 256), 256, 0, ctx.stream>>>(va);
   SPAI_LAUNCH_CHECK();
-  unsigned long long host_max[4];
-  SPAI_CUDA(cudaMemcpyAsync(host_max, maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
-  ctx.Sync();
-  const int64_t max_need = std::max<int64_t>(2, 4 * static_cast<int64_t>(host_max[1]));
-  MaskedArgs<T> args{View(x_csr), View(b), View(mask), need.data(), out, nullptr};
-  LaunchBins(ctx, MaskedKernel<T>, args, cols, max_need, true, sizeof(T), fallback);
 }
 
-template void Spgemm<double>(Ctx&, const DevCsc<double>&, const DevCsc<double>&, const DevCsc<double>&,
+template bool Spgemm<double>(Ctx&, const DevCsc<double>&, const DevCsc<double>&, const DevCsc<double>&,
                              DevCsc<double>&, Epilogue, SpgemmExtras, DevCsc<double>*);
-template void Spgemm<float>(Ctx&, const DevCsc<float>&, const DevCsc<float>&, const DevCsc<float>&, DevCsc<float>&,
+template bool Spgemm<float>(Ctx&, const DevCsc<float>&, const DevCsc<float>&, const DevCsc<float>&, DevCsc<float>&,
                             Epilogue, SpgemmExtras, DevCsc<float>*);
 template void SpgemmMasked<double>(Ctx&, const DevCsc<double>&, const DevCsc<double>&, const DevCsc<double>&,
                                    double*);

@@ -25,19 +25,21 @@ enum class Epilogue {
 struct SpgemmExtras {
   // Optional per-column partial sum of squares of the output column (storage order).
   double* col_squares = nullptr;
-  // kResidual only: also write Z = diag(pr) * C with the same pattern into z_val.
-  const void* row_scale = nullptr;  // T* pr
-  void* z_val = nullptr;            // T* (capacity nnz(C)); pattern shared with C
+  // kResidual: Z = diag(row_scale) * C is also written when c_z is given;
+  // kProjection: the row scale pr.
+  const void* row_scale = nullptr;  // const T*
   // kProjection: outputs
   double* proj_tt = nullptr;  // per column sum over rows of (pr_i c_i)^2
   double* proj_bt = nullptr;  // per column sum over rows in both of b_i * (pr_i c_i)
 };
 
 // x_csc and x_csr are the same matrix X in column and row compressed form.
-// The C matrix (when written) replaces `c`.  `c_z` receives Z when
-// extras.z_val is requested (same pattern, separate values).
+// The C matrix (when written) replaces `c`.  For kResidual with
+// extras.row_scale set and c_z given, Z = diag(row_scale) * C is written into
+// c_z as well; the return value says whether it was (it is not when an exact
+// zero had to be pruned from C).
 template <class T>
-void Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevCsc<T>& b, DevCsc<T>& c,
+bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevCsc<T>& b, DevCsc<T>& c,
             Epilogue epilogue, SpgemmExtras extras = SpgemmExtras(), DevCsc<T>* c_z = nullptr);
 
 // Masked product: out[p] = (X*B)(row(p), col(p)) for every entry p of the

@@ -1,0 +1,393 @@
+// Column-merging updates of M on sm_100a, one warp per column.
+//
+// Union (out = ys*Y (+) xs*X, or 0.5*(Y + X)): every lane takes entries of
+// both input columns and computes its output slot directly -- an entry of Y
+// lands at (#Y before it) + (#X rows below it that Y lacks), an entry of X
+// found nowhere in Y at (#unmatched X before it) + (#Y rows below it) -- from
+// binary searches into the other column and a per-column prefix of the
+// matched X entries kept in shared memory.  No serial merge, no sort.
+//
+// SymmetrizeAndDrop fuses the drop step of the global methods
+// (dropping.cpp:106-135, plus the optional per-column top-k): the merged
+// column of 0.5*(M + M^T) is built in shared memory, its 2-norm is summed in
+// row order by one lane (the reference's per-column sequential sum), the
+// relative threshold and the top-k rank rule are applied there, and only the
+// survivors are written.  One launch pair replaces transpose-union,
+// threshold-filter and top-k-filter passes over HBM.
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "device.cuh"
+#include "ops.cuh"
+#include "profile.cuh"
+
+namespace spai {
+
+namespace {
+
+constexpr int kUnionWarpCap = 1024;  // longest X column the warp union takes (shared-memory prefix)
+constexpr int kDropCap = 256;        // longest merged column of the fused drop kernel
+constexpr double kDblEps = 2.220446049250313080847e-16;
+
+__device__ __forceinline__ unsigned LaneMaskBelow() {
+  unsigned mask;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(mask));
+  return mask;
+}
+
+// First position in idx[lo, hi) whose row is >= key.
+__device__ __forceinline__ int64_t LowerBound(const int32_t* idx, int64_t lo, int64_t hi, int32_t key) {
+  while (lo < hi) {
+    const int64_t mid = lo + ((hi - lo) >> 1);
+    if (idx[mid] < key) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+// Values of one merged entry, in the arithmetic of the thread-per-column union.
+__device__ __forceinline__ double Both(double y, double x, bool scale_y, double ys, double xs, bool half_sum) {
+  if (half_sum) return Mul(0.5, Add(y, x));
+  return Add(scale_y ? Mul(ys, y) : y, Mul(xs, x));
+}
+
+__device__ __forceinline__ double LeftOnly(double y, bool scale_y, double ys, bool half_sum) {
+  if (half_sum) return Mul(0.5, Add(y, 0.0));
+  return Add(scale_y ? Mul(ys, y) : y, 0.0);
+}
+
+__device__ __forceinline__ double RightOnly(double x, double xs, bool half_sum) {
+  if (half_sum) return Mul(0.5, Add(0.0, x));
+  return Add(0.0, Mul(xs, x));
+}
+
+// Number of rows of X(:, j) also present in Y(:, j) (warp-uniform).
+template <class T>
+__device__ int64_t CommonRows(const CscView<T>& y, const CscView<T>& x, int64_t j, int lane) {
+  const int64_t ys = y.ptr[j];
+  const int64_t ye = y.ptr[j + 1];
+  const int64_t xs = x.ptr[j];
+  const int64_t xe = x.ptr[j + 1];
+  int64_t matched = 0;
+  for (int64_t base = xs; base < xe; base += kWarp) {
+    const int64_t q = base + lane;
+    bool hit = false;
+    if (q < xe) {
+      const int32_t row = x.idx[q];
+      const int64_t r = LowerBound(y.idx, ys, ye, row);
+      hit = r < ye && y.idx[r] == row;
+    }
+    matched += __popc(__ballot_sync(0xffffffffu, hit));
+  }
+  return matched;
+}
+
+// mx_prefix[i] = number of the first i entries of X(:, j) whose row is in
+// Y(:, j), for i = 0..nx.  Ends with __syncwarp.
+template <class T>
+__device__ void MatchedPrefix(const CscView<T>& y, const CscView<T>& x, int64_t j, int* mx_prefix, int lane) {
+  const int64_t ys = y.ptr[j];
+  const int64_t ye = y.ptr[j + 1];
+  const int64_t xs = x.ptr[j];
+  const int64_t xe = x.ptr[j + 1];
+  int running = 0;
+  for (int64_t base = xs; base < xe; base += kWarp) {
+    const int64_t q = base + lane;
+    bool hit = false;
+    if (q < xe) {
+      const int32_t row = x.idx[q];
+      const int64_t r = LowerBound(y.idx, ys, ye, row);
+      hit = r < ye && y.idx[r] == row;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (q < xe) mx_prefix[q - xs] = running + __popc(mask & LaneMaskBelow());
+    running += __popc(mask);
+  }
+  if (lane == 0) mx_prefix[xe - xs] = running;
+  __syncwarp();
+}
+
+// Calls emit(rank, row, value) for every entry of the merged column j; rank
+// is the entry's position in the merged, row-sorted column.
+template <class T, class Emit>
+__device__ void MergeColumn(const CscView<T>& y, const CscView<T>& x, int64_t j, bool scale_y, double ys_scale,
+                            double xs_scale, bool half_sum, const int* mx_prefix, int lane, Emit emit) {
+  const int64_t ys = y.ptr[j];
+  const int64_t ye = y.ptr[j + 1];
+  const int64_t xs = x.ptr[j];
+  const int64_t xe = x.ptr[j + 1];
+  for (int64_t p = ys + lane; p < ye; p += kWarp) {
+    const int32_t row = y.idx[p];
+    const int64_t r = LowerBound(x.idx, xs, xe, row);
+    const int64_t rank = (p - ys) + (r - xs) - mx_prefix[r - xs];
+    const double yv = static_cast<double>(y.val[p]);
+    double v;
+    if (r < xe && x.idx[r] == row) {
+      v = Both(yv, static_cast<double>(x.val[r]), scale_y, ys_scale, xs_scale, half_sum);
+    } else {
+      v = LeftOnly(yv, scale_y, ys_scale, half_sum);
+    }
+    emit(rank, row, v);
+  }
+  for (int64_t q = xs + lane; q < xe; q += kWarp) {
+    const int32_t row = x.idx[q];
+    const int64_t r = LowerBound(y.idx, ys, ye, row);
+    if (r < ye && y.idx[r] == row) continue;
+    const int64_t qq = q - xs;
+    const int64_t rank = qq - mx_prefix[qq] + (r - ys);
+    emit(rank, row, RightOnly(static_cast<double>(x.val[q]), xs_scale, half_sum));
+  }
+}
+
+template <class T>
+__global__ void UnionCountWarpKernel(CscView<T> y, CscView<T> x, int64_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = warp; j < y.cols; j += warps) {
+    const int64_t nx = x.ptr[j + 1] - x.ptr[j];
+    if (nx > kUnionWarpCap) continue;  // the thread-per-column kernel takes it
+    const int64_t ny = y.ptr[j + 1] - y.ptr[j];
+    const int64_t matched = CommonRows(y, x, j, lane);
+    if (lane == 0) counts[j] = ny + nx - matched;
+  }
+}
+
+template <class T>
+__global__ void UnionWriteWarpKernel(CscView<T> y, CscView<T> x, bool scale_y, double ys, double xs, bool half_sum,
+                                     bool prune, const int64_t* __restrict__ out_ptr, int32_t* __restrict__ out_idx,
+                                     T* __restrict__ out_val, int32_t* __restrict__ flag) {
+  extern __shared__ int union_smem[];
+  const int lane = threadIdx.x & 31;
+  int* mx_prefix = union_smem + (threadIdx.x >> 5) * (kUnionWarpCap + 1);
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  bool zero_seen = false;
+  for (int64_t j = warp; j < y.cols; j += warps) {
+    const int64_t nx = x.ptr[j + 1] - x.ptr[j];
+    if (nx > kUnionWarpCap) continue;
+    MatchedPrefix(y, x, j, mx_prefix, lane);
+    const int64_t base = out_ptr[j];
+    MergeColumn(y, x, j, scale_y, ys, xs, half_sum, mx_prefix, lane, [&](int64_t rank, int32_t row, double v) {
+      const T stored = static_cast<T>(v);
+      out_idx[base + rank] = row;
+      out_val[base + rank] = stored;
+      if (prune && fabs(static_cast<double>(stored)) <= 0.0) zero_seen = true;
+    });
+    __syncwarp();
+  }
+  if (__any_sync(0xffffffffu, zero_seen) && lane == 0) atomicOr(flag, 1);
+}
+
+// Per-warp shared memory of the fused drop kernel.
+struct DropSlab {
+  double* vals;
+  int32_t* keys;
+  int* mx_prefix;
+  unsigned char* keep;
+};
+
+__host__ __device__ constexpr size_t DropSlabBytes() {
+  return ((kDropCap * sizeof(double) + 15) & ~size_t(15)) + ((kDropCap * sizeof(int32_t) + 15) & ~size_t(15)) +
+         (((kDropCap + 1) * sizeof(int) + 15) & ~size_t(15)) + ((kDropCap + 15) & ~size_t(15));
+}
+
+__device__ DropSlab SlabFor(unsigned char* base) {
+  DropSlab s;
+  s.vals = reinterpret_cast<double*>(base);
+  base += (kDropCap * sizeof(double) + 15) & ~size_t(15);
+  s.keys = reinterpret_cast<int32_t*>(base);
+  base += (kDropCap * sizeof(int32_t) + 15) & ~size_t(15);
+  s.mx_prefix = reinterpret_cast<int*>(base);
+  base += ((kDropCap + 1) * sizeof(int) + 15) & ~size_t(15);
+  s.keep = base;
+  return s;
+}
+
+// Count pass (write == false): counts[j] = survivors of column j, overflow
+// set when a column exceeds kDropCap.  Write pass: the survivors in row order.
+template <class T>
+__global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric, int64_t topk, bool write,
+                                     int64_t* __restrict__ counts, const int64_t* __restrict__ out_ptr,
+                                     int32_t* __restrict__ out_idx, T* __restrict__ out_val,
+                                     int32_t* __restrict__ overflow) {
+  extern __shared__ __align__(16) unsigned char drop_smem[];
+  const int lane = threadIdx.x & 31;
+  DropSlab s = SlabFor(drop_smem + (threadIdx.x >> 5) * DropSlabBytes());
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = warp; j < m.cols; j += warps) {
+    const int64_t ny = m.ptr[j + 1] - m.ptr[j];
+    int count;
+    if (symmetric) {
+      const int64_t nx = mt.ptr[j + 1] - mt.ptr[j];
+      if (nx > kDropCap || ny > kDropCap) {
+        if (lane == 0) atomicOr(overflow, 1);
+        continue;
+      }
+      const int64_t merged = ny + nx - CommonRows(m, mt, j, lane);
+      if (merged > kDropCap) {
+        if (lane == 0) atomicOr(overflow, 1);
+        continue;
+      }
+      count = static_cast<int>(merged);
+      MatchedPrefix(m, mt, j, s.mx_prefix, lane);
+      MergeColumn(m, mt, j, false, 1.0, 1.0, true, s.mx_prefix, lane, [&](int64_t rank, int32_t row, double v) {
+        s.keys[rank] = row;
+        s.vals[rank] = static_cast<double>(static_cast<T>(v));  // the value M would store
+      });
+    } else {
+      if (ny > kDropCap) {
+        if (lane == 0) atomicOr(overflow, 1);
+        continue;
+      }
+      count = static_cast<int>(ny);
+      const int64_t base = m.ptr[j];
+      for (int i = lane; i < count; i += kWarp) {
+        s.keys[i] = m.idx[base + i];
+        s.vals[i] = static_cast<double>(m.val[base + i]);
+      }
+    }
+    __syncwarp();
+    // relative threshold: eps * ||M(:, j)||_2, summed in row order
+    double thr = 0.0;
+    if (lane == 0) {
+      double sq = 0.0;
+      for (int i = 0; i < count; ++i) sq = Add(sq, Mul(s.vals[i], s.vals[i]));
+      thr = Mul(kDblEps, sqrt(sq));
+    }
+    thr = __shfl_sync(0xffffffffu, thr, 0);
+    int kept = 0;
+    bool has_diag = false;
+    for (int base = 0; base < count; base += kWarp) {
+      const int i = base + lane;
+      bool keep = false;
+      bool diag = false;
+      if (i < count) {
+        const double v = s.vals[i];
+        diag = static_cast<int64_t>(s.keys[i]) == j;
+        keep = v != 0.0 && (diag || fabs(v) >= thr);
+        s.keep[i] = keep ? 1 : 0;
+      }
+      kept += __popc(__ballot_sync(0xffffffffu, keep));
+      if (__any_sync(0xffffffffu, keep && diag)) has_diag = true;
+    }
+    __syncwarp();
+    if (topk > 0 && kept > topk) {
+      // drop the `drop` smallest (|v|, row) among the kept off-diagonal entries
+      const int64_t candidates = kept - (has_diag ? 1 : 0);
+      const int64_t keep_off = topk - (has_diag ? 1 : 0) > 0 ? topk - (has_diag ? 1 : 0) : 0;
+      const int64_t drop = candidates - keep_off;
+      if (drop > 0) {
+        bool dropped_any[kDropCap / kWarp] = {};
+        for (int base = 0, r = 0; base < count; base += kWarp, ++r) {
+          const int i = base + lane;
+          if (i >= count || !s.keep[i] || static_cast<int64_t>(s.keys[i]) == j) continue;
+          const double a = fabs(s.vals[i]);
+          const int32_t row = s.keys[i];
+          int64_t rank = 0;
+          for (int q = 0; q < count; ++q) {
+            if (!s.keep[q] || static_cast<int64_t>(s.keys[q]) == j) continue;
+            const double aq = fabs(s.vals[q]);
+            rank += (aq < a || (aq == a && s.keys[q] < row)) ? 1 : 0;
+          }
+          dropped_any[r] = rank < drop;
+        }
+        __syncwarp();
+        for (int base = 0, r = 0; base < count; base += kWarp, ++r) {
+          const int i = base + lane;
+          if (i < count && dropped_any[r]) s.keep[i] = 0;
+        }
+        __syncwarp();
+        kept -= static_cast<int>(drop);
+      }
+    }
+    if (!write) {
+      if (lane == 0) counts[j] = kept;
+    } else {
+      int64_t out = out_ptr[j];
+      for (int base = 0; base < count; base += kWarp) {
+        const int i = base + lane;
+        const bool keep = i < count && s.keep[i] != 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int64_t o = out + __popc(mask & LaneMaskBelow());
+          out_idx[o] = s.keys[i];
+          out_val[o] = static_cast<T>(s.vals[i]);
+        }
+        out += __popc(mask);
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+int UnionWarpCap() { return kUnionWarpCap; }
+
+template <class T>
+void UnionCountWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, int64_t* counts) {
+  UnionCountWarpKernel<T><<<GridFor(y.cols * kWarp, 256), 256, 0, ctx.stream>>>(View(y), View(x), counts);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+void UnionWriteWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, bool scale_y, double ys, double xs, bool half_sum,
+                    bool prune, DevCsc<T>& out, int32_t* flag) {
+  constexpr int kWarps = 8;
+  const size_t smem = static_cast<size_t>(kWarps) * (kUnionWarpCap + 1) * sizeof(int);
+  UnionWriteWarpKernel<T><<<GridFor(y.cols * kWarp, kWarps * kWarp), kWarps * kWarp, smem, ctx.stream>>>(
+      View(y), View(x), scale_y, ys, xs, half_sum, prune, out.ptr.data(), out.idx.data(), out.val.data(), flag);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk) {
+  prof::Scope scope(ctx.stream, "drop_update", 0.0);
+  const int64_t cols = m.cols;
+  DevCsc<T> mt;
+  if (symmetric) Transpose(ctx, m, mt);
+  const CscView<T> mt_view = symmetric ? View(mt) : View(m);
+  constexpr int kWarps = 8;
+  const size_t smem = DropSlabBytes() * kWarps;
+  SPAI_CUDA(cudaFuncSetAttribute(SymmetrizeDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+  const int grid = GridFor(cols * kWarp, kWarps * kWarp);
+  ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+  int32_t* overflow = ctx.flags.data() + 1;
+  SPAI_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int32_t), ctx.stream));
+  SymmetrizeDropKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(m), mt_view, symmetric, topk, false,
+                                                                      ctx.counts.data(), nullptr, nullptr, nullptr,
+                                                                      overflow);
+  SPAI_LAUNCH_CHECK();
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 1, overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.Sync();
+  if (ctx.host_flags[1] != 0) return false;
+  DevCsc<T> out;
+  out.Shape(m.rows, cols, ctx.stream);
+  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());
+  out.ReserveNnz(nnz, ctx.stream);
+  SymmetrizeDropKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(m), mt_view, symmetric, topk, true, nullptr,
+                                                                      out.ptr.data(), out.idx.data(), out.val.data(),
+                                                                      overflow);
+  SPAI_LAUNCH_CHECK();
+  m.Swap(out);
+  return true;
+}
+
+template void UnionCountWarp<double>(Ctx&, const DevCsc<double>&, const DevCsc<double>&, int64_t*);
+template void UnionCountWarp<float>(Ctx&, const DevCsc<float>&, const DevCsc<float>&, int64_t*);
+template void UnionWriteWarp<double>(Ctx&, const DevCsc<double>&, const DevCsc<double>&, bool, double, double, bool,
+                                     bool, DevCsc<double>&, int32_t*);
+template void UnionWriteWarp<float>(Ctx&, const DevCsc<float>&, const DevCsc<float>&, bool, double, double, bool, bool,
+                                    DevCsc<float>&, int32_t*);
+template bool SymmetrizeAndDrop<double>(Ctx&, DevCsc<double>&, bool, int64_t);
+template bool SymmetrizeAndDrop<float>(Ctx&, DevCsc<float>&, bool, int64_t);
+
+}  // namespace spai

@@ -65,3 +65,36 @@ def test_fp64_topk_matches_oracle(require_gpu, family, name):
     got, want = _run_both(family, name, A, M0, None, topk=5, max_iterations=8, tolerance=1e-12, max_density=0.05)
     assert_same_result(got, want, f"{family}.{name} top-5")
     assert np.diff(got.M.indptr).max() <= 5
+
+
+@pytest.mark.parametrize("family,name", [("global_spai", "mr"), ("global_spai", "cg"), ("inner_outer", "lomr")])
+@pytest.mark.parametrize("topk", [0, 6])
+def test_fp64_wide_windows_hash_path(require_gpu, family, name, topk):
+    # random long-range couplings: row windows wider than the bitmap kernels take
+    A = problems.random_banded_spd(70_000, half_width=2, extra=2, seed=4)
+    M0 = problems.diagonal_inverse(A)
+    got, want = _run_both(family, name, A, M0, None, topk=topk, max_iterations=2, tolerance=1e-12,
+                          max_density=6.0 / A.shape[0])
+    assert_same_result(got, want, f"{family}.{name} wide top-{topk}")
+
+
+def _arrow(n):
+    """SPD arrow matrix: a dense first row and column over a diagonal."""
+    from scipy import sparse
+    rng = np.random.default_rng(11)
+    off = rng.uniform(0.1, 1.0, n - 1) / np.sqrt(n)
+    rows = np.concatenate([np.arange(1, n), np.zeros(n - 1, dtype=np.int64), np.arange(n)])
+    cols = np.concatenate([np.zeros(n - 1, dtype=np.int64), np.arange(1, n), np.arange(n)])
+    vals = np.concatenate([off, off, np.full(n, 4.0)])
+    a = sparse.csc_matrix((vals, (rows, cols)), shape=(n, n))
+    a.sort_indices()
+    return a
+
+
+@pytest.mark.parametrize("family,name", METHODS)
+def test_fp64_long_columns_fallbacks(require_gpu, family, name):
+    # a column of n entries: longer than the fused drop kernel and the warp union take
+    A = _arrow(1500)
+    M0 = problems.diagonal_inverse(A)
+    got, want = _run_both(family, name, A, M0, None, max_iterations=3, tolerance=1e-14, max_density=0.5)
+    assert_same_result(got, want, f"{family}.{name} arrow")
