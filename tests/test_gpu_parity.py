@@ -7,7 +7,7 @@ import pytest
 
 from oracle import pyoracle
 from parallellocallyoptimalapproximatesparsematrixinverses_b200 import global_spai, inner_outer, problems
-from tests.helpers import METHODS, assert_same_result
+from tests.helpers import METHODS, assert_same_result, relative_difference
 
 pytestmark = pytest.mark.gpu
 
@@ -98,3 +98,25 @@ def test_fp64_long_columns_fallbacks(require_gpu, family, name):
     M0 = problems.diagonal_inverse(A)
     got, want = _run_both(family, name, A, M0, None, max_iterations=3, tolerance=1e-14, max_density=0.5)
     assert_same_result(got, want, f"{family}.{name} arrow")
+
+
+@pytest.mark.parametrize("family,name", METHODS)
+@pytest.mark.parametrize("topk", [0, 8])
+def test_mixed_precision_error_against_fp64_oracle(require_gpu, family, name, topk):
+    """FP32 storage of A, M, R, Z with FP64 reductions, against the FP64 oracle:
+    ||R||_F histories within 1e-4 relative at every iteration and
+    ||M_mixed - M_fp64||_F / ||M_fp64||_F within 1e-4 (f32 unit roundoff is 6e-8)."""
+    A = problems.diffusion_2d(32, 1.0, 7)
+    M0 = problems.diagonal_inverse(A)
+    kw = dict(max_iterations=10, tolerance=1e-12, max_density=8.0 / A.shape[0])
+    method = getattr(FAMILIES[family], name)
+    ext = {"topk_per_column": topk} if topk else {}
+    got = method(A, M0=M0, precision="mixed", **kw, **ext)
+    want = pyoracle.run(family, name, A, M0=M0, order=pyoracle.ORDER_DEVICE, topk_per_column=topk, **kw)
+    gh = got.history["residual_norm"]
+    wh = want.history["residual_norm"]
+    assert gh.shape == wh.shape
+    hist_err = float(np.max(np.abs(gh - wh) / wh))
+    m_err = relative_difference(got.M, want.M)
+    assert hist_err <= 1e-4, f"{family}.{name} top-{topk}: history rel error {hist_err:.3e}"
+    assert m_err <= 1e-4, f"{family}.{name} top-{topk}: M rel error {m_err:.3e}"
