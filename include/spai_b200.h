@@ -105,6 +105,30 @@ int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, co
                  PcgParams params, double* history, int64_t* status, double* x_out, char* error,
                  int64_t error_capacity);
 
+/* PCG on DEVICE buffers that allocates no memory.  No counterpart in the
+ * reference: it is spai_pcg (FP64 M, same arithmetic, same bits) for callers
+ * that cannot let a library allocate -- a solver loop that has given the
+ * device's memory to its own pool, or one that must not stall other streams
+ * through cudaMalloc/cudaFree.
+ *   A and M: CSR on the current device, int64 offsets (n + 1), int32 column
+ *   indices and FP64 values (nnz each); b and x: n doubles on the device
+ *   (x is overwritten, x0 = 0); history: max_iterations host doubles.
+ *   stream: the cudaStream_t to run on (NULL: the default stream).
+ * Work vectors live in a fixed device array inside the library (16 MiB), so
+ * n is limited to 524,288 rows; larger n returns -1 with an error.  The
+ * array's address is looked up on the first call on each device, so make
+ * that first call before any stream capture on the device.  Calls that
+ * overlap on one GPU share the array and race: serialise them per device.
+ * Pointers are checked (device memory of the current device, long enough),
+ * offsets and indices are checked on the device.  Returns the number of
+ * history entries and sets *status as spai_pcg does; -1 with `error` on
+ * invalid input or CUDA failure. */
+int64_t spai_pcg_device_noalloc(int64_t n, int64_t a_nnz, const double* a_values, const int32_t* a_indices,
+                                const int64_t* a_offsets, int64_t m_nnz, const double* m_values,
+                                const int32_t* m_indices, const int64_t* m_offsets, const double* b, double* x,
+                                int64_t max_iterations, double tolerance, int64_t refresh_period, void* stream,
+                                double* history, int64_t* status, char* error, int64_t error_capacity);
+
 /* y = A x for CSR A (backward_error.pyx:56-66 `matvec`); returns 0, or -1 with `error`. */
 int64_t spai_matvec(int64_t n, const double* values, const int64_t* indices, const int64_t* offsets,
                     const double* x, double* y, int64_t device, char* error, int64_t error_capacity);

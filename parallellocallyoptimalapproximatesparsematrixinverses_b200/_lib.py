@@ -81,7 +81,7 @@ EXPORTED_SYMBOLS = (
     "spai_run_ex", "spai_pcg", "spai_matvec", "spai_session_create", "spai_session_run", "spai_session_history",
     "spai_session_result", "spai_session_set_rhs", "spai_session_pcg", "spai_session_destroy",
     "spai_kernel_launches", "spai_session_stream", "spai_profile_enable", "spai_profile_reset",
-    "spai_profile_read",
+    "spai_profile_read", "spai_pcg_device_noalloc",
 )
 
 _lib = None
@@ -128,6 +128,12 @@ def _declare(lib) -> None:
     lib.spai_profile_reset.argtypes = []
     lib.spai_profile_read.restype = _i64
     lib.spai_profile_read.argtypes = [ctypes.c_char_p, _pf64, _pi64, _pf64]
+    # device pointers are passed as integers (e.g. torch.Tensor.data_ptr())
+    lib.spai_pcg_device_noalloc.restype = _i64
+    lib.spai_pcg_device_noalloc.argtypes = [_i64, _i64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _i64,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                            ctypes.c_void_p, _i64, _f64, _i64, ctypes.c_void_p, _pf64, _pi64,
+                                            ctypes.c_char_p, _i64]
 
 
 def load():
