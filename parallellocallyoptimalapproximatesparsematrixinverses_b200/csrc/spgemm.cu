@@ -491,6 +491,246 @@ __global__ void ColumnSumsKernel(SumsArgs<T> a) {
 }
 
 // ---------------------------------------------------------------------------
+// Column path: stages 1-4 in one warp-per-column kernel for every column
+// whose row window fits the bitmap bins.  Per column, in shared memory:
+//   * B(:,j) in an open-addressing hash (row -> value);
+//   * the output rows in a two-level window bitmap (a summary bit per
+//     non-empty 32-row word), read back in ascending order and cleared while
+//     it is read, so a column never pays for the empty part of its window;
+// then lane r takes output rows r, r+32, ...: walks row i of X (CSR) in
+// ascending k, looks each k up in the hash and accumulates the products in
+// that order (acc starts at -0.0, so the first addition yields the first
+// product exactly: the same bits as "first product, then +=").  Per-column
+// sums are sequential in row order (lane 0 over a 32-entry staging buffer).
+// In count mode the kernel stops after the row set and writes its size.
+constexpr int kColumnRowsMax = 2048;   // largest output column (upper bound) the column path takes
+constexpr int kColumnHashMaxKeys = 1024;
+
+template <class T>
+struct ColumnArgs {
+  CscView<T> x;      // X by columns: candidate rows
+  CscView<T> x_csr;  // X by rows: products in ascending k
+  CscView<T> b;
+  const int32_t* win_lo;
+  const int32_t* win_words;
+  bool add_diag;
+  bool count_only;   // write counts[j] = |row set| and stop
+  int64_t* counts;
+  int mode;          // ValueMode: kStore, kResidual or kProjection
+  bool prune;
+  const int64_t* c_ptr;
+  int32_t* c_idx;
+  T* c_val;
+  T* z_val;             // kResidual: Z = pr * R (optional)
+  const T* row_scale;   // pr
+  double* col_squares;  // optional per-column sum of squares of C
+  double* proj_tt;
+  double* proj_bt;
+  int32_t* flag;
+};
+
+__host__ __device__ inline int SummaryWords(int words) { return (words + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp; }
+
+__host__ __device__ inline size_t ColumnSlabBytes(int words, int rows_cap, int hash_slots, size_t value_size) {
+  return Round16(static_cast<size_t>(words) * 4) + Round16(static_cast<size_t>(SummaryWords(words)) * 4) +
+         Round16(static_cast<size_t>(rows_cap) * 4) + Round16(static_cast<size_t>(hash_slots) * 4) +
+         Round16(static_cast<size_t>(hash_slots) * value_size) + 2 * Round16(kWarp * sizeof(double));
+}
+
+template <class T>
+__device__ __forceinline__ bool HashFind(const int32_t* keys, const T* vals, int bits, int32_t key, T& out) {
+  const uint32_t mask = (1u << bits) - 1u;
+  uint32_t h = Slot(key, bits);
+  while (true) {
+    const int32_t k = keys[h];
+    if (k == key) {
+      out = vals[h];
+      return true;
+    }
+    if (k == kEmpty) return false;
+    h = (h + 1u) & mask;
+  }
+}
+
+// Marks `off` in the two-level bitmap.
+__device__ __forceinline__ void MarkRow(uint32_t* bm, uint32_t* summary, int off) {
+  const int w = off >> 5;
+  const uint32_t old = atomicOr(&bm[w], 1u << (off & 31));
+  if (old == 0u) atomicOr(&summary[w >> 5], 1u << (w & 31));
+}
+
+// Reads the marked rows back in ascending order (into rows[] unless null),
+// clearing both levels; returns the warp-uniform count.
+__device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, int32_t lo, int32_t* rows, int lane) {
+  int total = 0;
+  for (int s0 = 0; s0 < summary_words; s0 += kWarp) {
+    const int s = s0 + lane;
+    const uint32_t sbits = summary[s];
+    int local = 0;
+    for (uint32_t t = sbits; t != 0u; t &= t - 1u) local += __popc(bm[(s << 5) + __ffs(t) - 1]);
+    int inclusive = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, inclusive, o);
+      if (lane >= o) inclusive += y;
+    }
+    int at = total + inclusive - local;
+    for (uint32_t t = sbits; t != 0u; t &= t - 1u) {
+      const int w = (s << 5) + __ffs(t) - 1;
+      uint32_t bits = bm[w];
+      bm[w] = 0u;
+      if (rows != nullptr) {
+        for (; bits != 0u; bits &= bits - 1u) rows[at++] = lo + (w << 5) + (__ffs(bits) - 1);
+      }
+    }
+    summary[s] = 0u;
+    total += __shfl_sync(0xffffffffu, inclusive, 31);
+  }
+  __syncwarp();
+  return total;
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int words_cap, int lo_words, int hi_words,
+                                                           int rows_cap, int hash_slots) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  const int lane = threadIdx.x & 31;
+  const int summary_cap = SummaryWords(words_cap);
+  unsigned char* base = smem + (threadIdx.x >> 5) * ColumnSlabBytes(words_cap, rows_cap, hash_slots, sizeof(T));
+  uint32_t* bm = reinterpret_cast<uint32_t*>(base);
+  base += Round16(static_cast<size_t>(words_cap) * 4);
+  uint32_t* summary = reinterpret_cast<uint32_t*>(base);
+  base += Round16(static_cast<size_t>(summary_cap) * 4);
+  int32_t* rows = reinterpret_cast<int32_t*>(base);
+  base += Round16(static_cast<size_t>(rows_cap) * 4);
+  int32_t* hkeys = reinterpret_cast<int32_t*>(base);
+  base += Round16(static_cast<size_t>(hash_slots) * 4);
+  T* hvals = reinterpret_cast<T*>(base);
+  base += Round16(static_cast<size_t>(hash_slots) * sizeof(T));
+  double* stage0 = reinterpret_cast<double*>(base);
+  double* stage1 = stage0 + kWarp;
+  const int hbits = Log2(hash_slots);
+  const bool projection = a.mode == static_cast<int>(ValueMode::kProjection);
+  const bool residual = a.mode == static_cast<int>(ValueMode::kResidual);
+  const bool sums = projection || a.col_squares != nullptr;
+  // both bitmap levels start clear and are left clear by DrainRows
+  ClearWords(bm, words_cap, lane);
+  ClearWords(summary, summary_cap, lane);
+  __syncwarp();
+  bool zero_seen = false;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t col = warp; col < a.b.cols; col += warps) {
+    const int words = a.win_words[col];
+    if (words <= lo_words || words > hi_words) continue;
+    const int32_t lo = a.win_lo[col];
+    const int64_t bs = a.b.ptr[col];
+    const int64_t be = a.b.ptr[col + 1];
+    if (!a.count_only) {
+      ClearTable(hkeys, hash_slots, lane);
+      __syncwarp();
+      for (int64_t p = bs + lane; p < be; p += kWarp) {
+        const int32_t k = a.b.idx[p];
+        const T v = a.b.val[p];
+        const uint32_t mask = (1u << hbits) - 1u;
+        uint32_t h = Slot(k, hbits);
+        while (atomicCAS(&hkeys[h], kEmpty, k) != kEmpty) h = (h + 1u) & mask;  // B's rows are distinct
+        hvals[h] = v;
+      }
+    }
+    if (a.add_diag && lane == 0) MarkRow(bm, summary, static_cast<int>(col) - lo);
+    for (int64_t p = bs + lane; p < be; p += kWarp) {
+      const int32_t k = a.b.idx[p];
+      const int64_t xs = a.x.ptr[k];
+      const int64_t xe = a.x.ptr[k + 1];
+      for (int64_t q0 = xs; q0 < xe; q0 += 8) {
+        int32_t r8[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) r8[u] = q0 + u < xe ? a.x.idx[q0 + u] : -1;
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          if (r8[u] >= 0) MarkRow(bm, summary, r8[u] - lo);
+        }
+      }
+    }
+    __syncwarp();
+    const int count = DrainRows(bm, summary, SummaryWords(words), lo, a.count_only ? nullptr : rows, lane);
+    if (a.count_only) {
+      if (lane == 0) a.counts[col] = count;
+      continue;
+    }
+    const int64_t c0 = projection ? 0 : a.c_ptr[col];
+    double sq = 0.0;
+    double tt = 0.0;
+    double bt = 0.0;
+    for (int r0 = 0; r0 < count; r0 += kWarp) {
+      const int r = r0 + lane;
+      if (r < count) {
+        const int32_t i = rows[r];
+        const int64_t xs = a.x_csr.ptr[i];
+        const int64_t xe = a.x_csr.ptr[i + 1];
+        double acc = -0.0;
+        for (int64_t q = xs; q < xe; ++q) {
+          T bv;
+          if (HashFind(hkeys, hvals, hbits, a.x_csr.idx[q], bv)) {
+            acc = Add(acc, Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv)));
+          }
+        }
+        if (projection) {
+          const T az = static_cast<T>(acc);
+          const double td = static_cast<double>(
+              static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(az))));
+          T zv;
+          stage0[lane] = Mul(td, td);
+          // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
+          stage1[lane] = HashFind(hkeys, hvals, hbits, i, zv) ? Mul(static_cast<double>(zv), td) : 0.0;
+        } else {
+          double v = acc;
+          if (residual) {
+            v = -acc;
+            if (static_cast<int64_t>(i) == col) v = Add(v, 1.0);
+          }
+          const T stored = static_cast<T>(v);
+          a.c_idx[c0 + r] = i;
+          a.c_val[c0 + r] = stored;
+          if (a.z_val != nullptr) {
+            a.z_val[c0 + r] = static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(stored)));
+          }
+          if (a.prune && fabs(static_cast<double>(stored)) <= 0.0) zero_seen = true;
+          const double sd = static_cast<double>(stored);
+          stage0[lane] = Mul(sd, sd);
+        }
+      }
+      if (sums) {
+        __syncwarp();
+        if (lane == 0) {
+          const int n = min(kWarp, count - r0);
+          if (projection) {
+            for (int l = 0; l < n; ++l) {
+              tt = Add(tt, stage0[l]);
+              bt = Add(bt, stage1[l]);
+            }
+          } else {
+            for (int l = 0; l < n; ++l) sq = Add(sq, stage0[l]);
+          }
+        }
+        __syncwarp();
+      }
+    }
+    if (lane == 0) {
+      if (projection) {
+        a.proj_tt[col] = tt;
+        a.proj_bt[col] = bt;
+      } else if (a.col_squares != nullptr) {
+        a.col_squares[col] = sq;
+      }
+    }
+    __syncwarp();
+  }
+  if (__any_sync(0xffffffffu, zero_seen) && lane == 0) atomicOr(a.flag, 1);
+}
+
+// ---------------------------------------------------------------------------
 // Hash need, window and bin populations of every output column.
 template <class T>
 __global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ need,
@@ -620,6 +860,28 @@ void LaunchRowSets(Ctx& ctx, RowSetArgs<T> args, const unsigned long long* host_
   }
 }
 
+// The column path over every populated bitmap bin.
+template <class T>
+void LaunchColumnProducts(Ctx& ctx, const ColumnArgs<T>& args, const unsigned long long* host_max, int rows_cap,
+                          int hash_slots) {
+  int lo_words = -1;
+  for (int bin = 0; bin < kWordBinCount; ++bin) {
+    const int words_cap = kWordBins[bin];
+    if (host_max[kPopulation + bin] > 0) {
+      const size_t per_warp = ColumnSlabBytes(words_cap, rows_cap, hash_slots, sizeof(T));
+      int warps = static_cast<int>((96 * 1024) / per_warp);
+      warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
+      const size_t smem = per_warp * warps;
+      SPAI_CUDA(cudaFuncSetAttribute(ColumnProductKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+      ColumnProductKernel<T><<<GridFor(args.b.cols * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(
+          args, words_cap, lo_words, words_cap, rows_cap, hash_slots);
+      SPAI_LAUNCH_CHECK();
+    }
+    lo_words = words_cap;
+  }
+}
+
 template <class T>
 double MatrixBytes(int64_t nnz, int64_t major) {
   return static_cast<double>(nnz) * static_cast<double>(sizeof(T) + sizeof(int32_t)) +
@@ -648,6 +910,41 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   SPAI_CUDA(cudaMemcpyAsync(host_max, ctx.sg_maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
   ctx.Sync();
 
+  const int64_t max_u = static_cast<int64_t>(host_max[kMaxUb]);
+  const int64_t max_nb = static_cast<int64_t>(host_max[kMaxNb]);
+  const bool column_path =
+      host_max[kHashColumns] == 0 && max_u <= kColumnRowsMax && max_nb <= kColumnHashMaxKeys;
+  const ValueMode mode = residual ? ValueMode::kResidual : (projection ? ValueMode::kProjection : ValueMode::kStore);
+  const bool prune = epilogue == Epilogue::kPruneZeros || residual;
+  const bool want_z = residual && extras.row_scale != nullptr && c_z != nullptr;
+  // algorithmic bytes: |X| + |B| + |C| (the projection writes per-column sums instead of C)
+  const double operand_bytes = MatrixBytes<T>(x_csr.nnz, x_csr.cols) + MatrixBytes<T>(b.nnz, b.cols);
+
+  ColumnArgs<T> ca{};
+  ca.x = View(x_csc);
+  ca.x_csr = View(x_csr);
+  ca.b = View(b);
+  ca.win_lo = ctx.sg_win_lo.data();
+  ca.win_words = ctx.sg_win_words.data();
+  ca.add_diag = residual;
+  ca.mode = static_cast<int>(mode);
+  ca.prune = prune;
+  ca.row_scale = static_cast<const T*>(extras.row_scale);
+  ca.col_squares = extras.col_squares;
+  ca.proj_tt = extras.proj_tt;
+  ca.proj_bt = extras.proj_bt;
+  ca.flag = ctx.flags.data();
+  const int rows_cap = NextPow2(max_u > kWarp ? max_u : kWarp);
+  const int hash_slots = NextPow2(2 * max_nb > kWarp ? 2 * max_nb : kWarp);
+
+  if (projection && column_path) {
+    // no output matrix: no count pass, no scan, no host round trip
+    prof::Scope scope(ctx.stream, "spgemm_numeric",
+                      operand_bytes + static_cast<double>(cols) * (sizeof(T) + 2 * sizeof(double)));
+    LaunchColumnProducts(ctx, ca, host_max, rows_cap, hash_slots);
+    return false;
+  }
+
   RowSetArgs<T> rs{};
   rs.x = View(x_csc);
   rs.b = View(b);
@@ -658,8 +955,15 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   rs.counts = ctx.sg_counts.data();
   {
     prof::Scope scope(ctx.stream, "spgemm_symbolic", 0.0);
-    rs.list = false;
-    LaunchRowSets(ctx, rs, host_max);
+    if (column_path) {
+      ColumnArgs<T> cc = ca;
+      cc.count_only = true;
+      cc.counts = ctx.sg_counts.data();
+      LaunchColumnProducts(ctx, cc, host_max, rows_cap, hash_slots);
+    } else {
+      rs.list = false;
+      LaunchRowSets(ctx, rs, host_max);
+    }
   }
 
   // output layout: C, or the transient row list of the projection
@@ -685,15 +989,11 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
     rows = result.idx.data();
     vals = result.val.data();
   }
-  ctx.sg_cols.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
   DevBuf<T> zbuf;
-  const bool want_z = residual && extras.row_scale != nullptr && c_z != nullptr;
   if (want_z) zbuf.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
-  const bool prune = epilogue == Epilogue::kPruneZeros || residual;
   SPAI_CUDA(cudaMemsetAsync(ctx.flags.data(), 0, sizeof(int32_t), ctx.stream));
   {
-    // algorithmic bytes: |X| + |B| + |C| (the projection writes per-column sums instead of C)
-    double bytes = MatrixBytes<T>(x_csr.nnz, x_csr.cols) + MatrixBytes<T>(b.nnz, b.cols);
+    double bytes = operand_bytes;
     if (projection) {
       bytes += static_cast<double>(cols) * (sizeof(T) + 2 * sizeof(double));
     } else {
@@ -702,33 +1002,41 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
       if (extras.col_squares != nullptr) bytes += static_cast<double>(cols) * sizeof(double);
     }
     prof::Scope scope(ctx.stream, "spgemm_numeric", bytes);
-    rs.list = true;
-    rs.c_ptr = c_ptr;
-    rs.rows = rows;
-    rs.cols = ctx.sg_cols.data();
-    LaunchRowSets(ctx, rs, host_max);
-    ValuesArgs<T> va{};
-    va.x_csr = View(x_csr);
-    va.b = View(b);
-    va.rows = rows;
-    va.cols = ctx.sg_cols.data();
-    va.count = nnz;
-    va.mode = static_cast<int>(residual ? ValueMode::kResidual
-                                        : (projection ? ValueMode::kProjection : ValueMode::kStore));
-    va.prune = prune;
-    va.out = vals;
-    va.z_out = want_z ? zbuf.data() : nullptr;
-    va.row_scale = static_cast<const T*>(extras.row_scale);
-    va.flag = ctx.flags.data();
-    if (nnz > 0) {
-      ValuesKernel<T><<<GridFor(nnz, 256), 256, 0, ctx.stream>>>(va);
-      SPAI_LAUNCH_CHECK();
-    }
-    if (projection || extras.col_squares != nullptr) {
-      SumsArgs<T> sa{c_ptr, rows, vals, View(b), projection, extras.col_squares, extras.proj_tt, extras.proj_bt,
-                     cols};
-      ColumnSumsKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(sa);
-      SPAI_LAUNCH_CHECK();
+    if (column_path) {
+      ca.c_ptr = c_ptr;
+      ca.c_idx = rows;
+      ca.c_val = vals;
+      ca.z_val = want_z ? zbuf.data() : nullptr;
+      LaunchColumnProducts(ctx, ca, host_max, rows_cap, hash_slots);
+    } else {
+      ctx.sg_cols.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
+      rs.list = true;
+      rs.c_ptr = c_ptr;
+      rs.rows = rows;
+      rs.cols = ctx.sg_cols.data();
+      LaunchRowSets(ctx, rs, host_max);
+      ValuesArgs<T> va{};
+      va.x_csr = View(x_csr);
+      va.b = View(b);
+      va.rows = rows;
+      va.cols = ctx.sg_cols.data();
+      va.count = nnz;
+      va.mode = static_cast<int>(mode);
+      va.prune = prune;
+      va.out = vals;
+      va.z_out = want_z ? zbuf.data() : nullptr;
+      va.row_scale = static_cast<const T*>(extras.row_scale);
+      va.flag = ctx.flags.data();
+      if (nnz > 0) {
+        ValuesKernel<T><<<GridFor(nnz, 256), 256, 0, ctx.stream>>>(va);
+        SPAI_LAUNCH_CHECK();
+      }
+      if (projection || extras.col_squares != nullptr) {
+        SumsArgs<T> sa{c_ptr, rows, vals, View(b), projection, extras.col_squares, extras.proj_tt, extras.proj_bt,
+                       cols};
+        ColumnSumsKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(sa);
+        SPAI_LAUNCH_CHECK();
+      }
     }
   }
   if (projection) return false;

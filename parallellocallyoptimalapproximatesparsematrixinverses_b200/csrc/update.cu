@@ -11,8 +11,9 @@
 // (dropping.cpp:106-135, plus the optional per-column top-k): the merged
 // column of 0.5*(M + M^T) is built in shared memory, its 2-norm is summed in
 // row order by one lane (the reference's per-column sequential sum), the
-// relative threshold and the top-k rank rule are applied there, and only the
-// survivors are written.  One launch pair replaces transpose-union,
+// relative threshold is applied there, the top-k rule by a bitonic sort of
+// (|v|, position) keys in registers, and the survivors are written once, at
+// an upper-bound offset, then compacted.  This replaces transpose-union,
 // threshold-filter and top-k-filter passes over HBM.
 
 #include <cuda_runtime.h>
@@ -209,13 +210,84 @@ __device__ DropSlab SlabFor(unsigned char* base) {
   return s;
 }
 
-// Count pass (write == false): counts[j] = survivors of column j, overflow
-// set when a column exceeds kDropCap.  Write pass: the survivors in row order.
+// (|v| bits, position) ordering; the position breaks ties exactly as the row does.
+__device__ __forceinline__ bool KeyGreater(unsigned long long a, uint32_t pa, unsigned long long b, uint32_t pb) {
+  return a > b || (a == b && pa > pb);
+}
+
+// Ascending bitonic sort of 32*R (key, position) pairs held as element
+// t*32 + lane in register t of each lane.
+template <int R>
+__device__ __forceinline__ void WarpBitonicSort(unsigned long long (&k)[R], uint32_t (&p)[R], int lane) {
+#pragma unroll
+  for (int size = 2; size <= kWarp * R; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= kWarp) {
+        const int ts = stride / kWarp;
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          const int u = t ^ ts;
+          if (u > t) {
+            const bool up = ((t * kWarp + lane) & size) == 0;
+            if (KeyGreater(k[t], p[t], k[u], p[u]) == up) {
+              const unsigned long long kk = k[t];
+              k[t] = k[u];
+              k[u] = kk;
+              const uint32_t pp = p[t];
+              p[t] = p[u];
+              p[u] = pp;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          const unsigned long long ok = __shfl_xor_sync(0xffffffffu, k[t], stride);
+          const uint32_t op = __shfl_xor_sync(0xffffffffu, p[t], stride);
+          const bool up = ((t * kWarp + lane) & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          const bool mine_greater = KeyGreater(k[t], p[t], ok, op);
+          // the lower slot of an ascending pair keeps the smaller element
+          if (mine_greater == (lower == up)) {
+            k[t] = ok;
+            p[t] = op;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Marks the `drop` smallest (|v|, row) kept off-diagonal entries of the
+// column held in the slab as dropped; count <= 32 * R.
+template <int R>
+__device__ void DropSmallest(DropSlab& s, int count, int64_t col, int drop, int lane) {
+  unsigned long long k[R];
+  uint32_t p[R];
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    const int e = t * kWarp + lane;
+    const bool candidate = e < count && s.keep[e] != 0 && static_cast<int64_t>(s.keys[e]) != col;
+    k[t] = candidate ? static_cast<unsigned long long>(__double_as_longlong(fabs(s.vals[e]))) : ~0ull;
+    p[t] = static_cast<uint32_t>(e);
+  }
+  WarpBitonicSort<R>(k, p, lane);
+  __syncwarp();
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    if (t * kWarp + lane < drop) s.keep[p[t]] = 0;
+  }
+  __syncwarp();
+}
+
+// One pass: survivors of column j go to out at ub_ptr[j] = m.ptr[j] (+
+// mt.ptr[j] when symmetric), their number to counts[j]; `overflow` is set
+// when a column exceeds kDropCap (the caller then discards the pass).
 template <class T>
-__global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric, int64_t topk, bool write,
-                                     int64_t* __restrict__ counts, const int64_t* __restrict__ out_ptr,
-                                     int32_t* __restrict__ out_idx, T* __restrict__ out_val,
-                                     int32_t* __restrict__ overflow) {
+__global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric, int64_t topk,
+                                     int64_t* __restrict__ counts, int32_t* __restrict__ out_idx,
+                                     T* __restrict__ out_val, int32_t* __restrict__ overflow) {
   extern __shared__ __align__(16) unsigned char drop_smem[];
   const int lane = threadIdx.x & 31;
   DropSlab s = SlabFor(drop_smem + (threadIdx.x >> 5) * DropSlabBytes());
@@ -230,13 +302,14 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
         if (lane == 0) atomicOr(overflow, 1);
         continue;
       }
-      const int64_t merged = ny + nx - CommonRows(m, mt, j, lane);
+      MatchedPrefix(m, mt, j, s.mx_prefix, lane);
+      const int64_t merged = ny + nx - s.mx_prefix[nx];
       if (merged > kDropCap) {
         if (lane == 0) atomicOr(overflow, 1);
+        __syncwarp();
         continue;
       }
       count = static_cast<int>(merged);
-      MatchedPrefix(m, mt, j, s.mx_prefix, lane);
       MergeColumn(m, mt, j, false, 1.0, 1.0, true, s.mx_prefix, lane, [&](int64_t rank, int32_t row, double v) {
         s.keys[rank] = row;
         s.vals[rank] = static_cast<double>(static_cast<T>(v));  // the value M would store
@@ -279,51 +352,57 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
     }
     __syncwarp();
     if (topk > 0 && kept > topk) {
-      // drop the `drop` smallest (|v|, row) among the kept off-diagonal entries
+      // drop the smallest (|v|, row) among the kept off-diagonal entries
       const int64_t candidates = kept - (has_diag ? 1 : 0);
       const int64_t keep_off = topk - (has_diag ? 1 : 0) > 0 ? topk - (has_diag ? 1 : 0) : 0;
-      const int64_t drop = candidates - keep_off;
+      const int drop = static_cast<int>(candidates - keep_off);
       if (drop > 0) {
-        bool dropped_any[kDropCap / kWarp] = {};
-        for (int base = 0, r = 0; base < count; base += kWarp, ++r) {
-          const int i = base + lane;
-          if (i >= count || !s.keep[i] || static_cast<int64_t>(s.keys[i]) == j) continue;
-          const double a = fabs(s.vals[i]);
-          const int32_t row = s.keys[i];
-          int64_t rank = 0;
-          for (int q = 0; q < count; ++q) {
-            if (!s.keep[q] || static_cast<int64_t>(s.keys[q]) == j) continue;
-            const double aq = fabs(s.vals[q]);
-            rank += (aq < a || (aq == a && s.keys[q] < row)) ? 1 : 0;
-          }
-          dropped_any[r] = rank < drop;
+        if (count <= kWarp) {
+          DropSmallest<1>(s, count, j, drop, lane);
+        } else if (count <= 2 * kWarp) {
+          DropSmallest<2>(s, count, j, drop, lane);
+        } else if (count <= 4 * kWarp) {
+          DropSmallest<4>(s, count, j, drop, lane);
+        } else {
+          DropSmallest<8>(s, count, j, drop, lane);
         }
-        __syncwarp();
-        for (int base = 0, r = 0; base < count; base += kWarp, ++r) {
-          const int i = base + lane;
-          if (i < count && dropped_any[r]) s.keep[i] = 0;
-        }
-        __syncwarp();
-        kept -= static_cast<int>(drop);
+        kept -= drop;
       }
     }
-    if (!write) {
-      if (lane == 0) counts[j] = kept;
-    } else {
-      int64_t out = out_ptr[j];
-      for (int base = 0; base < count; base += kWarp) {
-        const int i = base + lane;
-        const bool keep = i < count && s.keep[i] != 0;
-        const unsigned mask = __ballot_sync(0xffffffffu, keep);
-        if (keep) {
-          const int64_t o = out + __popc(mask & LaneMaskBelow());
-          out_idx[o] = s.keys[i];
-          out_val[o] = static_cast<T>(s.vals[i]);
-        }
-        out += __popc(mask);
+    int64_t out = m.ptr[j] + (symmetric ? mt.ptr[j] : 0);
+    for (int base = 0; base < count; base += kWarp) {
+      const int i = base + lane;
+      const bool keep = i < count && s.keep[i] != 0;
+      const unsigned mask = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int64_t o = out + __popc(mask & LaneMaskBelow());
+        out_idx[o] = s.keys[i];
+        out_val[o] = static_cast<T>(s.vals[i]);
       }
+      out += __popc(mask);
     }
+    if (lane == 0) counts[j] = kept;
     __syncwarp();
+  }
+}
+
+// out(:, j) = the first counts[j] entries at ub_ptr[j] of the padded arrays.
+template <class T>
+__global__ void CompactColumnsKernel(const int64_t* __restrict__ m_ptr, const int64_t* __restrict__ mt_ptr,
+                                     int64_t cols, const int64_t* __restrict__ out_ptr,
+                                     const int32_t* __restrict__ src_idx, const T* __restrict__ src_val,
+                                     int32_t* __restrict__ dst_idx, T* __restrict__ dst_val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = warp; j < cols; j += warps) {
+    const int64_t from = m_ptr[j] + (mt_ptr != nullptr ? mt_ptr[j] : 0);
+    const int64_t to = out_ptr[j];
+    const int64_t n = out_ptr[j + 1] - to;
+    for (int64_t i = lane; i < n; i += kWarp) {
+      dst_idx[to + i] = src_idx[from + i];
+      dst_val[to + i] = src_val[from + i];
+    }
   }
 }
 
@@ -359,23 +438,28 @@ bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk) {
   SPAI_CUDA(cudaFuncSetAttribute(SymmetrizeDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(smem)));
   const int grid = GridFor(cols * kWarp, kWarps * kWarp);
+  // survivors land at m.ptr[j] (+ mt.ptr[j]): an upper bound of column j's merged length
+  const int64_t padded = m.nnz + (symmetric ? mt.nnz : 0);
+  DevBuf<int32_t> tmp_idx;
+  DevBuf<T> tmp_val;
+  tmp_idx.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
+  tmp_val.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
   ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
   int32_t* overflow = ctx.flags.data() + 1;
   SPAI_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int32_t), ctx.stream));
-  SymmetrizeDropKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(m), mt_view, symmetric, topk, false,
-                                                                      ctx.counts.data(), nullptr, nullptr, nullptr,
-                                                                      overflow);
+  SymmetrizeDropKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(m), mt_view, symmetric, topk,
+                                                                      ctx.counts.data(), tmp_idx.data(),
+                                                                      tmp_val.data(), overflow);
   SPAI_LAUNCH_CHECK();
   SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 1, overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
-  ctx.Sync();
-  if (ctx.host_flags[1] != 0) return false;
   DevCsc<T> out;
   out.Shape(m.rows, cols, ctx.stream);
-  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());
+  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());  // synchronises: flag is read
+  if (ctx.host_flags[1] != 0) return false;
   out.ReserveNnz(nnz, ctx.stream);
-  SymmetrizeDropKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(m), mt_view, symmetric, topk, true, nullptr,
-                                                                      out.ptr.data(), out.idx.data(), out.val.data(),
-                                                                      overflow);
+  CompactColumnsKernel<T><<<grid, kWarps * kWarp, 0, ctx.stream>>>(m.ptr.data(), symmetric ? mt.ptr.data() : nullptr,
+                                                                   cols, out.ptr.data(), tmp_idx.data(),
+                                                                   tmp_val.data(), out.idx.data(), out.val.data());
   SPAI_LAUNCH_CHECK();
   m.Swap(out);
   return true;
