@@ -505,6 +505,22 @@ __global__ void ScaleColumnsKernel(CscView<T> x, T* __restrict__ val, const doub
 }
 
 // ---------------------------------------------------------------------------
+// ELL copy
+template <class T>
+__global__ void EllKernel(CscView<T> x, int width, int32_t* __restrict__ idx, T* __restrict__ val) {
+  for (int64_t c = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; c < x.cols;
+       c += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t start = x.ptr[c];
+    const int64_t len = x.ptr[c + 1] - start;
+    for (int s = 0; s < width; ++s) {
+      const bool in = s < len;
+      idx[c * width + s] = in ? x.idx[start + s] : -1;
+      if (val != nullptr) val[c * width + s] = in ? x.val[start + s] : T(0);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Transpose
 __global__ void RowCountKernel(const int32_t* __restrict__ idx, int64_t nnz, unsigned long long* __restrict__ counts) {
   for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz;
@@ -513,16 +529,122 @@ __global__ void RowCountKernel(const int32_t* __restrict__ idx, int64_t nnz, uns
   }
 }
 
+// Warp per column: every entry takes the next free slot of its row (the order
+// inside a row is fixed afterwards by the segment sort).
 template <class T>
-__global__ void ScatterKernel(CscView<T> x, const int64_t* __restrict__ t_ptr, unsigned long long* __restrict__ cursor,
+__global__ void ScatterKernel(CscView<T> x, const int64_t* __restrict__ t_ptr, unsigned int* __restrict__ cursor,
                               int32_t* __restrict__ t_idx, T* __restrict__ t_val) {
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = warp; j < x.cols; j += warps) {
+    for (int64_t p = x.ptr[j] + lane; p < x.ptr[j + 1]; p += kWarp) {
       const int32_t row = x.idx[p];
-      const int64_t dst = t_ptr[row] + static_cast<int64_t>(atomicAdd(&cursor[row], 1ull));
+      const int64_t dst = t_ptr[row] + static_cast<int64_t>(atomicAdd(&cursor[row], 1u));
       t_idx[dst] = static_cast<int32_t>(j);
       t_val[dst] = x.val[p];
+    }
+  }
+}
+
+// Largest value of counts[0, n) into *out (out zeroed by the caller).
+__global__ void MaxCountKernel(const int64_t* __restrict__ counts, int64_t n, unsigned long long* __restrict__ out) {
+  unsigned long long m = 0;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned long long c = static_cast<unsigned long long>(counts[i]);
+    m = c > m ? c : m;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long other = __shfl_xor_sync(0xffffffffu, m, o);
+    m = other > m ? other : m;
+  }
+  if ((threadIdx.x & 31) == 0 && m != 0ull) atomicMax(out, m);
+}
+
+// Ascending bitonic sort of 32*R (key, value) pairs, element t*32 + lane in
+// register t; keys are distinct except the INT32_MAX padding.
+template <int R, class T>
+__device__ __forceinline__ void WarpSortPairs(int32_t (&k)[R], T (&v)[R], int lane) {
+#pragma unroll
+  for (int size = 2; size <= kWarp * R; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= kWarp) {
+        const int ts = stride / kWarp;
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          const int u = t ^ ts;
+          if (u > t) {
+            const bool up = ((t * kWarp + lane) & size) == 0;
+            if ((k[t] > k[u]) == up) {
+              const int32_t kk = k[t];
+              k[t] = k[u];
+              k[u] = kk;
+              const T vv = v[t];
+              v[t] = v[u];
+              v[u] = vv;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int t = 0; t < R; ++t) {
+          const int32_t ok = __shfl_xor_sync(0xffffffffu, k[t], stride);
+          const T ov = __shfl_xor_sync(0xffffffffu, v[t], stride);
+          const bool up = ((t * kWarp + lane) & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          if ((k[t] > ok) == (lower == up)) {
+            k[t] = ok;
+            v[t] = ov;
+          }
+        }
+      }
+    }
+  }
+}
+
+template <int R, class T>
+__device__ __forceinline__ void SortSegmentInRegisters(int64_t start, int len, int32_t* idx, T* val, int lane) {
+  int32_t k[R];
+  T v[R];
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    const int e = t * kWarp + lane;
+    k[t] = e < len ? idx[start + e] : INT32_MAX;
+    v[t] = e < len ? val[start + e] : T(0);
+  }
+  WarpSortPairs<R, T>(k, v, lane);
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    const int e = t * kWarp + lane;
+    if (e < len) {
+      idx[start + e] = k[t];
+      val[start + e] = v[t];
+    }
+  }
+}
+
+// Warp per segment of at most 256 entries, sorted in registers.
+template <class T>
+__global__ void SegmentSortRegKernel(const int64_t* __restrict__ ptr, int64_t segments, int32_t* __restrict__ idx,
+                                     T* __restrict__ val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t s = warp; s < segments; s += warps) {
+    const int64_t start = ptr[s];
+    const int len = static_cast<int>(ptr[s + 1] - start);
+    if (len <= 1 || len > 8 * kWarp) continue;
+    if (len <= kWarp) {
+      SortSegmentInRegisters<1, T>(start, len, idx, val, lane);
+    } else if (len <= 2 * kWarp) {
+      SortSegmentInRegisters<2, T>(start, len, idx, val, lane);
+    } else if (len <= 4 * kWarp) {
+      SortSegmentInRegisters<4, T>(start, len, idx, val, lane);
+    } else {
+      SortSegmentInRegisters<8, T>(start, len, idx, val, lane);
     }
   }
 }
@@ -573,7 +695,7 @@ __global__ void SegmentSortWarpKernel(const int64_t* __restrict__ ptr, int64_t s
   for (int64_t s = warp; s < segments; s += warps) {
     const int64_t start = ptr[s];
     const int len = static_cast<int>(ptr[s + 1] - start);
-    if (len <= 1 || len > kWarpSortCap) continue;
+    if (len <= 8 * kWarp || len > kWarpSortCap) continue;
     int size = 1;
     while (size < len) size <<= 1;
     for (int i = lane; i < size; i += kWarp) {
@@ -641,18 +763,30 @@ __global__ void SegmentSortLongKernel(const int64_t* __restrict__ ptr, int64_t s
   }
 }
 
+// Sorts every segment [ptr[s], ptr[s+1]) by index; `longest` bounds the
+// segment lengths, so only the kernels that have work are launched.
 template <class T>
-void SortSegments(Ctx& ctx, const int64_t* ptr, int64_t segments, int32_t* idx, T* val) {
-  const size_t warp_smem = 4 * kWarpSortCap * (sizeof(int32_t) + sizeof(T));
-  SegmentSortWarpKernel<T><<<GridFor(segments * kWarp, 128), 128, warp_smem, ctx.stream>>>(ptr, segments, idx, val);
+void SortSegments(Ctx& ctx, const int64_t* ptr, int64_t segments, int32_t* idx, T* val, int64_t longest) {
+  if (longest <= 1) return;
+  SegmentSortRegKernel<T><<<GridFor(segments * kWarp, 256), 256, 0, ctx.stream>>>(ptr, segments, idx, val);
   SPAI_LAUNCH_CHECK();
-  const size_t block_smem = kBlockSortCap * (sizeof(int32_t) + sizeof(T));
-  SPAI_CUDA(cudaFuncSetAttribute(SegmentSortBlockKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(block_smem)));
-  SegmentSortBlockKernel<T><<<GridFor(segments * 1024, 1024) , 1024, block_smem, ctx.stream>>>(ptr, segments, idx, val);
-  SPAI_LAUNCH_CHECK();
-  SegmentSortLongKernel<T><<<GridFor(segments, 128), 128, 0, ctx.stream>>>(ptr, segments, idx, val);
-  SPAI_LAUNCH_CHECK();
+  if (longest > 8 * kWarp) {
+    const size_t warp_smem = 4 * kWarpSortCap * (sizeof(int32_t) + sizeof(T));
+    SegmentSortWarpKernel<T><<<GridFor(segments * kWarp, 128), 128, warp_smem, ctx.stream>>>(ptr, segments, idx, val);
+    SPAI_LAUNCH_CHECK();
+  }
+  if (longest > kWarpSortCap) {
+    const size_t block_smem = kBlockSortCap * (sizeof(int32_t) + sizeof(T));
+    SPAI_CUDA(cudaFuncSetAttribute(SegmentSortBlockKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(block_smem)));
+    SegmentSortBlockKernel<T><<<GridFor(segments * 1024, 1024), 1024, block_smem, ctx.stream>>>(ptr, segments, idx,
+                                                                                               val);
+    SPAI_LAUNCH_CHECK();
+  }
+  if (longest > kBlockSortCap) {
+    SegmentSortLongKernel<T><<<GridFor(segments, 128), 128, 0, ctx.stream>>>(ptr, segments, idx, val);
+    SPAI_LAUNCH_CHECK();
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -973,6 +1107,12 @@ void ScaleColumns(Ctx& ctx, DevCsc<T>& x, const double* scale) {
 }
 
 template <class T>
+void BuildEll(Ctx& ctx, const DevCsc<T>& x, int width, int32_t* idx, T* val) {
+  EllKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(View(x), width, idx, val);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
 void DropZeros(Ctx& ctx, DevCsc<T>& x) {
   RunFilter(ctx, x, KeepNonZero<T>{});
 }
@@ -1048,14 +1188,22 @@ void Transpose(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& t) {
     RowCountKernel<<<GridFor(x.nnz, 256), 256, 0, ctx.stream>>>(x.idx.data(), x.nnz, row_counts);
     SPAI_LAUNCH_CHECK();
   }
+  // the longest row, read back by the scan's synchronisation
+  unsigned long long* longest = ctx.select_state.data() + 3;
+  SPAI_CUDA(cudaMemsetAsync(longest, 0, sizeof(unsigned long long), ctx.stream));
+  MaxCountKernel<<<GridFor(x.rows, 256), 256, 0, ctx.stream>>>(ctx.counts.data(), x.rows, longest);
+  SPAI_LAUNCH_CHECK();
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_counts + 1, longest, sizeof(int64_t), cudaMemcpyDeviceToHost, ctx.stream));
   const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), x.rows, result.ptr.data());
+  const int64_t longest_row = ctx.host_counts[1];
   result.ReserveNnz(nnz, ctx.stream);
-  SPAI_CUDA(cudaMemsetAsync(row_counts, 0, sizeof(int64_t) * (x.rows + 1), ctx.stream));
+  unsigned int* cursor = reinterpret_cast<unsigned int*>(row_counts);
+  SPAI_CUDA(cudaMemsetAsync(cursor, 0, sizeof(unsigned int) * x.rows, ctx.stream));
   if (nnz > 0) {
-    ScatterKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(View(x), result.ptr.data(), row_counts,
-                                                                  result.idx.data(), result.val.data());
+    ScatterKernel<T><<<GridFor(x.cols * kWarp, 256), 256, 0, ctx.stream>>>(View(x), result.ptr.data(), cursor,
+                                                                          result.idx.data(), result.val.data());
     SPAI_LAUNCH_CHECK();
-    SortSegments<T>(ctx, result.ptr.data(), x.rows, result.idx.data(), result.val.data());
+    SortSegments<T>(ctx, result.ptr.data(), x.rows, result.idx.data(), result.val.data(), longest_row);
   }
   t.Swap(result);
 }
@@ -1108,6 +1256,7 @@ void ConvertValues(Ctx& ctx, const S* src, D* dst, int64_t n) {
   template void DiagScale<T>(Ctx&, const T*, const DevCsc<T>&, DevCsc<T>&, bool);                             \
   template void ScaleColumns<T>(Ctx&, DevCsc<T>&, const double*);                                             \
   template void DropZeros<T>(Ctx&, DevCsc<T>&);                                                               \
+  template void BuildEll<T>(Ctx&, const DevCsc<T>&, int, int32_t*, T*);                                         \
   template void PruneColumnRelative<T>(Ctx&, DevCsc<T>&);                                                     \
   template void PruneAbsAtMost<T>(Ctx&, DevCsc<T>&, double);                                                  \
   template void KeepTopKPerColumn<T>(Ctx&, DevCsc<T>&, int64_t, bool);                                        \

@@ -96,6 +96,12 @@ void UnionWriteWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, bool scale
                     bool prune, DevCsc<T>& out, int32_t* flag);
 int UnionWarpCap();
 
+// Fixed-width (ELL) copy of x: slot s of column c is entry s of x(:, c), or
+// index -1 (value 0) past the column's end; width >= the longest column.
+// val may be null (indices only).
+template <class T>
+void BuildEll(Ctx& ctx, const DevCsc<T>& x, int width, int32_t* idx, T* val);
+
 // Row scaling out = diag(d) * b (Pr * X with a diagonal Pr); optional zero pruning.
 template <class T>
 void DiagScale(Ctx& ctx, const T* d, const DevCsc<T>& b, DevCsc<T>& out, bool prune_zeros);

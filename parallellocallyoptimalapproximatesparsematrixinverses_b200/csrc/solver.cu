@@ -145,6 +145,7 @@ class Solver final : public SolverBase {
       UploadCsc(ctx_, a, a_, stage_idx, stage_val);
     }
     Transpose(ctx_, A(), a_csr_);
+    BuildAEll(a);
     // ||A e_k||^2 per column (methods_common.cpp:65-76)
     col_norm2_.Reserve(static_cast<size_t>(n_), ctx_.stream);
     if (opt_.dropping) {
@@ -323,6 +324,38 @@ class Solver final : public SolverBase {
     return 0.0;
   }
 
+  // ELL copies of A when no row or column of A holds more than kMaxEllWidth entries.
+  void BuildAEll(const HostCsc& a) {
+    ell_width_ = 0;
+    int64_t longest = 0;
+    std::vector<int64_t> row_len(static_cast<size_t>(a.rows), 0);
+    for (int64_t j = 0; j < a.cols; ++j) {
+      longest = std::max(longest, a.ptr[j + 1] - a.ptr[j]);
+      for (int64_t p = a.ptr[j]; p < a.ptr[j + 1]; ++p) ++row_len[static_cast<size_t>(a.idx[p])];
+    }
+    for (const int64_t len : row_len) longest = std::max(longest, len);
+    if (longest > kMaxEllWidth) return;
+    const int width = static_cast<int>(std::max<int64_t>(4, (longest + 3) / 4 * 4));
+    const size_t slots = static_cast<size_t>(n_) * static_cast<size_t>(width);
+    a_cols_ell_.Reserve(slots, ctx_.stream);
+    a_rows_ell_.Reserve(slots, ctx_.stream);
+    a_rows_ell_val_.Reserve(slots, ctx_.stream);
+    BuildEll(ctx_, A(), width, a_cols_ell_.data(), static_cast<T*>(nullptr));
+    BuildEll(ctx_, a_csr_, width, a_rows_ell_.data(), a_rows_ell_val_.data());
+    ell_width_ = width;
+  }
+
+  SpgemmExtras AExtras() const {
+    SpgemmExtras extras;
+    if (ell_width_ > 0) {
+      extras.x_cols_ell = a_cols_ell_.data();
+      extras.x_rows_ell = a_rows_ell_.data();
+      extras.x_rows_ell_val = a_rows_ell_val_.data();
+      extras.ell_width = ell_width_;
+    }
+    return extras;
+  }
+
   void Empty(DevCsc<T>& x) {
     x.Shape(n_, n_, ctx_.stream);
     x.ReserveNnz(0, ctx_.stream);
@@ -331,7 +364,7 @@ class Solver final : public SolverBase {
 
   // ---- products (state_manager.cpp:47-66; dropping.cpp:97-104) ------------
   void MulA(const DevCsc<T>& in, DevCsc<T>& out) {
-    Spgemm(ctx_, A(), a_csr_, in, out, opt_.dropping ? Epilogue::kPlain : Epilogue::kPruneZeros);
+    Spgemm(ctx_, A(), a_csr_, in, out, opt_.dropping ? Epilogue::kPlain : Epilogue::kPruneZeros, AExtras());
   }
 
   void MulPr(const DevCsc<T>& in, DevCsc<T>& out) {
@@ -345,7 +378,7 @@ class Solver final : public SolverBase {
   // R = I - A*M, with the per-column squares of R (for ||R||_F) and, when Pr
   // is diagonal and the dropping path keeps R's pattern, Z = Pr*R in the same pass.
   void Residual() {
-    SpgemmExtras extras;
+    SpgemmExtras extras = AExtras();
     extras.col_squares = ctx_.Partial(kResidualPartial, n_);
     DevCsc<T>* z_out = nullptr;
     // the global methods (symmetric_) use Z = Pr*R right after every dropping-path residual
@@ -548,7 +581,7 @@ class Solver final : public SolverBase {
     if (pr_diagonal_) {
       double* tt = ctx_.Partial(0, n_);
       double* bt = ctx_.Partial(1, n_);
-      SpgemmExtras extras;
+      SpgemmExtras extras = AExtras();
       extras.row_scale = pr_vec_.data();
       extras.proj_tt = tt;
       extras.proj_bt = bt;
@@ -666,7 +699,7 @@ class Solver final : public SolverBase {
         Spgemm(ctx_, outer, outer_csr, r_, z_, opt_.dropping ? Epilogue::kPlain : Epilogue::kPruneZeros);
         MulA(z_, az_);
         if (locally_optimal) {
-          Spgemm(ctx_, A(), a_csr_, q_, ap_, Epilogue::kPlain);
+          Spgemm(ctx_, A(), a_csr_, q_, ap_, Epilogue::kPlain, AExtras());
         }
         double* r_az = ctx_.Partial(0, n_);
         double* az_az = ctx_.Partial(1, n_);
@@ -735,6 +768,12 @@ class Solver final : public SolverBase {
   DevCsc<T> pr_csr_;
   DevCsc<T> m0_;
   DevCsc<T> m_, r_, z_, p_, ap_, az_, tmp_, q_;
+  // fixed-width copies of A for the SpGEMM column kernel (stencil-like A only)
+  DevBuf<int32_t> a_cols_ell_;
+  DevBuf<int32_t> a_rows_ell_;
+  DevBuf<T> a_rows_ell_val_;
+  int ell_width_ = 0;
+  static constexpr int kMaxEllWidth = 16;
   DevCsc<T> z_fused_;             // Pr*R written by the last residual product
   bool r_squares_ready_ = false;  // Partial(kResidualPartial) holds R's column squares
   bool z_fused_ready_ = false;

@@ -527,6 +527,10 @@ struct ColumnArgs {
   double* proj_tt;
   double* proj_bt;
   int32_t* flag;
+  const int32_t* x_cols_ell;  // optional ELL copies of X (see SpgemmExtras)
+  const int32_t* x_rows_ell;
+  const T* x_rows_ell_val;
+  int ell_width;
 };
 
 __host__ __device__ inline int SummaryWords(int words) { return (words + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp; }
@@ -535,6 +539,23 @@ __host__ __device__ inline size_t ColumnSlabBytes(int words, int rows_cap, int h
   return Round16(static_cast<size_t>(words) * 4) + Round16(static_cast<size_t>(SummaryWords(words)) * 4) +
          Round16(static_cast<size_t>(rows_cap) * 4) + Round16(static_cast<size_t>(hash_slots) * 4) +
          Round16(static_cast<size_t>(hash_slots) * value_size) + 2 * Round16(kWarp * sizeof(double));
+}
+
+__device__ __forceinline__ void LoadFour(const float* p, float (&v)[4]) {
+  const float4 q = *reinterpret_cast<const float4*>(p);
+  v[0] = q.x;
+  v[1] = q.y;
+  v[2] = q.z;
+  v[3] = q.w;
+}
+
+__device__ __forceinline__ void LoadFour(const double* p, double (&v)[4]) {
+  const double2 q0 = reinterpret_cast<const double2*>(p)[0];
+  const double2 q1 = reinterpret_cast<const double2*>(p)[1];
+  v[0] = q0.x;
+  v[1] = q0.y;
+  v[2] = q1.x;
+  v[3] = q1.y;
 }
 
 template <class T>
@@ -639,17 +660,30 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
       }
     }
     if (a.add_diag && lane == 0) MarkRow(bm, summary, static_cast<int>(col) - lo);
-    for (int64_t p = bs + lane; p < be; p += kWarp) {
-      const int32_t k = a.b.idx[p];
-      const int64_t xs = a.x.ptr[k];
-      const int64_t xe = a.x.ptr[k + 1];
-      for (int64_t q0 = xs; q0 < xe; q0 += 8) {
-        int32_t r8[8];
+    if (a.ell_width > 0) {
+      for (int64_t p = bs + lane; p < be; p += kWarp) {
+        const int4* src = reinterpret_cast<const int4*>(a.x_cols_ell + static_cast<int64_t>(a.b.idx[p]) * a.ell_width);
+        for (int u = 0; u < a.ell_width / 4; ++u) {
+          const int4 r4 = src[u];
+          if (r4.x >= 0) MarkRow(bm, summary, r4.x - lo);
+          if (r4.y >= 0) MarkRow(bm, summary, r4.y - lo);
+          if (r4.z >= 0) MarkRow(bm, summary, r4.z - lo);
+          if (r4.w >= 0) MarkRow(bm, summary, r4.w - lo);
+        }
+      }
+    } else {
+      for (int64_t p = bs + lane; p < be; p += kWarp) {
+        const int32_t k = a.b.idx[p];
+        const int64_t xs = a.x.ptr[k];
+        const int64_t xe = a.x.ptr[k + 1];
+        for (int64_t q0 = xs; q0 < xe; q0 += 8) {
+          int32_t r8[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) r8[u] = q0 + u < xe ? a.x.idx[q0 + u] : -1;
+          for (int u = 0; u < 8; ++u) r8[u] = q0 + u < xe ? a.x.idx[q0 + u] : -1;
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          if (r8[u] >= 0) MarkRow(bm, summary, r8[u] - lo);
+          for (int u = 0; u < 8; ++u) {
+            if (r8[u] >= 0) MarkRow(bm, summary, r8[u] - lo);
+          }
         }
       }
     }
@@ -667,13 +701,31 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
       const int r = r0 + lane;
       if (r < count) {
         const int32_t i = rows[r];
-        const int64_t xs = a.x_csr.ptr[i];
-        const int64_t xe = a.x_csr.ptr[i + 1];
         double acc = -0.0;
-        for (int64_t q = xs; q < xe; ++q) {
-          T bv;
-          if (HashFind(hkeys, hvals, hbits, a.x_csr.idx[q], bv)) {
-            acc = Add(acc, Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv)));
+        if (a.ell_width > 0) {
+          const int4* ks = reinterpret_cast<const int4*>(a.x_rows_ell + static_cast<int64_t>(i) * a.ell_width);
+          const T* vs = a.x_rows_ell_val + static_cast<int64_t>(i) * a.ell_width;
+          for (int u = 0; u < a.ell_width / 4; ++u) {
+            const int4 k4 = ks[u];
+            T v4[4];
+            LoadFour(vs + 4 * u, v4);
+            const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              T bv;
+              if (kk[e] >= 0 && HashFind(hkeys, hvals, hbits, kk[e], bv)) {
+                acc = Add(acc, Mul(static_cast<double>(v4[e]), static_cast<double>(bv)));
+              }
+            }
+          }
+        } else {
+          const int64_t xs = a.x_csr.ptr[i];
+          const int64_t xe = a.x_csr.ptr[i + 1];
+          for (int64_t q = xs; q < xe; ++q) {
+            T bv;
+            if (HashFind(hkeys, hvals, hbits, a.x_csr.idx[q], bv)) {
+              acc = Add(acc, Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv)));
+            }
           }
         }
         if (projection) {
@@ -702,28 +754,39 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
         }
       }
       if (sums) {
+        // sequential in row order; lane 0 sums stage0, lane 1 (projection) stage1
         __syncwarp();
-        if (lane == 0) {
+        if (lane < (projection ? 2 : 1)) {
+          const double* src = lane == 0 ? stage0 : stage1;
+          double s = lane == 0 ? (projection ? tt : sq) : bt;
           const int n = min(kWarp, count - r0);
-          if (projection) {
-            for (int l = 0; l < n; ++l) {
-              tt = Add(tt, stage0[l]);
-              bt = Add(bt, stage1[l]);
+          if (n == kWarp) {
+            const double2* src2 = reinterpret_cast<const double2*>(src);
+#pragma unroll
+            for (int l = 0; l < kWarp / 2; ++l) {
+              const double2 v = src2[l];
+              s = Add(s, v.x);
+              s = Add(s, v.y);
             }
           } else {
-            for (int l = 0; l < n; ++l) sq = Add(sq, stage0[l]);
+            for (int l = 0; l < n; ++l) s = Add(s, src[l]);
+          }
+          if (lane == 1) {
+            bt = s;
+          } else if (projection) {
+            tt = s;
+          } else {
+            sq = s;
           }
         }
         __syncwarp();
       }
     }
-    if (lane == 0) {
-      if (projection) {
-        a.proj_tt[col] = tt;
-        a.proj_bt[col] = bt;
-      } else if (a.col_squares != nullptr) {
-        a.col_squares[col] = sq;
-      }
+    if (projection) {
+      if (lane == 0) a.proj_tt[col] = tt;
+      if (lane == 1) a.proj_bt[col] = bt;
+    } else if (lane == 0 && a.col_squares != nullptr) {
+      a.col_squares[col] = sq;
     }
     __syncwarp();
   }
@@ -934,8 +997,13 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   ca.proj_tt = extras.proj_tt;
   ca.proj_bt = extras.proj_bt;
   ca.flag = ctx.flags.data();
+  ca.x_cols_ell = extras.x_cols_ell;
+  ca.x_rows_ell = extras.x_rows_ell;
+  ca.x_rows_ell_val = static_cast<const T*>(extras.x_rows_ell_val);
+  ca.ell_width = extras.ell_width;
   const int rows_cap = NextPow2(max_u > kWarp ? max_u : kWarp);
-  const int hash_slots = NextPow2(2 * max_nb > kWarp ? 2 * max_nb : kWarp);
+  // load factor <= 1/4 while the table stays small, <= 1/2 beyond
+  const int hash_slots = NextPow2(4 * max_nb <= 1024 ? (4 * max_nb > kWarp ? 4 * max_nb : kWarp) : 2 * max_nb);
 
   if (projection && column_path) {
     // no output matrix: no count pass, no scan, no host round trip

@@ -31,6 +31,13 @@ struct SpgemmExtras {
   // kProjection: outputs
   double* proj_tt = nullptr;  // per column sum over rows of (pr_i c_i)^2
   double* proj_bt = nullptr;  // per column sum over rows in both of b_i * (pr_i c_i)
+  // Optional fixed-width (ELL) copies of X with `ell_width` slots per column /
+  // row (a multiple of 4), entries in storage order, padded with index -1:
+  // the column kernel then reads a whole column or row of X with 16-byte loads.
+  const int32_t* x_cols_ell = nullptr;      // rows of X(:, k)
+  const int32_t* x_rows_ell = nullptr;      // columns of X(i, :)
+  const void* x_rows_ell_val = nullptr;     // values of X(i, :) (const T*)
+  int ell_width = 0;
 };
 
 // x_csc and x_csr are the same matrix X in column and row compressed form.

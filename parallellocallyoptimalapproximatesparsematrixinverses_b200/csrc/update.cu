@@ -185,29 +185,99 @@ __global__ void UnionWriteWarpKernel(CscView<T> y, CscView<T> x, bool scale_y, d
   if (__any_sync(0xffffffffu, zero_seen) && lane == 0) atomicOr(flag, 1);
 }
 
-// Per-warp shared memory of the fused drop kernel.
+// Per-warp shared memory of the fused drop kernel: the merged column (keys,
+// vals, keep), the matched prefix, and the row indices of both input columns.
 struct DropSlab {
   double* vals;
   int32_t* keys;
   int* mx_prefix;
   unsigned char* keep;
+  int32_t* yk;
+  int32_t* xk;
 };
 
+__host__ __device__ constexpr size_t Round16Bytes(size_t v) { return (v + 15) & ~size_t(15); }
+
 __host__ __device__ constexpr size_t DropSlabBytes() {
-  return ((kDropCap * sizeof(double) + 15) & ~size_t(15)) + ((kDropCap * sizeof(int32_t) + 15) & ~size_t(15)) +
-         (((kDropCap + 1) * sizeof(int) + 15) & ~size_t(15)) + ((kDropCap + 15) & ~size_t(15));
+  return Round16Bytes(kDropCap * sizeof(double)) + Round16Bytes(kDropCap * sizeof(int32_t)) +
+         Round16Bytes((kDropCap + 1) * sizeof(int)) + Round16Bytes(kDropCap) + 2 * Round16Bytes(kDropCap * 4);
 }
 
 __device__ DropSlab SlabFor(unsigned char* base) {
   DropSlab s;
   s.vals = reinterpret_cast<double*>(base);
-  base += (kDropCap * sizeof(double) + 15) & ~size_t(15);
+  base += Round16Bytes(kDropCap * sizeof(double));
   s.keys = reinterpret_cast<int32_t*>(base);
-  base += (kDropCap * sizeof(int32_t) + 15) & ~size_t(15);
+  base += Round16Bytes(kDropCap * sizeof(int32_t));
   s.mx_prefix = reinterpret_cast<int*>(base);
-  base += ((kDropCap + 1) * sizeof(int) + 15) & ~size_t(15);
+  base += Round16Bytes((kDropCap + 1) * sizeof(int));
   s.keep = base;
+  base += Round16Bytes(kDropCap);
+  s.yk = reinterpret_cast<int32_t*>(base);
+  base += Round16Bytes(kDropCap * 4);
+  s.xk = reinterpret_cast<int32_t*>(base);
   return s;
+}
+
+// First position in keys[0, n) whose row is >= key (keys in shared memory).
+__device__ __forceinline__ int LowerBoundShared(const int32_t* keys, int n, int32_t key) {
+  int lo = 0;
+  int hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (keys[mid] < key) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+// MatchedPrefix and MergeColumn (half sums) over row keys staged in shared
+// memory; values are read from the input columns.
+template <class T, class Emit>
+__device__ int MergeHalfSumShared(const CscView<T>& y, const CscView<T>& x, int64_t j, DropSlab& s, int lane,
+                                  Emit emit) {
+  const int64_t ys = y.ptr[j];
+  const int64_t xs = x.ptr[j];
+  const int ny = static_cast<int>(y.ptr[j + 1] - ys);
+  const int nx = static_cast<int>(x.ptr[j + 1] - xs);
+  for (int i = lane; i < ny; i += kWarp) s.yk[i] = y.idx[ys + i];
+  for (int i = lane; i < nx; i += kWarp) s.xk[i] = x.idx[xs + i];
+  __syncwarp();
+  int running = 0;
+  for (int base = 0; base < nx; base += kWarp) {
+    const int q = base + lane;
+    bool hit = false;
+    if (q < nx) {
+      const int32_t row = s.xk[q];
+      const int r = LowerBoundShared(s.yk, ny, row);
+      hit = r < ny && s.yk[r] == row;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (q < nx) s.mx_prefix[q] = running + __popc(mask & LaneMaskBelow());
+    running += __popc(mask);
+  }
+  if (lane == 0) s.mx_prefix[nx] = running;
+  __syncwarp();
+  const int merged = ny + nx - running;
+  if (merged > kDropCap) return merged;
+  for (int p = lane; p < ny; p += kWarp) {
+    const int32_t row = s.yk[p];
+    const int r = LowerBoundShared(s.xk, nx, row);
+    const double yv = static_cast<double>(y.val[ys + p]);
+    const double v = (r < nx && s.xk[r] == row) ? Both(yv, static_cast<double>(x.val[xs + r]), false, 1.0, 1.0, true)
+                                                : LeftOnly(yv, false, 1.0, true);
+    emit(p + r - s.mx_prefix[r], row, v);
+  }
+  for (int q = lane; q < nx; q += kWarp) {
+    const int32_t row = s.xk[q];
+    const int r = LowerBoundShared(s.yk, ny, row);
+    if (r < ny && s.yk[r] == row) continue;
+    emit(q - s.mx_prefix[q] + r, row, RightOnly(static_cast<double>(x.val[xs + q]), 1.0, true));
+  }
+  return merged;
 }
 
 // (|v| bits, position) ordering; the position breaks ties exactly as the row does.
@@ -302,18 +372,16 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
         if (lane == 0) atomicOr(overflow, 1);
         continue;
       }
-      MatchedPrefix(m, mt, j, s.mx_prefix, lane);
-      const int64_t merged = ny + nx - s.mx_prefix[nx];
+      const int merged = MergeHalfSumShared(m, mt, j, s, lane, [&](int rank, int32_t row, double v) {
+        s.keys[rank] = row;
+        s.vals[rank] = static_cast<double>(static_cast<T>(v));  // the value M would store
+      });
       if (merged > kDropCap) {
         if (lane == 0) atomicOr(overflow, 1);
         __syncwarp();
         continue;
       }
-      count = static_cast<int>(merged);
-      MergeColumn(m, mt, j, false, 1.0, 1.0, true, s.mx_prefix, lane, [&](int64_t rank, int32_t row, double v) {
-        s.keys[rank] = row;
-        s.vals[rank] = static_cast<double>(static_cast<T>(v));  // the value M would store
-      });
+      count = merged;
     } else {
       if (ny > kDropCap) {
         if (lane == 0) atomicOr(overflow, 1);
@@ -331,7 +399,14 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
     double thr = 0.0;
     if (lane == 0) {
       double sq = 0.0;
-      for (int i = 0; i < count; ++i) sq = Add(sq, Mul(s.vals[i], s.vals[i]));
+      const double2* v2 = reinterpret_cast<const double2*>(s.vals);
+      int i = 0;
+      for (; i + 1 < count; i += 2) {
+        const double2 v = v2[i >> 1];
+        sq = Add(sq, Mul(v.x, v.x));
+        sq = Add(sq, Mul(v.y, v.y));
+      }
+      if (i < count) sq = Add(sq, Mul(s.vals[i], s.vals[i]));
       thr = Mul(kDblEps, sqrt(sq));
     }
     thr = __shfl_sync(0xffffffffu, thr, 0);
