@@ -558,19 +558,67 @@ __device__ __forceinline__ void LoadFour(const double* p, double (&v)[4]) {
   v[3] = q1.y;
 }
 
+// Two-choice bucketed hash of B(:,j): bucket = 2 slots (one 8-byte word of
+// keys); a key lives in bucket h1 or h2 of its row, so a lookup is two
+// fixed loads.  A key that finds both buckets full is placed by linear
+// probing from the bucket after h2 (`displaced`, warp-uniform), and only
+// then do lookups that miss both buckets continue probing.
+__device__ __forceinline__ uint32_t Bucket1(int32_t key, int bits) {
+  return (static_cast<uint32_t>(key) * 2654435761u) >> (32 - bits);
+}
+
+__device__ __forceinline__ uint32_t Bucket2(int32_t key, int bits, uint32_t h1) {
+  const uint32_t h = (static_cast<uint32_t>(key) * 0x85EBCA6Bu + 0x9E3779B9u) >> (32 - bits);
+  return h == h1 ? (h ^ 1u) & ((1u << bits) - 1u) : h;
+}
+
+// Returns false when the key had to be displaced.
 template <class T>
-__device__ __forceinline__ bool HashFind(const int32_t* keys, const T* vals, int bits, int32_t key, T& out) {
-  const uint32_t mask = (1u << bits) - 1u;
-  uint32_t h = Slot(key, bits);
-  while (true) {
-    const int32_t k = keys[h];
-    if (k == key) {
-      out = vals[h];
+__device__ __forceinline__ bool BucketInsert(int32_t* keys, T* vals, int bits, int32_t key, T v) {
+  const uint32_t h1 = Bucket1(key, bits);
+  const uint32_t h2 = Bucket2(key, bits, h1);
+  const uint32_t slots[4] = {2 * h1, 2 * h1 + 1, 2 * h2, 2 * h2 + 1};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    if (atomicCAS(&keys[slots[i]], kEmpty, key) == kEmpty) {
+      vals[slots[i]] = v;
       return true;
     }
-    if (k == kEmpty) return false;
-    h = (h + 1u) & mask;
   }
+  const uint32_t mask = (2u << bits) - 1u;
+  uint32_t s = (2 * h2 + 2) & mask;
+  while (atomicCAS(&keys[s], kEmpty, key) != kEmpty) s = (s + 1u) & mask;
+  vals[s] = v;
+  return false;
+}
+
+template <class T>
+__device__ __forceinline__ bool BucketFind(const int32_t* keys, const T* vals, int bits, bool displaced, int32_t key,
+                                           T& out) {
+  const uint32_t h1 = Bucket1(key, bits);
+  const uint32_t h2 = Bucket2(key, bits, h1);
+  const int2 a = reinterpret_cast<const int2*>(keys)[h1];
+  const int2 b = reinterpret_cast<const int2*>(keys)[h2];
+  int slot = b.y == key ? static_cast<int>(2 * h2 + 1) : -1;
+  slot = b.x == key ? static_cast<int>(2 * h2) : slot;
+  slot = a.y == key ? static_cast<int>(2 * h1 + 1) : slot;
+  slot = a.x == key ? static_cast<int>(2 * h1) : slot;
+  if (slot < 0 && displaced) {
+    const uint32_t mask = (2u << bits) - 1u;
+    uint32_t s = (2 * h2 + 2) & mask;
+    while (true) {
+      const int32_t k = keys[s];
+      if (k == key) {
+        slot = static_cast<int>(s);
+        break;
+      }
+      if (k == kEmpty) break;
+      s = (s + 1u) & mask;
+    }
+  }
+  if (slot < 0) return false;
+  out = vals[slot];
+  return true;
 }
 
 // Marks `off` in the two-level bitmap.
@@ -611,7 +659,8 @@ __device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, int
   return total;
 }
 
-template <class T>
+// kEll: the ELL width of X (compile time, so its loops unroll), 0 without.
+template <class T, int kEll>
 __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int words_cap, int lo_words, int hi_words,
                                                            int rows_cap, int hash_slots) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -630,7 +679,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
   base += Round16(static_cast<size_t>(hash_slots) * sizeof(T));
   double* stage0 = reinterpret_cast<double*>(base);
   double* stage1 = stage0 + kWarp;
-  const int hbits = Log2(hash_slots);
+  const int hbits = Log2(hash_slots) - 1;  // buckets of two slots
   const bool projection = a.mode == static_cast<int>(ValueMode::kProjection);
   const bool residual = a.mode == static_cast<int>(ValueMode::kResidual);
   const bool sums = projection || a.col_squares != nullptr;
@@ -647,23 +696,20 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
     const int32_t lo = a.win_lo[col];
     const int64_t bs = a.b.ptr[col];
     const int64_t be = a.b.ptr[col + 1];
+    bool displaced = false;
     if (!a.count_only) {
       ClearTable(hkeys, hash_slots, lane);
       __syncwarp();
-      for (int64_t p = bs + lane; p < be; p += kWarp) {
-        const int32_t k = a.b.idx[p];
-        const T v = a.b.val[p];
-        const uint32_t mask = (1u << hbits) - 1u;
-        uint32_t h = Slot(k, hbits);
-        while (atomicCAS(&hkeys[h], kEmpty, k) != kEmpty) h = (h + 1u) & mask;  // B's rows are distinct
-        hvals[h] = v;
-      }
+      bool placed = true;
+      for (int64_t p = bs + lane; p < be; p += kWarp) placed &= BucketInsert(hkeys, hvals, hbits, a.b.idx[p], a.b.val[p]);
+      displaced = !__all_sync(0xffffffffu, placed);
     }
     if (a.add_diag && lane == 0) MarkRow(bm, summary, static_cast<int>(col) - lo);
-    if (a.ell_width > 0) {
+    if constexpr (kEll > 0) {
       for (int64_t p = bs + lane; p < be; p += kWarp) {
-        const int4* src = reinterpret_cast<const int4*>(a.x_cols_ell + static_cast<int64_t>(a.b.idx[p]) * a.ell_width);
-        for (int u = 0; u < a.ell_width / 4; ++u) {
+        const int4* src = reinterpret_cast<const int4*>(a.x_cols_ell + static_cast<int64_t>(a.b.idx[p]) * kEll);
+#pragma unroll
+        for (int u = 0; u < kEll / 4; ++u) {
           const int4 r4 = src[u];
           if (r4.x >= 0) MarkRow(bm, summary, r4.x - lo);
           if (r4.y >= 0) MarkRow(bm, summary, r4.y - lo);
@@ -702,10 +748,11 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
       if (r < count) {
         const int32_t i = rows[r];
         double acc = -0.0;
-        if (a.ell_width > 0) {
-          const int4* ks = reinterpret_cast<const int4*>(a.x_rows_ell + static_cast<int64_t>(i) * a.ell_width);
-          const T* vs = a.x_rows_ell_val + static_cast<int64_t>(i) * a.ell_width;
-          for (int u = 0; u < a.ell_width / 4; ++u) {
+        if constexpr (kEll > 0) {
+          const int4* ks = reinterpret_cast<const int4*>(a.x_rows_ell + static_cast<int64_t>(i) * kEll);
+          const T* vs = a.x_rows_ell_val + static_cast<int64_t>(i) * kEll;
+#pragma unroll
+          for (int u = 0; u < kEll / 4; ++u) {
             const int4 k4 = ks[u];
             T v4[4];
             LoadFour(vs + 4 * u, v4);
@@ -713,7 +760,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               T bv;
-              if (kk[e] >= 0 && HashFind(hkeys, hvals, hbits, kk[e], bv)) {
+              if (kk[e] >= 0 && BucketFind(hkeys, hvals, hbits, displaced, kk[e], bv)) {
                 acc = Add(acc, Mul(static_cast<double>(v4[e]), static_cast<double>(bv)));
               }
             }
@@ -723,7 +770,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
           const int64_t xe = a.x_csr.ptr[i + 1];
           for (int64_t q = xs; q < xe; ++q) {
             T bv;
-            if (HashFind(hkeys, hvals, hbits, a.x_csr.idx[q], bv)) {
+            if (BucketFind(hkeys, hvals, hbits, displaced, a.x_csr.idx[q], bv)) {
               acc = Add(acc, Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv)));
             }
           }
@@ -735,7 +782,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
           T zv;
           stage0[lane] = Mul(td, td);
           // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
-          stage1[lane] = HashFind(hkeys, hvals, hbits, i, zv) ? Mul(static_cast<double>(zv), td) : 0.0;
+          stage1[lane] = BucketFind(hkeys, hvals, hbits, displaced, i, zv) ? Mul(static_cast<double>(zv), td) : 0.0;
         } else {
           double v = acc;
           if (residual) {
@@ -935,9 +982,16 @@ void LaunchColumnProducts(Ctx& ctx, const ColumnArgs<T>& args, const unsigned lo
       int warps = static_cast<int>((96 * 1024) / per_warp);
       warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
       const size_t smem = per_warp * warps;
-      SPAI_CUDA(cudaFuncSetAttribute(ColumnProductKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     static_cast<int>(smem)));
-      ColumnProductKernel<T><<<GridFor(args.b.cols * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(
+      void (*kernel)(ColumnArgs<T>, int, int, int, int, int) = ColumnProductKernel<T, 0>;
+      switch (args.ell_width) {
+        case 4: kernel = ColumnProductKernel<T, 4>; break;
+        case 8: kernel = ColumnProductKernel<T, 8>; break;
+        case 12: kernel = ColumnProductKernel<T, 12>; break;
+        case 16: kernel = ColumnProductKernel<T, 16>; break;
+        default: break;
+      }
+      SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      kernel<<<GridFor(args.b.cols * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(
           args, words_cap, lo_words, words_cap, rows_cap, hash_slots);
       SPAI_LAUNCH_CHECK();
     }

@@ -351,6 +351,85 @@ __device__ void DropSmallest(DropSlab& s, int count, int64_t col, int drop, int 
   __syncwarp();
 }
 
+// Keeps the keep_off largest (|v|, row) kept off-diagonal entries of the
+// column in the slab and marks the other candidates dropped.  Exact
+// prefilter: the keep_off-th largest of the 32 per-lane maxima bounds the
+// cut from below, so only candidates at or above it (usually <= 32) are
+// sorted; otherwise the full sort of DropSmallest decides.
+template <int R>
+__device__ void KeepLargest(DropSlab& s, int count, int64_t col, int candidates, int keep_off, int lane) {
+  if (keep_off == 0) {
+    for (int e = lane; e < count; e += kWarp) {
+      if (s.keep[e] != 0 && static_cast<int64_t>(s.keys[e]) != col) s.keep[e] = 0;
+    }
+    __syncwarp();
+    return;
+  }
+  unsigned long long k[R];
+  uint32_t p[R];
+  unsigned long long best = 0ull;
+  uint32_t best_p = 0u;
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    const int e = t * kWarp + lane;
+    const bool candidate = e < count && s.keep[e] != 0 && static_cast<int64_t>(s.keys[e]) != col;
+    // candidates have |v| > 0, so 0 sorts every other slot below them
+    k[t] = candidate ? static_cast<unsigned long long>(__double_as_longlong(fabs(s.vals[e]))) : 0ull;
+    p[t] = static_cast<uint32_t>(e);
+    if (KeyGreater(k[t], p[t], best, best_p)) {
+      best = k[t];
+      best_p = p[t];
+    }
+  }
+  if (keep_off <= kWarp) {
+    unsigned long long m[1] = {best};
+    uint32_t mp[1] = {best_p};
+    WarpBitonicSort<1>(m, mp, lane);
+    const unsigned long long cut = __shfl_sync(0xffffffffu, m[0], kWarp - keep_off);
+    const uint32_t cut_p = __shfl_sync(0xffffffffu, mp[0], kWarp - keep_off);
+    int survivors = 0;
+    bool mine[R];
+#pragma unroll
+    for (int t = 0; t < R; ++t) {
+      mine[t] = k[t] != 0ull && !KeyGreater(cut, cut_p, k[t], p[t]);
+      survivors += __popc(__ballot_sync(0xffffffffu, mine[t]));
+    }
+    if (survivors <= kWarp) {
+      // gather the survivors into one register per lane, staged in the
+      // (no longer needed) input-key area of the slab
+      unsigned long long* stage_k = reinterpret_cast<unsigned long long*>(s.xk);
+      uint32_t* stage_p = reinterpret_cast<uint32_t*>(s.xk + 2 * kWarp);
+      int filled = 0;
+#pragma unroll
+      for (int t = 0; t < R; ++t) {
+        const unsigned mask = __ballot_sync(0xffffffffu, mine[t]);
+        if (mine[t]) {
+          const int at = filled + __popc(mask & LaneMaskBelow());
+          stage_k[at] = k[t];
+          stage_p[at] = p[t];
+        }
+        filled += __popc(mask);
+      }
+      __syncwarp();
+      unsigned long long gk[1] = {lane < filled ? stage_k[lane] : 0ull};
+      // padding sorts below every survivor and is never marked
+      uint32_t gpp[1] = {lane < filled ? stage_p[lane] : 0xFFFF0000u + static_cast<uint32_t>(lane)};
+      __syncwarp();
+      WarpBitonicSort<1>(gk, gpp, lane);
+      // every candidate is dropped except the keep_off largest survivors
+#pragma unroll
+      for (int t = 0; t < R; ++t) {
+        if (k[t] != 0ull) s.keep[p[t]] = 0;
+      }
+      __syncwarp();
+      if (lane >= kWarp - keep_off && gpp[0] < 0xFFFF0000u) s.keep[gpp[0]] = 1;
+      __syncwarp();
+      return;
+    }
+  }
+  DropSmallest<R>(s, count, col, candidates - keep_off, lane);
+}
+
 // One pass: survivors of column j go to out at ub_ptr[j] = m.ptr[j] (+
 // mt.ptr[j] when symmetric), their number to counts[j]; `overflow` is set
 // when a column exceeds kDropCap (the caller then discards the pass).
@@ -432,14 +511,16 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
       const int64_t keep_off = topk - (has_diag ? 1 : 0) > 0 ? topk - (has_diag ? 1 : 0) : 0;
       const int drop = static_cast<int>(candidates - keep_off);
       if (drop > 0) {
+        const int c = static_cast<int>(candidates);
+        const int ko = static_cast<int>(keep_off);
         if (count <= kWarp) {
-          DropSmallest<1>(s, count, j, drop, lane);
+          KeepLargest<1>(s, count, j, c, ko, lane);
         } else if (count <= 2 * kWarp) {
-          DropSmallest<2>(s, count, j, drop, lane);
+          KeepLargest<2>(s, count, j, c, ko, lane);
         } else if (count <= 4 * kWarp) {
-          DropSmallest<4>(s, count, j, drop, lane);
+          KeepLargest<4>(s, count, j, c, ko, lane);
         } else {
-          DropSmallest<8>(s, count, j, drop, lane);
+          KeepLargest<8>(s, count, j, c, ko, lane);
         }
         kept -= drop;
       }
