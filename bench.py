@@ -280,7 +280,8 @@ def run_ours(args):
     lib.spai_profile_read(b"spgemm_numeric", ctypes.byref(ms), ctypes.byref(cnt), ctypes.byref(byt))
     peak, peak_kind = measured_peak_hbm()
     kernel_table = {}
-    for name in (b"spgemm_numeric", b"spgemm_symbolic", b"union", b"transpose", b"filter", b"pcg_spmv"):
+    for name in (b"spgemm_numeric", b"spgemm_symbolic", b"spgemm_compact", b"drop_update", b"union", b"transpose",
+                 b"filter", b"pcg_spmv"):
         m2, c2, b2 = ctypes.c_double(0.0), ctypes.c_int64(0), ctypes.c_double(0.0)
         lib.spai_profile_read(name, ctypes.byref(m2), ctypes.byref(c2), ctypes.byref(b2))
         kernel_table[name.decode()] = {"ms": round(m2.value, 3), "launches": c2.value,
@@ -320,8 +321,8 @@ def run_ours(args):
             },
             "speedup_mixed_vs_fp64": round(f_step / step_ms_max, 3),
             "roofline": {
-                "kernel": "spgemm_numeric (row-set list, values and column-sum kernels of R = I - A*M and of the "
-                          "fused MR projection)",
+                "kernel": "spgemm_numeric (ColumnProductKernel, one warp per output column: R = I - A*M with "
+                          "Z = Pr*R and the column sums fused, and the fused MR projection of A*Z)",
                 "measured": "library CUDA events on the session stream, in a second pass of the same mixed steps",
                 "bound": "hbm",
                 "achieved": round(achieved, 1),

@@ -505,6 +505,27 @@ __global__ void ScaleColumnsKernel(CscView<T> x, T* __restrict__ val, const doub
 }
 
 // ---------------------------------------------------------------------------
+// Padded -> compact columns (warp per column)
+template <class T>
+__global__ void CompactPaddedKernel(const int64_t* __restrict__ base, const int64_t* __restrict__ base2, int64_t cols,
+                                    const int64_t* __restrict__ out_ptr, const int32_t* __restrict__ src_idx,
+                                    const T* __restrict__ src_val, int32_t* __restrict__ dst_idx,
+                                    T* __restrict__ dst_val) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = warp; j < cols; j += warps) {
+    const int64_t from = base[j] + (base2 != nullptr ? base2[j] : 0);
+    const int64_t to = out_ptr[j];
+    const int64_t n = out_ptr[j + 1] - to;
+    for (int64_t i = lane; i < n; i += kWarp) {
+      if (dst_idx != nullptr) dst_idx[to + i] = src_idx[from + i];
+      dst_val[to + i] = src_val[from + i];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // ELL copy
 template <class T>
 __global__ void EllKernel(CscView<T> x, int width, int32_t* __restrict__ idx, T* __restrict__ val) {
@@ -959,6 +980,10 @@ void Ctx::Destroy() {
   sg_proj_vals.Release();
   sg_fallback.Release();
   sg_maxima.Release();
+  sg_ub_ptr.Release();
+  sg_pad_idx.Release();
+  sg_pad_val.Release();
+  sg_pad_z.Release();
   if (stream != nullptr) {
     cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
@@ -973,6 +998,17 @@ void Ctx::Destroy() {
 }
 
 void Ctx::Sync() { SPAI_CUDA(cudaStreamSynchronize(stream)); }
+
+void ScanCountsAsync(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out) {
+  if (n <= 0) {
+    SPAI_CUDA(cudaMemsetAsync(out, 0, sizeof(int64_t), ctx.stream));
+    return;
+  }
+  int64_t need = 0;
+  for (int64_t m = n; m > 1; m = CeilDiv(m, kScanTile)) need += 2 * CeilDiv(m, kScanTile) + 2;
+  ctx.scan_blocks.Reserve(static_cast<size_t>(need + 8), ctx.stream);
+  ScanRecursive(ctx, counts, n, out, ctx.scan_blocks, 0);
+}
 
 int64_t ScanCounts(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out) {
   if (n <= 0) {
@@ -1059,6 +1095,13 @@ void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T
   const int64_t cap = UnionWarpCap();
   const bool half_sum = mode == UnionMode::kHalfSum;
   prof::Scope scope(ctx.stream, "union", 0.0);
+  {
+    DevCsc<T> single;
+    if (UnionPadded(ctx, y, scale_y, ys, x, xs, half_sum, !half_sum, single)) {
+      out.Swap(single);
+      return;
+    }
+  }
   UnionCountWarp(ctx, y, x, ctx.counts.data());
   UnionKernel<T, false><<<grid, 128, 0, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, static_cast<int>(mode), cap,
                                                       ctx.counts.data(), nullptr, nullptr, nullptr);
@@ -1104,6 +1147,14 @@ void ScaleColumns(Ctx& ctx, DevCsc<T>& x, const double* scale) {
   ScaleColumnsKernel<T><<<GridFor(x.cols, 128), 128, 0, ctx.stream>>>(View(x), x.val.data(), scale);
   SPAI_LAUNCH_CHECK();
   DropZeros(ctx, x);
+}
+
+template <class T>
+void CompactPadded(Ctx& ctx, const int64_t* base, const int64_t* base2, int64_t cols, const int64_t* out_ptr,
+                   const int32_t* src_idx, const T* src_val, int32_t* dst_idx, T* dst_val) {
+  CompactPaddedKernel<T><<<GridFor(cols * kWarp, 256), 256, 0, ctx.stream>>>(base, base2, cols, out_ptr, src_idx,
+                                                                            src_val, dst_idx, dst_val);
+  SPAI_LAUNCH_CHECK();
 }
 
 template <class T>
@@ -1257,6 +1308,8 @@ void ConvertValues(Ctx& ctx, const S* src, D* dst, int64_t n) {
   template void ScaleColumns<T>(Ctx&, DevCsc<T>&, const double*);                                             \
   template void DropZeros<T>(Ctx&, DevCsc<T>&);                                                               \
   template void BuildEll<T>(Ctx&, const DevCsc<T>&, int, int32_t*, T*);                                         \
+  template void CompactPadded<T>(Ctx&, const int64_t*, const int64_t*, int64_t, const int64_t*, const int32_t*,      \
+                                 const T*, int32_t*, T*);                                                        \
   template void PruneColumnRelative<T>(Ctx&, DevCsc<T>&);                                                     \
   template void PruneAbsAtMost<T>(Ctx&, DevCsc<T>&, double);                                                  \
   template void KeepTopKPerColumn<T>(Ctx&, DevCsc<T>&, int64_t, bool);                                        \

@@ -39,6 +39,10 @@ struct Ctx {
   DevBuf<unsigned char> sg_proj_vals;
   DevBuf<unsigned char> sg_fallback;
   DevBuf<unsigned long long> sg_maxima;
+  DevBuf<int64_t> sg_ub_ptr;             // padded column offsets (scan of the upper bounds)
+  DevBuf<int32_t> sg_pad_idx;            // padded output rows
+  DevBuf<unsigned char> sg_pad_val;      // padded output values
+  DevBuf<unsigned char> sg_pad_z;        // padded fused Z values
   double* host_scalars = nullptr;   // pinned, kScalarSlots
   int64_t* host_counts = nullptr;   // pinned, 8
   int32_t* host_flags = nullptr;    // pinned, 8
@@ -57,6 +61,15 @@ struct Ctx {
 // out[0] = 0, out[i + 1] = counts[0] + ... + counts[i]; returns out[n] (one
 // device-to-host read).  counts and out must not alias.
 int64_t ScanCounts(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out);
+// The same scan without the read-back (stream-ordered, no synchronisation).
+void ScanCountsAsync(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out);
+
+// Moves column j of a padded matrix -- out_ptr[j+1] - out_ptr[j] entries
+// starting at base[j] (+ base2[j] when base2 is given) of src -- to
+// out_ptr[j] of dst.  dst_idx may be null (values only).
+template <class T>
+void CompactPadded(Ctx& ctx, const int64_t* base, const int64_t* base2, int64_t cols, const int64_t* out_ptr,
+                   const int32_t* src_idx, const T* src_val, int32_t* dst_idx, T* dst_val);
 
 // Canonical reduction: the fixed 4096-wide tree over `n` partial sums.
 // Results land in ctx.scalars[slot + i] for i < arrays; read them with
@@ -95,6 +108,11 @@ template <class T>
 void UnionWriteWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, bool scale_y, double ys, double xs, bool half_sum,
                     bool prune, DevCsc<T>& out, int32_t* flag);
 int UnionWarpCap();
+// Single-pass union into `out` (fresh); false when a column is too long for
+// it (then nothing is written and the two-pass kernels must run).
+template <class T>
+bool UnionPadded(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T>& x, double xs, bool half_sum,
+                 bool prune, DevCsc<T>& out);
 
 // Fixed-width (ELL) copy of x: slot s of column c is entry s of x(:, c), or
 // index -1 (value 0) past the column's end; width >= the longest column.

@@ -70,6 +70,12 @@ void Reset() {
   g_totals.clear();
 }
 
+void AddBytes(const char* name, double bytes) {
+  if (!Enabled()) return;
+  std::lock_guard<std::mutex> lock(g_mutex);
+  g_totals[name].bytes += bytes;
+}
+
 bool Read(const std::string& name, double* ms, int64_t* count, double* bytes) {
   std::lock_guard<std::mutex> lock(g_mutex);
   Drain();

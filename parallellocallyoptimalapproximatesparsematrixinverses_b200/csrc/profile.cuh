@@ -16,6 +16,9 @@ namespace prof {
 bool Enabled();
 void SetEnabled(bool on);
 void Reset();
+// Adds algorithmic bytes to a class after the fact (for a launch whose output
+// size is only known once it has run).
+void AddBytes(const char* name, double bytes);
 // Totals for one class: elapsed milliseconds, launches, algorithmic bytes.
 bool Read(const std::string& name, double* ms, int64_t* count, double* bytes);
 

@@ -46,6 +46,7 @@ constexpr int kMaxUb = 0;
 constexpr int kMaxNb = 1;
 constexpr int kPopulation = 4;
 constexpr int kHashColumns = 8;
+constexpr int kSumUb = 9;
 constexpr int kMaximaSlots = 16;
 
 __device__ __forceinline__ unsigned LaneMaskBelow() {
@@ -84,22 +85,6 @@ __device__ inline void ClearTable(int32_t* table, int size, int lane) {
 
 __device__ inline void ClearWords(uint32_t* words, int size, int lane) {
   for (int i = lane; i < size; i += kWarp) words[i] = 0u;
-}
-
-// One atomic per warp instead of one per thread.
-__device__ __forceinline__ void WarpAtomicAdd(unsigned long long* target, unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicAdd(target, v);
-}
-
-__device__ __forceinline__ void WarpAtomicMax(unsigned long long* target, unsigned long long v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const unsigned long long other = __shfl_xor_sync(0xffffffffu, v, o);
-    v = other > v ? other : v;
-  }
-  if ((threadIdx.x & 31) == 0 && v != 0ull) atomicMax(target, v);
 }
 
 // Calls f(row) for every candidate row of output column `col`, the rows of
@@ -502,7 +487,8 @@ __global__ void ColumnSumsKernel(SumsArgs<T> a) {
 // that order (acc starts at -0.0, so the first addition yields the first
 // product exactly: the same bits as "first product, then +=").  Per-column
 // sums are sequential in row order (lane 0 over a 32-entry staging buffer).
-// In count mode the kernel stops after the row set and writes its size.
+// C (and Z) are written column by column at padded offsets, exact zeros
+// squeezed out when pruning, with counts[j] = the surviving length.
 constexpr int kColumnRowsMax = 2048;   // largest output column (upper bound) the column path takes
 constexpr int kColumnHashMaxKeys = 1024;
 
@@ -514,11 +500,10 @@ struct ColumnArgs {
   const int32_t* win_lo;
   const int32_t* win_words;
   bool add_diag;
-  bool count_only;   // write counts[j] = |row set| and stop
-  int64_t* counts;
+  int64_t* counts;   // store/residual: surviving length of every column
   int mode;          // ValueMode: kStore, kResidual or kProjection
-  bool prune;
-  const int64_t* c_ptr;
+  bool prune;        // drop exact zeros while writing
+  const int64_t* c_ptr;  // padded column offsets (upper bounds)
   int32_t* c_idx;
   T* c_val;
   T* z_val;             // kResidual: Z = pr * R (optional)
@@ -526,7 +511,6 @@ struct ColumnArgs {
   double* col_squares;  // optional per-column sum of squares of C
   double* proj_tt;
   double* proj_bt;
-  int32_t* flag;
   const int32_t* x_cols_ell;  // optional ELL copies of X (see SpgemmExtras)
   const int32_t* x_rows_ell;
   const T* x_rows_ell_val;
@@ -687,7 +671,6 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
   ClearWords(bm, words_cap, lane);
   ClearWords(summary, summary_cap, lane);
   __syncwarp();
-  bool zero_seen = false;
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   for (int64_t col = warp; col < a.b.cols; col += warps) {
@@ -696,14 +679,11 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
     const int32_t lo = a.win_lo[col];
     const int64_t bs = a.b.ptr[col];
     const int64_t be = a.b.ptr[col + 1];
-    bool displaced = false;
-    if (!a.count_only) {
-      ClearTable(hkeys, hash_slots, lane);
-      __syncwarp();
-      bool placed = true;
-      for (int64_t p = bs + lane; p < be; p += kWarp) placed &= BucketInsert(hkeys, hvals, hbits, a.b.idx[p], a.b.val[p]);
-      displaced = !__all_sync(0xffffffffu, placed);
-    }
+    ClearTable(hkeys, hash_slots, lane);
+    __syncwarp();
+    bool placed = true;
+    for (int64_t p = bs + lane; p < be; p += kWarp) placed &= BucketInsert(hkeys, hvals, hbits, a.b.idx[p], a.b.val[p]);
+    const bool displaced = !__all_sync(0xffffffffu, placed);
     if (a.add_diag && lane == 0) MarkRow(bm, summary, static_cast<int>(col) - lo);
     if constexpr (kEll > 0) {
       for (int64_t p = bs + lane; p < be; p += kWarp) {
@@ -734,17 +714,17 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
       }
     }
     __syncwarp();
-    const int count = DrainRows(bm, summary, SummaryWords(words), lo, a.count_only ? nullptr : rows, lane);
-    if (a.count_only) {
-      if (lane == 0) a.counts[col] = count;
-      continue;
-    }
+    const int count = DrainRows(bm, summary, SummaryWords(words), lo, rows, lane);
     const int64_t c0 = projection ? 0 : a.c_ptr[col];
+    int kept = 0;
     double sq = 0.0;
     double tt = 0.0;
     double bt = 0.0;
     for (int r0 = 0; r0 < count; r0 += kWarp) {
       const int r = r0 + lane;
+      bool have = false;
+      int32_t row_out = 0;
+      T stored = T(0);
       if (r < count) {
         const int32_t i = rows[r];
         double acc = -0.0;
@@ -789,16 +769,27 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
             v = -acc;
             if (static_cast<int64_t>(i) == col) v = Add(v, 1.0);
           }
-          const T stored = static_cast<T>(v);
-          a.c_idx[c0 + r] = i;
-          a.c_val[c0 + r] = stored;
-          if (a.z_val != nullptr) {
-            a.z_val[c0 + r] = static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(stored)));
-          }
-          if (a.prune && fabs(static_cast<double>(stored)) <= 0.0) zero_seen = true;
+          stored = static_cast<T>(v);
+          row_out = i;
+          have = true;
           const double sd = static_cast<double>(stored);
           stage0[lane] = Mul(sd, sd);
         }
+      }
+      if (!projection) {
+        // Eigen prune(0.0): exact zeros leave C (they add nothing to the column sums)
+        const bool keep = have && !(a.prune && fabs(static_cast<double>(stored)) <= 0.0);
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int64_t o = c0 + kept + __popc(mask & LaneMaskBelow());
+          a.c_idx[o] = row_out;
+          a.c_val[o] = stored;
+          if (a.z_val != nullptr) {
+            a.z_val[o] =
+                static_cast<T>(Mul(static_cast<double>(a.row_scale[row_out]), static_cast<double>(stored)));
+          }
+        }
+        kept += __popc(mask);
       }
       if (sums) {
         // sequential in row order; lane 0 sums stage0, lane 1 (projection) stage1
@@ -832,29 +823,41 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
     if (projection) {
       if (lane == 0) a.proj_tt[col] = tt;
       if (lane == 1) a.proj_bt[col] = bt;
-    } else if (lane == 0 && a.col_squares != nullptr) {
-      a.col_squares[col] = sq;
+    } else if (lane == 0) {
+      a.counts[col] = kept;
+      if (a.col_squares != nullptr) a.col_squares[col] = sq;
     }
     __syncwarp();
   }
-  if (__any_sync(0xffffffffu, zero_seen) && lane == 0) atomicOr(a.flag, 1);
 }
 
 // ---------------------------------------------------------------------------
 // Hash need, window and bin populations of every output column.
+// Thread per output column (every column in flight at once): candidate
+// count, row window and bin; block-level reduction of the maxima, the sum of
+// the upper bounds and the bin populations.
 template <class T>
-__global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ need,
-                           int32_t* __restrict__ win_lo, int32_t* __restrict__ win_words,
-                           unsigned long long* __restrict__ maxima) {
+__global__ void __launch_bounds__(256) NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ need,
+                                                  int64_t* __restrict__ ub, int32_t* __restrict__ win_lo,
+                                                  int32_t* __restrict__ win_words,
+                                                  unsigned long long* __restrict__ maxima) {
+  __shared__ unsigned long long block_max[3];  // max ub, max nnz(B col), sum of ub
+  __shared__ unsigned long long block_pop[kWordBinCount + 1];
+  if (threadIdx.x < 3) block_max[threadIdx.x] = 0ull;
+  if (threadIdx.x < kWordBinCount + 1) block_pop[threadIdx.x] = 0ull;
+  __syncthreads();
   unsigned long long local_ub = 0;
   unsigned long long local_nb = 0;
+  unsigned long long local_sum = 0;
   unsigned long long population[kWordBinCount + 1] = {};
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < b.cols;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t bs = b.ptr[j];
+    const int64_t be = b.ptr[j + 1];
     int64_t u = add_diag ? 1 : 0;
     int32_t lo = add_diag ? static_cast<int32_t>(j) : INT32_MAX;
     int32_t hi = add_diag ? static_cast<int32_t>(j) : -1;
-    for (int64_t p = b.ptr[j]; p < b.ptr[j + 1]; ++p) {
+    for (int64_t p = bs; p < be; ++p) {
       const int32_t k = b.idx[p];
       const int64_t xs = x.ptr[k];
       const int64_t xe = x.ptr[k + 1];
@@ -864,33 +867,50 @@ __global__ void NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* _
         hi = max(hi, x.idx[xe - 1]);
       }
     }
-    need[j] = 2 * u;
     int words = 0;
     if (hi >= lo) {
       const int64_t w = (static_cast<int64_t>(hi) - lo) / 32 + 1;
       words = w > INT32_MAX ? INT32_MAX : static_cast<int>(w);
     }
+    need[j] = 2 * u;
+    ub[j] = u;
     win_lo[j] = hi >= lo ? lo : 0;
     win_words[j] = words;
     // bins: <= 128, 512, 1040, 2048 words (kWordBins), else the hash path
-    if (words <= 128) {
-      ++population[0];
-    } else if (words <= 512) {
-      ++population[1];
-    } else if (words <= 1040) {
-      ++population[2];
-    } else if (words <= kBitmapMaxWords) {
-      ++population[3];
-    } else {
-      ++population[4];
-    }
+    const int bin = words <= 128 ? 0 : (words <= 512 ? 1 : (words <= 1040 ? 2 : (words <= kBitmapMaxWords ? 3 : 4)));
+#pragma unroll
+    for (int i = 0; i <= kWordBinCount; ++i) population[i] += bin == i ? 1ull : 0ull;
+    local_sum += static_cast<unsigned long long>(u);
     local_ub = max(local_ub, static_cast<unsigned long long>(u));
-    local_nb = max(local_nb, static_cast<unsigned long long>(b.ptr[j + 1] - b.ptr[j]));
+    local_nb = max(local_nb, static_cast<unsigned long long>(be - bs));
   }
-  WarpAtomicMax(&maxima[kMaxUb], local_ub);
-  WarpAtomicMax(&maxima[kMaxNb], local_nb);
-  for (int i = 0; i < kWordBinCount; ++i) WarpAtomicAdd(&maxima[kPopulation + i], population[i]);
-  WarpAtomicAdd(&maxima[kHashColumns], population[kWordBinCount]);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    local_ub = max(local_ub, __shfl_xor_sync(0xffffffffu, local_ub, o));
+    local_nb = max(local_nb, __shfl_xor_sync(0xffffffffu, local_nb, o));
+    local_sum += __shfl_xor_sync(0xffffffffu, local_sum, o);
+#pragma unroll
+    for (int i = 0; i <= kWordBinCount; ++i) population[i] += __shfl_xor_sync(0xffffffffu, population[i], o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    atomicMax(&block_max[0], local_ub);
+    atomicMax(&block_max[1], local_nb);
+    if (local_sum != 0ull) atomicAdd(&block_max[2], local_sum);
+#pragma unroll
+    for (int i = 0; i <= kWordBinCount; ++i) {
+      if (population[i] != 0ull) atomicAdd(&block_pop[i], population[i]);
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (block_max[0] != 0ull) atomicMax(&maxima[kMaxUb], block_max[0]);
+    if (block_max[1] != 0ull) atomicMax(&maxima[kMaxNb], block_max[1]);
+    if (block_max[2] != 0ull) atomicAdd(&maxima[kSumUb], block_max[2]);
+    for (int i = 0; i < kWordBinCount; ++i) {
+      if (block_pop[i] != 0ull) atomicAdd(&maxima[kPopulation + i], block_pop[i]);
+    }
+    if (block_pop[kWordBinCount] != 0ull) atomicAdd(&maxima[kHashColumns], block_pop[kWordBinCount]);
+  }
 }
 
 template <class T>
@@ -1019,9 +1039,10 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   ctx.sg_win_words.Reserve(static_cast<size_t>(cols), ctx.stream);
   ctx.sg_maxima.Reserve(kMaximaSlots, ctx.stream);
   SPAI_CUDA(cudaMemsetAsync(ctx.sg_maxima.data(), 0, kMaximaSlots * sizeof(unsigned long long), ctx.stream));
-  NeedKernel<T><<<GridFor(cols, 128), 128, 0, ctx.stream>>>(View(x_csc), View(b), residual, ctx.sg_need.data(),
-                                                           ctx.sg_win_lo.data(), ctx.sg_win_words.data(),
-                                                           ctx.sg_maxima.data());
+  NeedKernel<T><<<GridFor(cols, 256), 256, 0, ctx.stream>>>(View(x_csc), View(b), residual,
+                                                                   ctx.sg_need.data(), ctx.sg_counts.data(),
+                                                                   ctx.sg_win_lo.data(), ctx.sg_win_words.data(),
+                                                                   ctx.sg_maxima.data());
   SPAI_LAUNCH_CHECK();
   unsigned long long host_max[kMaximaSlots];
   SPAI_CUDA(cudaMemcpyAsync(host_max, ctx.sg_maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
@@ -1050,7 +1071,6 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   ca.col_squares = extras.col_squares;
   ca.proj_tt = extras.proj_tt;
   ca.proj_bt = extras.proj_bt;
-  ca.flag = ctx.flags.data();
   ca.x_cols_ell = extras.x_cols_ell;
   ca.x_rows_ell = extras.x_rows_ell;
   ca.x_rows_ell_val = static_cast<const T*>(extras.x_rows_ell_val);
@@ -1066,6 +1086,60 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
     LaunchColumnProducts(ctx, ca, host_max, rows_cap, hash_slots);
     return false;
   }
+  if (column_path) {
+    // one pass into padded columns (offsets: scan of the upper bounds NeedKernel left in sg_counts),
+    // then one scan of the surviving lengths and a compaction
+    const int64_t padded = static_cast<int64_t>(host_max[kSumUb]);
+    const size_t slots = static_cast<size_t>(padded > 0 ? padded : 1);
+    ctx.sg_ub_ptr.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+    ctx.sg_pad_idx.Reserve(slots, ctx.stream);
+    ctx.sg_pad_val.Reserve(slots * sizeof(T), ctx.stream);
+    if (want_z) ctx.sg_pad_z.Reserve(slots * sizeof(T), ctx.stream);
+    ScanCountsAsync(ctx, ctx.sg_counts.data(), cols, ctx.sg_ub_ptr.data());
+    T* pad_val = reinterpret_cast<T*>(ctx.sg_pad_val.data());
+    T* pad_z = want_z ? reinterpret_cast<T*>(ctx.sg_pad_z.data()) : nullptr;
+    ca.c_ptr = ctx.sg_ub_ptr.data();
+    ca.c_idx = ctx.sg_pad_idx.data();
+    ca.c_val = pad_val;
+    ca.z_val = pad_z;
+    ca.counts = ctx.sg_counts.data();
+    DevCsc<T> result;
+    result.Shape(x_csc.rows, cols, ctx.stream);
+    int64_t nnz = 0;
+    {
+      prof::Scope scope(ctx.stream, "spgemm_numeric", 0.0);
+      LaunchColumnProducts(ctx, ca, host_max, rows_cap, hash_slots);
+    }
+    nnz = ScanCounts(ctx, ctx.sg_counts.data(), cols, result.ptr.data());
+    result.ReserveNnz(nnz, ctx.stream);
+    {
+      // the numeric pass: |X| + |B| read, C (and Z, the column sums) written once
+      double bytes = operand_bytes + MatrixBytes<T>(nnz, cols);
+      if (want_z) bytes += static_cast<double>(nnz) * sizeof(T);
+      if (extras.col_squares != nullptr) bytes += static_cast<double>(cols) * sizeof(double);
+      prof::AddBytes("spgemm_numeric", bytes);
+    }
+    {
+      // the compaction reads and writes C (and Z) once more
+      double bytes = 2.0 * MatrixBytes<T>(nnz, cols);
+      if (want_z) bytes += 2.0 * static_cast<double>(nnz) * (sizeof(T) + sizeof(int32_t));
+      prof::Scope scope(ctx.stream, "spgemm_compact", bytes);
+      CompactPadded(ctx, ctx.sg_ub_ptr.data(), static_cast<const int64_t*>(nullptr), cols, result.ptr.data(),
+                    ctx.sg_pad_idx.data(), pad_val, result.idx.data(), result.val.data());
+      if (want_z) {
+        DevCsc<T> z;
+        z.Shape(result.rows, cols, ctx.stream);
+        z.ReserveNnz(nnz, ctx.stream);
+        SPAI_CUDA(cudaMemcpyAsync(z.ptr.data(), result.ptr.data(), sizeof(int64_t) * (cols + 1),
+                                  cudaMemcpyDeviceToDevice, ctx.stream));
+        CompactPadded(ctx, ctx.sg_ub_ptr.data(), static_cast<const int64_t*>(nullptr), cols, z.ptr.data(),
+                      ctx.sg_pad_idx.data(), pad_z, z.idx.data(), z.val.data());
+        c_z->Swap(z);
+      }
+    }
+    c.Swap(result);
+    return want_z;
+  }
 
   RowSetArgs<T> rs{};
   rs.x = View(x_csc);
@@ -1077,15 +1151,8 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   rs.counts = ctx.sg_counts.data();
   {
     prof::Scope scope(ctx.stream, "spgemm_symbolic", 0.0);
-    if (column_path) {
-      ColumnArgs<T> cc = ca;
-      cc.count_only = true;
-      cc.counts = ctx.sg_counts.data();
-      LaunchColumnProducts(ctx, cc, host_max, rows_cap, hash_slots);
-    } else {
-      rs.list = false;
-      LaunchRowSets(ctx, rs, host_max);
-    }
+    rs.list = false;
+    LaunchRowSets(ctx, rs, host_max);
   }
 
   // output layout: C, or the transient row list of the projection
@@ -1124,13 +1191,7 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
       if (extras.col_squares != nullptr) bytes += static_cast<double>(cols) * sizeof(double);
     }
     prof::Scope scope(ctx.stream, "spgemm_numeric", bytes);
-    if (column_path) {
-      ca.c_ptr = c_ptr;
-      ca.c_idx = rows;
-      ca.c_val = vals;
-      ca.z_val = want_z ? zbuf.data() : nullptr;
-      LaunchColumnProducts(ctx, ca, host_max, rows_cap, hash_slots);
-    } else {
+    {
       ctx.sg_cols.Reserve(static_cast<size_t>(nnz > 0 ? nnz : 1), ctx.stream);
       rs.list = true;
       rs.c_ptr = c_ptr;

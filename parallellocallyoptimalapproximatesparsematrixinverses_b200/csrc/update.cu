@@ -234,50 +234,119 @@ __device__ __forceinline__ int LowerBoundShared(const int32_t* keys, int n, int3
   return lo;
 }
 
-// MatchedPrefix and MergeColumn (half sums) over row keys staged in shared
-// memory; values are read from the input columns.
+// MatchedPrefix and MergeColumn over row keys staged in shared memory
+// (yk, xk: the two columns' rows; pre: nx + 1 ints); values are read from
+// the input columns.  Emits nothing and returns the merged length when it
+// exceeds `cap`.
 template <class T, class Emit>
-__device__ int MergeHalfSumShared(const CscView<T>& y, const CscView<T>& x, int64_t j, DropSlab& s, int lane,
-                                  Emit emit) {
+__device__ int MergeShared(const CscView<T>& y, const CscView<T>& x, int64_t j, int32_t* yk, int32_t* xk, int* pre,
+                           bool scale_y, double ys_scale, double xs_scale, bool half_sum, int cap, int lane,
+                           Emit emit) {
   const int64_t ys = y.ptr[j];
   const int64_t xs = x.ptr[j];
   const int ny = static_cast<int>(y.ptr[j + 1] - ys);
   const int nx = static_cast<int>(x.ptr[j + 1] - xs);
-  for (int i = lane; i < ny; i += kWarp) s.yk[i] = y.idx[ys + i];
-  for (int i = lane; i < nx; i += kWarp) s.xk[i] = x.idx[xs + i];
+  for (int i = lane; i < ny; i += kWarp) yk[i] = y.idx[ys + i];
+  for (int i = lane; i < nx; i += kWarp) xk[i] = x.idx[xs + i];
   __syncwarp();
   int running = 0;
   for (int base = 0; base < nx; base += kWarp) {
     const int q = base + lane;
     bool hit = false;
     if (q < nx) {
-      const int32_t row = s.xk[q];
-      const int r = LowerBoundShared(s.yk, ny, row);
-      hit = r < ny && s.yk[r] == row;
+      const int32_t row = xk[q];
+      const int r = LowerBoundShared(yk, ny, row);
+      hit = r < ny && yk[r] == row;
     }
     const unsigned mask = __ballot_sync(0xffffffffu, hit);
-    if (q < nx) s.mx_prefix[q] = running + __popc(mask & LaneMaskBelow());
+    if (q < nx) pre[q] = running + __popc(mask & LaneMaskBelow());
     running += __popc(mask);
   }
-  if (lane == 0) s.mx_prefix[nx] = running;
+  if (lane == 0) pre[nx] = running;
   __syncwarp();
   const int merged = ny + nx - running;
-  if (merged > kDropCap) return merged;
+  if (merged > cap) return merged;
   for (int p = lane; p < ny; p += kWarp) {
-    const int32_t row = s.yk[p];
-    const int r = LowerBoundShared(s.xk, nx, row);
+    const int32_t row = yk[p];
+    const int r = LowerBoundShared(xk, nx, row);
     const double yv = static_cast<double>(y.val[ys + p]);
-    const double v = (r < nx && s.xk[r] == row) ? Both(yv, static_cast<double>(x.val[xs + r]), false, 1.0, 1.0, true)
-                                                : LeftOnly(yv, false, 1.0, true);
-    emit(p + r - s.mx_prefix[r], row, v);
+    const double v = (r < nx && xk[r] == row)
+                         ? Both(yv, static_cast<double>(x.val[xs + r]), scale_y, ys_scale, xs_scale, half_sum)
+                         : LeftOnly(yv, scale_y, ys_scale, half_sum);
+    emit(p + r - pre[r], row, v);
   }
   for (int q = lane; q < nx; q += kWarp) {
-    const int32_t row = s.xk[q];
-    const int r = LowerBoundShared(s.yk, ny, row);
-    if (r < ny && s.yk[r] == row) continue;
-    emit(q - s.mx_prefix[q] + r, row, RightOnly(static_cast<double>(x.val[xs + q]), 1.0, true));
+    const int32_t row = xk[q];
+    const int r = LowerBoundShared(yk, ny, row);
+    if (r < ny && yk[r] == row) continue;
+    emit(q - pre[q] + r, row, RightOnly(static_cast<double>(x.val[xs + q]), xs_scale, half_sum));
   }
   return merged;
+}
+
+constexpr int kUnionPadCap = 512;  // longest input column of the single-pass union
+
+// Single-pass union: column j of the result goes to out at y.ptr[j] +
+// x.ptr[j] (an upper bound of its offset); exact zeros are pruned in place
+// (kAxpby) and counts[j] is the surviving length.  Columns with an input
+// longer than kUnionPadCap set `overflow` (the caller then uses the
+// two-pass kernels).
+template <class T>
+__global__ void UnionPaddedKernel(CscView<T> y, CscView<T> x, bool scale_y, double ys_scale, double xs_scale,
+                                  bool half_sum, bool prune, int64_t* __restrict__ counts,
+                                  int32_t* __restrict__ out_idx, T* __restrict__ out_val,
+                                  int32_t* __restrict__ overflow) {
+  extern __shared__ __align__(16) int32_t union_pad_smem[];
+  const int lane = threadIdx.x & 31;
+  int32_t* yk = union_pad_smem + (threadIdx.x >> 5) * (3 * kUnionPadCap + 4);
+  int32_t* xk = yk + kUnionPadCap;
+  int* pre = xk + kUnionPadCap;
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  for (int64_t j = warp; j < y.cols; j += warps) {
+    const int64_t ny = y.ptr[j + 1] - y.ptr[j];
+    const int64_t nx = x.ptr[j + 1] - x.ptr[j];
+    if (ny > kUnionPadCap || nx > kUnionPadCap) {
+      if (lane == 0) atomicOr(overflow, 1);
+      continue;
+    }
+    const int64_t base = y.ptr[j] + x.ptr[j];
+    bool zero = false;
+    const int merged = MergeShared(y, x, j, yk, xk, pre, scale_y, ys_scale, xs_scale, half_sum, 2 * kUnionPadCap,
+                                   lane, [&](int rank, int32_t row, double v) {
+                                     const T stored = static_cast<T>(v);
+                                     out_idx[base + rank] = row;
+                                     out_val[base + rank] = stored;
+                                     if (prune && fabs(static_cast<double>(stored)) <= 0.0) zero = true;
+                                   });
+    int kept = merged;
+    if (__any_sync(0xffffffffu, zero)) {
+      // rare: squeeze the exact zeros out of this column, in order
+      __syncwarp();
+      int64_t at = base;
+      for (int i0 = 0; i0 < merged; i0 += kWarp) {
+        const int i = i0 + lane;
+        int32_t r = 0;
+        T v = T(0);
+        if (i < merged) {
+          r = out_idx[base + i];
+          v = out_val[base + i];
+        }
+        const bool keep = i < merged && !(fabs(static_cast<double>(v)) <= 0.0);
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        __syncwarp();
+        if (keep) {
+          out_idx[at + __popc(mask & LaneMaskBelow())] = r;
+          out_val[at + __popc(mask & LaneMaskBelow())] = v;
+        }
+        at += __popc(mask);
+        __syncwarp();
+      }
+      kept = static_cast<int>(at - base);
+    }
+    if (lane == 0) counts[j] = kept;
+    __syncwarp();
+  }
 }
 
 // (|v| bits, position) ordering; the position breaks ties exactly as the row does.
@@ -451,7 +520,8 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
         if (lane == 0) atomicOr(overflow, 1);
         continue;
       }
-      const int merged = MergeHalfSumShared(m, mt, j, s, lane, [&](int rank, int32_t row, double v) {
+      const int merged = MergeShared(m, mt, j, s.yk, s.xk, s.mx_prefix, false, 1.0, 1.0, true, kDropCap, lane,
+                                     [&](int rank, int32_t row, double v) {
         s.keys[rank] = row;
         s.vals[rank] = static_cast<double>(static_cast<T>(v));  // the value M would store
       });
@@ -542,26 +612,6 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
   }
 }
 
-// out(:, j) = the first counts[j] entries at ub_ptr[j] of the padded arrays.
-template <class T>
-__global__ void CompactColumnsKernel(const int64_t* __restrict__ m_ptr, const int64_t* __restrict__ mt_ptr,
-                                     int64_t cols, const int64_t* __restrict__ out_ptr,
-                                     const int32_t* __restrict__ src_idx, const T* __restrict__ src_val,
-                                     int32_t* __restrict__ dst_idx, T* __restrict__ dst_val) {
-  const int lane = threadIdx.x & 31;
-  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
-  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t j = warp; j < cols; j += warps) {
-    const int64_t from = m_ptr[j] + (mt_ptr != nullptr ? mt_ptr[j] : 0);
-    const int64_t to = out_ptr[j];
-    const int64_t n = out_ptr[j + 1] - to;
-    for (int64_t i = lane; i < n; i += kWarp) {
-      dst_idx[to + i] = src_idx[from + i];
-      dst_val[to + i] = src_val[from + i];
-    }
-  }
-}
-
 }  // namespace
 
 int UnionWarpCap() { return kUnionWarpCap; }
@@ -580,6 +630,37 @@ void UnionWriteWarp(Ctx& ctx, const DevCsc<T>& y, const DevCsc<T>& x, bool scale
   UnionWriteWarpKernel<T><<<GridFor(y.cols * kWarp, kWarps * kWarp), kWarps * kWarp, smem, ctx.stream>>>(
       View(y), View(x), scale_y, ys, xs, half_sum, prune, out.ptr.data(), out.idx.data(), out.val.data(), flag);
   SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+bool UnionPadded(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T>& x, double xs, bool half_sum,
+                 bool prune, DevCsc<T>& out) {
+  const int64_t cols = y.cols;
+  const int64_t padded = y.nnz + x.nnz;
+  DevBuf<int32_t> tmp_idx;
+  DevBuf<T> tmp_val;
+  tmp_idx.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
+  tmp_val.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
+  ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
+  int32_t* overflow = ctx.flags.data() + 2;
+  SPAI_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int32_t), ctx.stream));
+  constexpr int kWarps = 8;
+  const size_t smem = static_cast<size_t>(kWarps) * (3 * kUnionPadCap + 4) * sizeof(int32_t);
+  SPAI_CUDA(cudaFuncSetAttribute(UnionPaddedKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(smem)));
+  const int grid = GridFor(cols * kWarp, kWarps * kWarp);
+  UnionPaddedKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, half_sum, prune,
+                                                                   ctx.counts.data(), tmp_idx.data(), tmp_val.data(),
+                                                                   overflow);
+  SPAI_LAUNCH_CHECK();
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 2, overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+  out.Shape(y.rows, cols, ctx.stream);
+  const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());  // synchronises: flag is read
+  if (ctx.host_flags[2] != 0) return false;
+  out.ReserveNnz(nnz, ctx.stream);
+  CompactPadded(ctx, y.ptr.data(), x.ptr.data(), cols, out.ptr.data(), tmp_idx.data(), tmp_val.data(), out.idx.data(),
+                out.val.data());
+  return true;
 }
 
 template <class T>
@@ -613,10 +694,8 @@ bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk) {
   const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());  // synchronises: flag is read
   if (ctx.host_flags[1] != 0) return false;
   out.ReserveNnz(nnz, ctx.stream);
-  CompactColumnsKernel<T><<<grid, kWarps * kWarp, 0, ctx.stream>>>(m.ptr.data(), symmetric ? mt.ptr.data() : nullptr,
-                                                                   cols, out.ptr.data(), tmp_idx.data(),
-                                                                   tmp_val.data(), out.idx.data(), out.val.data());
-  SPAI_LAUNCH_CHECK();
+  CompactPadded(ctx, m.ptr.data(), symmetric ? mt.ptr.data() : nullptr, cols, out.ptr.data(), tmp_idx.data(),
+                tmp_val.data(), out.idx.data(), out.val.data());
   m.Swap(out);
   return true;
 }
@@ -627,6 +706,10 @@ template void UnionWriteWarp<double>(Ctx&, const DevCsc<double>&, const DevCsc<d
                                      bool, DevCsc<double>&, int32_t*);
 template void UnionWriteWarp<float>(Ctx&, const DevCsc<float>&, const DevCsc<float>&, bool, double, double, bool, bool,
                                     DevCsc<float>&, int32_t*);
+template bool UnionPadded<double>(Ctx&, const DevCsc<double>&, bool, double, const DevCsc<double>&, double, bool,
+                                  bool, DevCsc<double>&);
+template bool UnionPadded<float>(Ctx&, const DevCsc<float>&, bool, double, const DevCsc<float>&, double, bool, bool,
+                                 DevCsc<float>&);
 template bool SymmetrizeAndDrop<double>(Ctx&, DevCsc<double>&, bool, int64_t);
 template bool SymmetrizeAndDrop<float>(Ctx&, DevCsc<float>&, bool, int64_t);
 

@@ -120,3 +120,29 @@ def test_mixed_precision_error_against_fp64_oracle(require_gpu, family, name, to
     m_err = relative_difference(got.M, want.M)
     assert hist_err <= 1e-4, f"{family}.{name} top-{topk}: history rel error {hist_err:.3e}"
     assert m_err <= 1e-4, f"{family}.{name} top-{topk}: M rel error {m_err:.3e}"
+
+
+@pytest.mark.parametrize("topk", [0, 10])
+def test_fp64_reference_cpu_configuration(require_gpu, topk):
+    """The reference's own CPU-runnable case: 5-point Laplacian 64 x 64 (n = 4096),
+    M0 = diag(A)^-1, Global MR for 20 iterations with dropping to 10 entries per
+    column (global budget max_density = 10/n, or per-column top-10), then PCG
+    to 1e-8 with the symmetric part of M on b = A x*, x* ~ N(0, 1) (seed 0)."""
+    from scipy import sparse
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import backward_error
+    A = problems.laplacian_2d(64)
+    n = A.shape[0]
+    M0 = problems.diagonal_inverse(A)
+    got, want = _run_both("global_spai", "mr", A, M0, None, topk=topk, max_iterations=20, tolerance=1e-12,
+                          max_density=10.0 / n)
+    assert_same_result(got, want, f"laplacian 64x64 top-{topk}")
+    msym = sparse.csr_matrix((got.M + got.M.T) * 0.5)
+    msym.sort_indices()
+    a = sparse.csr_matrix(A)
+    a.sort_indices()
+    b, _ = problems.solution_rhs(A, seed=0)
+    hist, status = backward_error.pcg(a.data, a.indices, a.indptr, msym.data, msym.indices, msym.indptr, b, 2000, 1,
+                                      1e-8)
+    want_hist, want_status = pyoracle.pcg(a, msym, b, 2000, 1e-8, order=pyoracle.ORDER_DEVICE)
+    assert status == want_status == 1
+    assert np.array_equal(hist.view(np.int64), want_hist.view(np.int64))
