@@ -36,6 +36,16 @@ class CudaError : public std::runtime_error {
 // Counts every kernel launch of the library (reported by spai_kernel_launches).
 void CountLaunch();
 
+// Per-stream cache of released device blocks.  A block released on stream s
+// is handed to the next allocation on s that fits it (at least the request,
+// at most twice it): stream order makes the reuse safe without events, and
+// the iteration loop, whose buffers recur at similar sizes every step, stops
+// calling the allocator.  CacheFlush frees a stream's blocks (before the
+// stream is destroyed).
+void* CacheTake(cudaStream_t stream, size_t bytes, size_t* capacity_bytes);
+void CacheGive(cudaStream_t stream, void* block, size_t bytes);
+void CacheFlush(cudaStream_t stream);
+
 #define SPAI_LAUNCH_CHECK()          \
   do {                               \
     ::spai::CountLaunch();           \
@@ -50,9 +60,8 @@ inline int64_t CeilDiv(int64_t a, int64_t b) { return (a + b - 1) / b; }
 // times, never more than the work needs.
 int GridFor(int64_t work_items, int threads_per_block);
 
-// Stream-ordered device buffer backed by the device's default memory pool
-// (cudaMallocAsync); the pool keeps freed blocks, so re-growing buffers
-// inside the iteration loop does not reach the driver allocator.
+// Stream-ordered device buffer: blocks come from the per-stream cache above,
+// else from the device's default memory pool (cudaMallocAsync).
 template <class T>
 class DevBuf {
  public:
@@ -78,15 +87,22 @@ class DevBuf {
     }
     Release();
     const size_t cap = n + n / 4 + 64;
-    SPAI_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr_), cap * sizeof(T), stream));
-    capacity_ = cap;
+    size_t got = 0;
+    void* block = CacheTake(stream, cap * sizeof(T), &got);
+    if (block != nullptr) {
+      ptr_ = static_cast<T*>(block);
+      capacity_ = got / sizeof(T);
+    } else {
+      SPAI_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ptr_), cap * sizeof(T), stream));
+      capacity_ = cap;
+    }
     size_ = n;
     stream_ = stream;
   }
 
   void Release() {
     if (ptr_ != nullptr) {
-      cudaFreeAsync(ptr_, stream_);
+      CacheGive(stream_, ptr_, capacity_ * sizeof(T));
       ptr_ = nullptr;
     }
     capacity_ = 0;

@@ -8,6 +8,8 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <limits>
 
 #include "device.cuh"
@@ -184,24 +186,25 @@ __global__ void ColumnDotsKernel(CscView<T> x, CscView<T> y, double* __restrict_
 
 // ---------------------------------------------------------------------------
 // Union (thread per column, two phases)
+// Values in the storage type's arithmetic (FP64 for double, FP32 for float storage).
 template <class T>
-__device__ __forceinline__ double UnionBoth(double y, double x, bool scale_y, double ys, double xs, int mode) {
-  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(0.5, Add(y, x));
-  const double yv = scale_y ? Mul(ys, y) : y;
+__device__ __forceinline__ T UnionBoth(T y, T x, bool scale_y, T ys, T xs, int mode) {
+  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(T(0.5), Add(y, x));
+  const T yv = scale_y ? Mul(ys, y) : y;
   return Add(yv, Mul(xs, x));
 }
 
 template <class T>
-__device__ __forceinline__ double UnionLeft(double y, bool scale_y, double ys, int mode) {
-  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(0.5, Add(y, 0.0));
-  const double yv = scale_y ? Mul(ys, y) : y;
-  return Add(yv, 0.0);
+__device__ __forceinline__ T UnionLeft(T y, bool scale_y, T ys, int mode) {
+  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(T(0.5), Add(y, T(0)));
+  const T yv = scale_y ? Mul(ys, y) : y;
+  return Add(yv, T(0));
 }
 
 template <class T>
-__device__ __forceinline__ double UnionRight(double x, double xs, int mode) {
-  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(0.5, Add(0.0, x));
-  return Add(0.0, Mul(xs, x));
+__device__ __forceinline__ T UnionRight(T x, T xs, int mode) {
+  if (mode == static_cast<int>(UnionMode::kHalfSum)) return Mul(T(0.5), Add(T(0), x));
+  return Add(T(0), Mul(xs, x));
 }
 
 // One thread per column: used for columns whose X part is longer than the
@@ -220,25 +223,26 @@ __global__ void UnionKernel(CscView<T> y, CscView<T> x, bool scale_y, double ys,
     const int64_t qe = x.ptr[j + 1];
     int64_t o = kWrite ? out_ptr[j] : 0;
     int64_t count = 0;
+    const T yst = static_cast<T>(ys);
+    const T xst = static_cast<T>(xs);
     while (p < pe || q < qe) {
       int32_t row;
-      double v;
+      T stored;
       if (p < pe && q < qe && y.idx[p] == x.idx[q]) {
         row = y.idx[p];
-        v = UnionBoth<T>(static_cast<double>(y.val[p]), static_cast<double>(x.val[q]), scale_y, ys, xs, mode);
+        stored = UnionBoth<T>(y.val[p], x.val[q], scale_y, yst, xst, mode);
         ++p;
         ++q;
       } else if (p < pe && (q >= qe || y.idx[p] < x.idx[q])) {
         row = y.idx[p];
-        v = UnionLeft<T>(static_cast<double>(y.val[p]), scale_y, ys, mode);
+        stored = UnionLeft<T>(y.val[p], scale_y, yst, mode);
         ++p;
       } else {
         row = x.idx[q];
-        v = UnionRight<T>(static_cast<double>(x.val[q]), xs, mode);
+        stored = UnionRight<T>(x.val[q], xst, mode);
         ++q;
       }
-      const T stored = static_cast<T>(v);
-      if (prune && fabs(static_cast<double>(stored)) <= 0.0) continue;
+      if (prune && stored == T(0)) continue;
       if (kWrite) {
         out_idx[o] = row;
         out_val[o] = stored;
@@ -489,7 +493,7 @@ __global__ void DiagScaleKernel(const T* __restrict__ d, const int32_t* __restri
                                 int64_t nnz, T* __restrict__ out) {
   for (int64_t p = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; p < nnz;
        p += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    out[p] = static_cast<T>(Mul(static_cast<double>(d[idx[p]]), static_cast<double>(val[p])));
+    out[p] = Mul(d[idx[p]], val[p]);
   }
 }
 
@@ -497,10 +501,8 @@ template <class T>
 __global__ void ScaleColumnsKernel(CscView<T> x, T* __restrict__ val, const double* __restrict__ scale) {
   for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
        j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const double s = scale[j];
-    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) {
-      val[p] = static_cast<T>(Mul(static_cast<double>(val[p]), s));
-    }
+    const T s = static_cast<T>(scale[j]);
+    for (int64_t p = x.ptr[j]; p < x.ptr[j + 1]; ++p) val[p] = Mul(val[p], s);
   }
 }
 
@@ -937,6 +939,52 @@ int GridFor(int64_t work_items, int threads_per_block) {
   return static_cast<int>(needed < cap ? needed : cap);
 }
 
+namespace {
+struct CachedBlock {
+  void* ptr;
+  size_t bytes;
+};
+constexpr size_t kCacheBlocksPerStream = 64;
+std::mutex g_cache_mutex;
+std::map<cudaStream_t, std::vector<CachedBlock>> g_block_cache;
+}  // namespace
+
+void* CacheTake(cudaStream_t stream, size_t bytes, size_t* capacity_bytes) {
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  auto it = g_block_cache.find(stream);
+  if (it == g_block_cache.end()) return nullptr;
+  std::vector<CachedBlock>& blocks = it->second;
+  size_t best = blocks.size();
+  for (size_t i = 0; i < blocks.size(); ++i) {
+    const size_t b = blocks[i].bytes;
+    if (b >= bytes && b <= 2 * bytes + (size_t{1} << 20) && (best == blocks.size() || b < blocks[best].bytes)) best = i;
+  }
+  if (best == blocks.size()) return nullptr;
+  void* p = blocks[best].ptr;
+  *capacity_bytes = blocks[best].bytes;
+  blocks.erase(blocks.begin() + static_cast<std::ptrdiff_t>(best));
+  return p;
+}
+
+void CacheGive(cudaStream_t stream, void* block, size_t bytes) {
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  std::vector<CachedBlock>& blocks = g_block_cache[stream];
+  blocks.push_back(CachedBlock{block, bytes});
+  if (blocks.size() > kCacheBlocksPerStream) {
+    // the oldest block goes back to the pool
+    cudaFreeAsync(blocks.front().ptr, stream);
+    blocks.erase(blocks.begin());
+  }
+}
+
+void CacheFlush(cudaStream_t stream) {
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  auto it = g_block_cache.find(stream);
+  if (it == g_block_cache.end()) return;
+  for (const CachedBlock& b : it->second) cudaFreeAsync(b.ptr, stream);
+  g_block_cache.erase(it);
+}
+
 void Ctx::Init(int device_ordinal) {
   device = device_ordinal;
   SPAI_CUDA(cudaSetDevice(device));
@@ -984,7 +1032,10 @@ void Ctx::Destroy() {
   sg_pad_idx.Release();
   sg_pad_val.Release();
   sg_pad_z.Release();
+  pad_idx.Release();
+  pad_val.Release();
   if (stream != nullptr) {
+    CacheFlush(stream);
     cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
     stream = nullptr;

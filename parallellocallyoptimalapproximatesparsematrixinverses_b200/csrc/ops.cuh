@@ -43,6 +43,8 @@ struct Ctx {
   DevBuf<int32_t> sg_pad_idx;            // padded output rows
   DevBuf<unsigned char> sg_pad_val;      // padded output values
   DevBuf<unsigned char> sg_pad_z;        // padded fused Z values
+  DevBuf<int32_t> pad_idx;               // padded rows of the union and drop steps
+  DevBuf<unsigned char> pad_val;         // padded values of the union and drop steps
   double* host_scalars = nullptr;   // pinned, kScalarSlots
   int64_t* host_counts = nullptr;   // pinned, 8
   int32_t* host_flags = nullptr;    // pinned, 8

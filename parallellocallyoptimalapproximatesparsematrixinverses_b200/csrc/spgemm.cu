@@ -15,6 +15,10 @@
 //     binary search (eight searches in flight per thread), and accumulates
 //     the first product x*y then += x*y in ascending k: the reference's
 //     accumulation order (Eigen's conservative sparse product), no FMA.
+//     Products and sums use the storage type's arithmetic: FP64 for double
+//     storage (bit-compatible with the reference), FP32 multiply and
+//     accumulate for float storage (the mixed-precision form); the global
+//     reductions built from them are FP64 either way.
 //  4. column sums     (one thread per column) -- sequential per-column sums in
 //     row order for the global reductions (||R||^2, the MR projection).
 //
@@ -367,7 +371,7 @@ __global__ void __launch_bounds__(256) ValuesKernel(ValuesArgs<T> a) {
     const int blen = static_cast<int>(a.b.ptr[j + 1] - bs);
     const int64_t xs = a.x_csr.ptr[i];
     const int64_t xe = a.x_csr.ptr[i + 1];
-    double acc = 0.0;
+    T acc = T(0);  // the storage type's arithmetic (see ColumnProductKernel)
     bool has = false;
     for (int64_t q0 = xs; q0 < xe; q0 += 8) {
       int32_t kk[8];
@@ -393,32 +397,29 @@ __global__ void __launch_bounds__(256) ValuesKernel(ValuesArgs<T> a) {
 #pragma unroll
       for (int u = 0; u < 8; ++u) {
         if (blen > 0 && q0 + u < xe && a.b.idx[at[u]] == kk[u]) {
-          const double prod = Mul(static_cast<double>(xv[u]), static_cast<double>(a.b.val[at[u]]));
+          const T prod = Mul(xv[u], a.b.val[at[u]]);
           acc = has ? Add(acc, prod) : prod;
           has = true;
         }
       }
     }
     if (a.mode == static_cast<int>(ValueMode::kMasked)) {
-      a.out_f64[p] = has ? acc : 0.0;
+      a.out_f64[p] = has ? static_cast<double>(acc) : 0.0;
       continue;
     }
     if (a.mode == static_cast<int>(ValueMode::kProjection)) {
-      const T az = static_cast<T>(acc);
-      a.out[p] = static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(az)));
+      a.out[p] = Mul(a.row_scale[i], acc);
       continue;
     }
-    double v = acc;
+    T v = acc;
     if (a.mode == static_cast<int>(ValueMode::kResidual)) {
-      v = has ? -acc : 0.0;
-      if (i == j) v = has ? Add(v, 1.0) : 1.0;
+      v = has ? -acc : T(0);
+      if (i == j) v = has ? Add(v, T(1)) : T(1);
     }
-    const T stored = static_cast<T>(v);
+    const T stored = v;
     a.out[p] = stored;
-    if (a.z_out != nullptr) {
-      a.z_out[p] = static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(stored)));
-    }
-    if (a.prune && fabs(static_cast<double>(stored)) <= 0.0) zero_seen = true;
+    if (a.z_out != nullptr) a.z_out[p] = Mul(a.row_scale[i], stored);
+    if (a.prune && stored == T(0)) zero_seen = true;  // Eigen prune(0.0): +-0 go, NaN stays
   }
   if (__any_sync(0xffffffffu, zero_seen) && (threadIdx.x & 31) == 0) atomicOr(a.flag, 1);
 }
@@ -727,7 +728,8 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
       T stored = T(0);
       if (r < count) {
         const int32_t i = rows[r];
-        double acc = -0.0;
+        // the storage type's arithmetic: FP64 for double storage, FP32 multiply and accumulate for float storage
+        T acc = T(-0.0);
         if constexpr (kEll > 0) {
           const int4* ks = reinterpret_cast<const int4*>(a.x_rows_ell + static_cast<int64_t>(i) * kEll);
           const T* vs = a.x_rows_ell_val + static_cast<int64_t>(i) * kEll;
@@ -740,9 +742,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
 #pragma unroll
             for (int e = 0; e < 4; ++e) {
               T bv;
-              if (kk[e] >= 0 && BucketFind(hkeys, hvals, hbits, displaced, kk[e], bv)) {
-                acc = Add(acc, Mul(static_cast<double>(v4[e]), static_cast<double>(bv)));
-              }
+              if (kk[e] >= 0 && BucketFind(hkeys, hvals, hbits, displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
             }
           }
         } else {
@@ -750,26 +750,22 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
           const int64_t xe = a.x_csr.ptr[i + 1];
           for (int64_t q = xs; q < xe; ++q) {
             T bv;
-            if (BucketFind(hkeys, hvals, hbits, displaced, a.x_csr.idx[q], bv)) {
-              acc = Add(acc, Mul(static_cast<double>(a.x_csr.val[q]), static_cast<double>(bv)));
-            }
+            if (BucketFind(hkeys, hvals, hbits, displaced, a.x_csr.idx[q], bv)) acc = Add(acc, Mul(a.x_csr.val[q], bv));
           }
         }
         if (projection) {
-          const T az = static_cast<T>(acc);
-          const double td = static_cast<double>(
-              static_cast<T>(Mul(static_cast<double>(a.row_scale[i]), static_cast<double>(az))));
+          const double td = static_cast<double>(Mul(a.row_scale[i], acc));
           T zv;
           stage0[lane] = Mul(td, td);
           // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
           stage1[lane] = BucketFind(hkeys, hvals, hbits, displaced, i, zv) ? Mul(static_cast<double>(zv), td) : 0.0;
         } else {
-          double v = acc;
+          T v = acc;
           if (residual) {
             v = -acc;
-            if (static_cast<int64_t>(i) == col) v = Add(v, 1.0);
+            if (static_cast<int64_t>(i) == col) v = Add(v, T(1));
           }
-          stored = static_cast<T>(v);
+          stored = v;
           row_out = i;
           have = true;
           const double sd = static_cast<double>(stored);
@@ -778,16 +774,13 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
       }
       if (!projection) {
         // Eigen prune(0.0): exact zeros leave C (they add nothing to the column sums)
-        const bool keep = have && !(a.prune && fabs(static_cast<double>(stored)) <= 0.0);
+        const bool keep = have && !(a.prune && stored == T(0));
         const unsigned mask = __ballot_sync(0xffffffffu, keep);
         if (keep) {
           const int64_t o = c0 + kept + __popc(mask & LaneMaskBelow());
           a.c_idx[o] = row_out;
           a.c_val[o] = stored;
-          if (a.z_val != nullptr) {
-            a.z_val[o] =
-                static_cast<T>(Mul(static_cast<double>(a.row_scale[row_out]), static_cast<double>(stored)));
-          }
+          if (a.z_val != nullptr) a.z_val[o] = Mul(a.row_scale[row_out], stored);
         }
         kept += __popc(mask);
       }

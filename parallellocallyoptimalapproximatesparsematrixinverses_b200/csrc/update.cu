@@ -51,20 +51,24 @@ __device__ __forceinline__ int64_t LowerBound(const int32_t* idx, int64_t lo, in
   return lo;
 }
 
-// Values of one merged entry, in the arithmetic of the thread-per-column union.
-__device__ __forceinline__ double Both(double y, double x, bool scale_y, double ys, double xs, bool half_sum) {
-  if (half_sum) return Mul(0.5, Add(y, x));
+// Values of one merged entry, in the arithmetic of the thread-per-column
+// union: the storage type's (FP64 for double, FP32 for float storage).
+template <class T>
+__device__ __forceinline__ T Both(T y, T x, bool scale_y, T ys, T xs, bool half_sum) {
+  if (half_sum) return Mul(T(0.5), Add(y, x));
   return Add(scale_y ? Mul(ys, y) : y, Mul(xs, x));
 }
 
-__device__ __forceinline__ double LeftOnly(double y, bool scale_y, double ys, bool half_sum) {
-  if (half_sum) return Mul(0.5, Add(y, 0.0));
-  return Add(scale_y ? Mul(ys, y) : y, 0.0);
+template <class T>
+__device__ __forceinline__ T LeftOnly(T y, bool scale_y, T ys, bool half_sum) {
+  if (half_sum) return Mul(T(0.5), Add(y, T(0)));
+  return Add(scale_y ? Mul(ys, y) : y, T(0));
 }
 
-__device__ __forceinline__ double RightOnly(double x, double xs, bool half_sum) {
-  if (half_sum) return Mul(0.5, Add(0.0, x));
-  return Add(0.0, Mul(xs, x));
+template <class T>
+__device__ __forceinline__ T RightOnly(T x, T xs, bool half_sum) {
+  if (half_sum) return Mul(T(0.5), Add(T(0), x));
+  return Add(T(0), Mul(xs, x));
 }
 
 // Number of rows of X(:, j) also present in Y(:, j) (warp-uniform).
@@ -126,13 +130,10 @@ __device__ void MergeColumn(const CscView<T>& y, const CscView<T>& x, int64_t j,
     const int32_t row = y.idx[p];
     const int64_t r = LowerBound(x.idx, xs, xe, row);
     const int64_t rank = (p - ys) + (r - xs) - mx_prefix[r - xs];
-    const double yv = static_cast<double>(y.val[p]);
-    double v;
-    if (r < xe && x.idx[r] == row) {
-      v = Both(yv, static_cast<double>(x.val[r]), scale_y, ys_scale, xs_scale, half_sum);
-    } else {
-      v = LeftOnly(yv, scale_y, ys_scale, half_sum);
-    }
+    const T ysc = static_cast<T>(ys_scale);
+    const T xsc = static_cast<T>(xs_scale);
+    const T v = (r < xe && x.idx[r] == row) ? Both(y.val[p], x.val[r], scale_y, ysc, xsc, half_sum)
+                                            : LeftOnly(y.val[p], scale_y, ysc, half_sum);
     emit(rank, row, v);
   }
   for (int64_t q = xs + lane; q < xe; q += kWarp) {
@@ -141,7 +142,7 @@ __device__ void MergeColumn(const CscView<T>& y, const CscView<T>& x, int64_t j,
     if (r < ye && y.idx[r] == row) continue;
     const int64_t qq = q - xs;
     const int64_t rank = qq - mx_prefix[qq] + (r - ys);
-    emit(rank, row, RightOnly(static_cast<double>(x.val[q]), xs_scale, half_sum));
+    emit(rank, row, RightOnly(x.val[q], static_cast<T>(xs_scale), half_sum));
   }
 }
 
@@ -174,11 +175,10 @@ __global__ void UnionWriteWarpKernel(CscView<T> y, CscView<T> x, bool scale_y, d
     if (nx > kUnionWarpCap) continue;
     MatchedPrefix(y, x, j, mx_prefix, lane);
     const int64_t base = out_ptr[j];
-    MergeColumn(y, x, j, scale_y, ys, xs, half_sum, mx_prefix, lane, [&](int64_t rank, int32_t row, double v) {
-      const T stored = static_cast<T>(v);
+    MergeColumn(y, x, j, scale_y, ys, xs, half_sum, mx_prefix, lane, [&](int64_t rank, int32_t row, T stored) {
       out_idx[base + rank] = row;
       out_val[base + rank] = stored;
-      if (prune && fabs(static_cast<double>(stored)) <= 0.0) zero_seen = true;
+      if (prune && stored == T(0)) zero_seen = true;
     });
     __syncwarp();
   }
@@ -266,20 +266,21 @@ __device__ int MergeShared(const CscView<T>& y, const CscView<T>& x, int64_t j, 
   __syncwarp();
   const int merged = ny + nx - running;
   if (merged > cap) return merged;
+  const T ysc = static_cast<T>(ys_scale);
+  const T xsc = static_cast<T>(xs_scale);
   for (int p = lane; p < ny; p += kWarp) {
     const int32_t row = yk[p];
     const int r = LowerBoundShared(xk, nx, row);
-    const double yv = static_cast<double>(y.val[ys + p]);
-    const double v = (r < nx && xk[r] == row)
-                         ? Both(yv, static_cast<double>(x.val[xs + r]), scale_y, ys_scale, xs_scale, half_sum)
-                         : LeftOnly(yv, scale_y, ys_scale, half_sum);
+    const T yv = y.val[ys + p];
+    const T v = (r < nx && xk[r] == row) ? Both(yv, x.val[xs + r], scale_y, ysc, xsc, half_sum)
+                                         : LeftOnly(yv, scale_y, ysc, half_sum);
     emit(p + r - pre[r], row, v);
   }
   for (int q = lane; q < nx; q += kWarp) {
     const int32_t row = xk[q];
     const int r = LowerBoundShared(yk, ny, row);
     if (r < ny && yk[r] == row) continue;
-    emit(q - pre[q] + r, row, RightOnly(static_cast<double>(x.val[xs + q]), xs_scale, half_sum));
+    emit(q - pre[q] + r, row, RightOnly(x.val[xs + q], xsc, half_sum));
   }
   return merged;
 }
@@ -313,11 +314,10 @@ __global__ void UnionPaddedKernel(CscView<T> y, CscView<T> x, bool scale_y, doub
     const int64_t base = y.ptr[j] + x.ptr[j];
     bool zero = false;
     const int merged = MergeShared(y, x, j, yk, xk, pre, scale_y, ys_scale, xs_scale, half_sum, 2 * kUnionPadCap,
-                                   lane, [&](int rank, int32_t row, double v) {
-                                     const T stored = static_cast<T>(v);
+                                   lane, [&](int rank, int32_t row, T stored) {
                                      out_idx[base + rank] = row;
                                      out_val[base + rank] = stored;
-                                     if (prune && fabs(static_cast<double>(stored)) <= 0.0) zero = true;
+                                     if (prune && stored == T(0)) zero = true;
                                    });
     int kept = merged;
     if (__any_sync(0xffffffffu, zero)) {
@@ -332,7 +332,7 @@ __global__ void UnionPaddedKernel(CscView<T> y, CscView<T> x, bool scale_y, doub
           r = out_idx[base + i];
           v = out_val[base + i];
         }
-        const bool keep = i < merged && !(fabs(static_cast<double>(v)) <= 0.0);
+        const bool keep = i < merged && !(v == T(0));
         const unsigned mask = __ballot_sync(0xffffffffu, keep);
         __syncwarp();
         if (keep) {
@@ -521,9 +521,9 @@ __global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric
         continue;
       }
       const int merged = MergeShared(m, mt, j, s.yk, s.xk, s.mx_prefix, false, 1.0, 1.0, true, kDropCap, lane,
-                                     [&](int rank, int32_t row, double v) {
+                                     [&](int rank, int32_t row, T v) {
         s.keys[rank] = row;
-        s.vals[rank] = static_cast<double>(static_cast<T>(v));  // the value M would store
+        s.vals[rank] = static_cast<double>(v);  // the value M would store
       });
       if (merged > kDropCap) {
         if (lane == 0) atomicOr(overflow, 1);
@@ -637,10 +637,11 @@ bool UnionPadded(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const De
                  bool prune, DevCsc<T>& out) {
   const int64_t cols = y.cols;
   const int64_t padded = y.nnz + x.nnz;
-  DevBuf<int32_t> tmp_idx;
-  DevBuf<T> tmp_val;
-  tmp_idx.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
-  tmp_val.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
+  const size_t slots = static_cast<size_t>(padded > 0 ? padded : 1);
+  ctx.pad_idx.Reserve(slots, ctx.stream);
+  ctx.pad_val.Reserve(slots * sizeof(T), ctx.stream);
+  int32_t* tmp_idx = ctx.pad_idx.data();
+  T* tmp_val = reinterpret_cast<T*>(ctx.pad_val.data());
   ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
   int32_t* overflow = ctx.flags.data() + 2;
   SPAI_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int32_t), ctx.stream));
@@ -650,15 +651,14 @@ bool UnionPadded(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const De
                                  static_cast<int>(smem)));
   const int grid = GridFor(cols * kWarp, kWarps * kWarp);
   UnionPaddedKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(y), View(x), scale_y, ys, xs, half_sum, prune,
-                                                                   ctx.counts.data(), tmp_idx.data(), tmp_val.data(),
-                                                                   overflow);
+                                                                   ctx.counts.data(), tmp_idx, tmp_val, overflow);
   SPAI_LAUNCH_CHECK();
   SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 2, overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
   out.Shape(y.rows, cols, ctx.stream);
   const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());  // synchronises: flag is read
   if (ctx.host_flags[2] != 0) return false;
   out.ReserveNnz(nnz, ctx.stream);
-  CompactPadded(ctx, y.ptr.data(), x.ptr.data(), cols, out.ptr.data(), tmp_idx.data(), tmp_val.data(), out.idx.data(),
+  CompactPadded(ctx, y.ptr.data(), x.ptr.data(), cols, out.ptr.data(), tmp_idx, tmp_val, out.idx.data(),
                 out.val.data());
   return true;
 }
@@ -677,16 +677,16 @@ bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk) {
   const int grid = GridFor(cols * kWarp, kWarps * kWarp);
   // survivors land at m.ptr[j] (+ mt.ptr[j]): an upper bound of column j's merged length
   const int64_t padded = m.nnz + (symmetric ? mt.nnz : 0);
-  DevBuf<int32_t> tmp_idx;
-  DevBuf<T> tmp_val;
-  tmp_idx.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
-  tmp_val.Reserve(static_cast<size_t>(padded > 0 ? padded : 1), ctx.stream);
+  const size_t slots = static_cast<size_t>(padded > 0 ? padded : 1);
+  ctx.pad_idx.Reserve(slots, ctx.stream);
+  ctx.pad_val.Reserve(slots * sizeof(T), ctx.stream);
+  int32_t* tmp_idx = ctx.pad_idx.data();
+  T* tmp_val = reinterpret_cast<T*>(ctx.pad_val.data());
   ctx.counts.Reserve(static_cast<size_t>(cols + 1), ctx.stream);
   int32_t* overflow = ctx.flags.data() + 1;
   SPAI_CUDA(cudaMemsetAsync(overflow, 0, sizeof(int32_t), ctx.stream));
   SymmetrizeDropKernel<T><<<grid, kWarps * kWarp, smem, ctx.stream>>>(View(m), mt_view, symmetric, topk,
-                                                                      ctx.counts.data(), tmp_idx.data(),
-                                                                      tmp_val.data(), overflow);
+                                                                      ctx.counts.data(), tmp_idx, tmp_val, overflow);
   SPAI_LAUNCH_CHECK();
   SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 1, overflow, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
   DevCsc<T> out;
@@ -694,8 +694,8 @@ bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk) {
   const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());  // synchronises: flag is read
   if (ctx.host_flags[1] != 0) return false;
   out.ReserveNnz(nnz, ctx.stream);
-  CompactPadded(ctx, m.ptr.data(), symmetric ? mt.ptr.data() : nullptr, cols, out.ptr.data(), tmp_idx.data(),
-                tmp_val.data(), out.idx.data(), out.val.data());
+  CompactPadded(ctx, m.ptr.data(), symmetric ? mt.ptr.data() : nullptr, cols, out.ptr.data(), tmp_idx, tmp_val,
+                out.idx.data(), out.val.data());
   m.Swap(out);
   return true;
 }
