@@ -1029,6 +1029,7 @@ void Ctx::Destroy() {
   sg_fallback.Release();
   sg_maxima.Release();
   sg_ub_ptr.Release();
+  sg_bin_cols.Release();
   sg_pad_idx.Release();
   sg_pad_val.Release();
   sg_pad_z.Release();

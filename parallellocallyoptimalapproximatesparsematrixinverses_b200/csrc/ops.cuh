@@ -40,6 +40,7 @@ struct Ctx {
   DevBuf<unsigned char> sg_fallback;
   DevBuf<unsigned long long> sg_maxima;
   DevBuf<int64_t> sg_ub_ptr;             // padded column offsets (scan of the upper bounds)
+  DevBuf<int32_t> sg_bin_cols;           // column lists of the SpGEMM window bins
   DevBuf<int32_t> sg_pad_idx;            // padded output rows
   DevBuf<unsigned char> sg_pad_val;      // padded output values
   DevBuf<unsigned char> sg_pad_z;        // padded fused Z values

@@ -646,8 +646,9 @@ __device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, int
 
 // kEll: the ELL width of X (compile time, so its loops unroll), 0 without.
 template <class T, int kEll>
-__global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int words_cap, int lo_words, int hi_words,
-                                                           int rows_cap, int hash_slots) {
+__global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, const int32_t* __restrict__ cols_list,
+                                                           int64_t list_len, int words_cap, int rows_cap,
+                                                           int hash_slots) {
   extern __shared__ __align__(16) unsigned char smem[];
   const int lane = threadIdx.x & 31;
   const int summary_cap = SummaryWords(words_cap);
@@ -674,9 +675,9 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
   __syncwarp();
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
-  for (int64_t col = warp; col < a.b.cols; col += warps) {
+  for (int64_t at_list = warp; at_list < list_len; at_list += warps) {
+    const int64_t col = cols_list[at_list];
     const int words = a.win_words[col];
-    if (words <= lo_words || words > hi_words) continue;
     const int32_t lo = a.win_lo[col];
     const int64_t bs = a.b.ptr[col];
     const int64_t be = a.b.ptr[col + 1];
@@ -825,84 +826,88 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, int 
 }
 
 // ---------------------------------------------------------------------------
-// Hash need, window and bin populations of every output column.
-// Thread per output column (every column in flight at once): candidate
-// count, row window and bin; block-level reduction of the maxima, the sum of
-// the upper bounds and the bin populations.
+// Hash need, window and bin of every output column, thread per column (every
+// column in flight at once).  Each column is appended to its bin's list (one
+// atomic per warp and bin; the fill counters are the bin populations the host
+// reads); block-level reduction of the maxima and of the sum of the bounds.
 template <class T>
 __global__ void __launch_bounds__(256) NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ need,
                                                   int64_t* __restrict__ ub, int32_t* __restrict__ win_lo,
-                                                  int32_t* __restrict__ win_words,
+                                                  int32_t* __restrict__ win_words, int32_t* __restrict__ bin_cols,
                                                   unsigned long long* __restrict__ maxima) {
   __shared__ unsigned long long block_max[3];  // max ub, max nnz(B col), sum of ub
-  __shared__ unsigned long long block_pop[kWordBinCount + 1];
   if (threadIdx.x < 3) block_max[threadIdx.x] = 0ull;
-  if (threadIdx.x < kWordBinCount + 1) block_pop[threadIdx.x] = 0ull;
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   unsigned long long local_ub = 0;
   unsigned long long local_nb = 0;
   unsigned long long local_sum = 0;
-  unsigned long long population[kWordBinCount + 1] = {};
-  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < b.cols;
-       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t bs = b.ptr[j];
-    const int64_t be = b.ptr[j + 1];
-    int64_t u = add_diag ? 1 : 0;
-    int32_t lo = add_diag ? static_cast<int32_t>(j) : INT32_MAX;
-    int32_t hi = add_diag ? static_cast<int32_t>(j) : -1;
-    for (int64_t p = bs; p < be; ++p) {
-      const int32_t k = b.idx[p];
-      const int64_t xs = x.ptr[k];
-      const int64_t xe = x.ptr[k + 1];
-      if (xe > xs) {
-        u += xe - xs;
-        lo = min(lo, x.idx[xs]);
-        hi = max(hi, x.idx[xe - 1]);
+  for (int64_t base = static_cast<int64_t>(blockIdx.x) * blockDim.x; base < b.cols;
+       base += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t j = base + threadIdx.x;
+    int bin = -1;  // every lane takes part in the ballots below, columns past the end included
+    if (j < b.cols) {
+      const int64_t bs = b.ptr[j];
+      const int64_t be = b.ptr[j + 1];
+      int64_t u = add_diag ? 1 : 0;
+      int32_t lo = add_diag ? static_cast<int32_t>(j) : INT32_MAX;
+      int32_t hi = add_diag ? static_cast<int32_t>(j) : -1;
+      for (int64_t p = bs; p < be; ++p) {
+        const int32_t k = b.idx[p];
+        const int64_t xs = x.ptr[k];
+        const int64_t xe = x.ptr[k + 1];
+        if (xe > xs) {
+          u += xe - xs;
+          lo = min(lo, x.idx[xs]);
+          hi = max(hi, x.idx[xe - 1]);
+        }
+      }
+      int words = 0;
+      if (hi >= lo) {
+        const int64_t w = (static_cast<int64_t>(hi) - lo) / 32 + 1;
+        words = w > INT32_MAX ? INT32_MAX : static_cast<int>(w);
+      }
+      need[j] = 2 * u;
+      ub[j] = u;
+      win_lo[j] = hi >= lo ? lo : 0;
+      win_words[j] = words;
+      // bins: <= 128, 512, 1040, 2048 words (kWordBins), else the hash path
+      bin = words <= 128 ? 0 : (words <= 512 ? 1 : (words <= 1040 ? 2 : (words <= kBitmapMaxWords ? 3 : 4)));
+      local_sum += static_cast<unsigned long long>(u);
+      local_ub = max(local_ub, static_cast<unsigned long long>(u));
+      local_nb = max(local_nb, static_cast<unsigned long long>(be - bs));
+    }
+#pragma unroll
+    for (int i = 0; i <= kWordBinCount; ++i) {
+      const unsigned mask = __ballot_sync(0xffffffffu, bin == i);
+      if (mask == 0u) continue;
+      const int leader = __ffs(mask) - 1;
+      unsigned long long first = 0ull;
+      unsigned long long* fill = i < kWordBinCount ? &maxima[kPopulation + i] : &maxima[kHashColumns];
+      if (lane == leader) first = atomicAdd(fill, static_cast<unsigned long long>(__popc(mask)));
+      first = __shfl_sync(0xffffffffu, first, leader);
+      if (bin == i) {
+        bin_cols[static_cast<int64_t>(i) * b.cols + static_cast<int64_t>(first) + __popc(mask & LaneMaskBelow())] =
+            static_cast<int32_t>(j);
       }
     }
-    int words = 0;
-    if (hi >= lo) {
-      const int64_t w = (static_cast<int64_t>(hi) - lo) / 32 + 1;
-      words = w > INT32_MAX ? INT32_MAX : static_cast<int>(w);
-    }
-    need[j] = 2 * u;
-    ub[j] = u;
-    win_lo[j] = hi >= lo ? lo : 0;
-    win_words[j] = words;
-    // bins: <= 128, 512, 1040, 2048 words (kWordBins), else the hash path
-    const int bin = words <= 128 ? 0 : (words <= 512 ? 1 : (words <= 1040 ? 2 : (words <= kBitmapMaxWords ? 3 : 4)));
-#pragma unroll
-    for (int i = 0; i <= kWordBinCount; ++i) population[i] += bin == i ? 1ull : 0ull;
-    local_sum += static_cast<unsigned long long>(u);
-    local_ub = max(local_ub, static_cast<unsigned long long>(u));
-    local_nb = max(local_nb, static_cast<unsigned long long>(be - bs));
   }
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     local_ub = max(local_ub, __shfl_xor_sync(0xffffffffu, local_ub, o));
     local_nb = max(local_nb, __shfl_xor_sync(0xffffffffu, local_nb, o));
     local_sum += __shfl_xor_sync(0xffffffffu, local_sum, o);
-#pragma unroll
-    for (int i = 0; i <= kWordBinCount; ++i) population[i] += __shfl_xor_sync(0xffffffffu, population[i], o);
   }
-  if ((threadIdx.x & 31) == 0) {
+  if (lane == 0) {
     atomicMax(&block_max[0], local_ub);
     atomicMax(&block_max[1], local_nb);
     if (local_sum != 0ull) atomicAdd(&block_max[2], local_sum);
-#pragma unroll
-    for (int i = 0; i <= kWordBinCount; ++i) {
-      if (population[i] != 0ull) atomicAdd(&block_pop[i], population[i]);
-    }
   }
   __syncthreads();
   if (threadIdx.x == 0) {
     if (block_max[0] != 0ull) atomicMax(&maxima[kMaxUb], block_max[0]);
     if (block_max[1] != 0ull) atomicMax(&maxima[kMaxNb], block_max[1]);
     if (block_max[2] != 0ull) atomicAdd(&maxima[kSumUb], block_max[2]);
-    for (int i = 0; i < kWordBinCount; ++i) {
-      if (block_pop[i] != 0ull) atomicAdd(&maxima[kPopulation + i], block_pop[i]);
-    }
-    if (block_pop[kWordBinCount] != 0ull) atomicAdd(&maxima[kHashColumns], block_pop[kWordBinCount]);
   }
 }
 
@@ -983,32 +988,33 @@ void LaunchRowSets(Ctx& ctx, RowSetArgs<T> args, const unsigned long long* host_
   }
 }
 
-// The column path over every populated bitmap bin.
+// The column path: one launch per populated bitmap bin, over that bin's
+// column list (written by NeedKernel), with the bin's shared-memory layout.
 template <class T>
 void LaunchColumnProducts(Ctx& ctx, const ColumnArgs<T>& args, const unsigned long long* host_max, int rows_cap,
                           int hash_slots) {
-  int lo_words = -1;
   for (int bin = 0; bin < kWordBinCount; ++bin) {
+    const int64_t population = static_cast<int64_t>(host_max[kPopulation + bin]);
+    if (population == 0) continue;
     const int words_cap = kWordBins[bin];
-    if (host_max[kPopulation + bin] > 0) {
-      const size_t per_warp = ColumnSlabBytes(words_cap, rows_cap, hash_slots, sizeof(T));
-      int warps = static_cast<int>((96 * 1024) / per_warp);
-      warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
-      const size_t smem = per_warp * warps;
-      void (*kernel)(ColumnArgs<T>, int, int, int, int, int) = ColumnProductKernel<T, 0>;
-      switch (args.ell_width) {
-        case 4: kernel = ColumnProductKernel<T, 4>; break;
-        case 8: kernel = ColumnProductKernel<T, 8>; break;
-        case 12: kernel = ColumnProductKernel<T, 12>; break;
-        case 16: kernel = ColumnProductKernel<T, 16>; break;
-        default: break;
-      }
-      SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-      kernel<<<GridFor(args.b.cols * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(
-          args, words_cap, lo_words, words_cap, rows_cap, hash_slots);
-      SPAI_LAUNCH_CHECK();
+    const size_t per_warp = ColumnSlabBytes(words_cap, rows_cap, hash_slots, sizeof(T));
+    int warps = static_cast<int>((96 * 1024) / per_warp);
+    warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
+    const size_t smem = per_warp * warps;
+    void (*kernel)(ColumnArgs<T>, const int32_t*, int64_t, int, int, int) = ColumnProductKernel<T, 0>;
+    switch (args.ell_width) {
+      case 4: kernel = ColumnProductKernel<T, 4>; break;
+      case 8: kernel = ColumnProductKernel<T, 8>; break;
+      case 12: kernel = ColumnProductKernel<T, 12>; break;
+      case 16: kernel = ColumnProductKernel<T, 16>; break;
+      default: break;
     }
-    lo_words = words_cap;
+    SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    const int32_t* list = ctx.sg_bin_cols.data() + static_cast<int64_t>(bin) * args.b.cols;
+    kernel<<<GridFor(population * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(args, list, population,
+                                                                                           words_cap, rows_cap,
+                                                                                           hash_slots);
+    SPAI_LAUNCH_CHECK();
   }
 }
 
@@ -1031,11 +1037,12 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   ctx.sg_win_lo.Reserve(static_cast<size_t>(cols), ctx.stream);
   ctx.sg_win_words.Reserve(static_cast<size_t>(cols), ctx.stream);
   ctx.sg_maxima.Reserve(kMaximaSlots, ctx.stream);
+  ctx.sg_bin_cols.Reserve(static_cast<size_t>(kWordBinCount + 1) * static_cast<size_t>(cols), ctx.stream);
   SPAI_CUDA(cudaMemsetAsync(ctx.sg_maxima.data(), 0, kMaximaSlots * sizeof(unsigned long long), ctx.stream));
   NeedKernel<T><<<GridFor(cols, 256), 256, 0, ctx.stream>>>(View(x_csc), View(b), residual,
                                                                    ctx.sg_need.data(), ctx.sg_counts.data(),
                                                                    ctx.sg_win_lo.data(), ctx.sg_win_words.data(),
-                                                                   ctx.sg_maxima.data());
+                                                                   ctx.sg_bin_cols.data(), ctx.sg_maxima.data());
   SPAI_LAUNCH_CHECK();
   unsigned long long host_max[kMaximaSlots];
   SPAI_CUDA(cudaMemcpyAsync(host_max, ctx.sg_maxima.data(), sizeof(host_max), cudaMemcpyDeviceToHost, ctx.stream));
