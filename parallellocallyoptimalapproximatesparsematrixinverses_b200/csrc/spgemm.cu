@@ -30,6 +30,9 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "device.cuh"
 #include "ops.cuh"
@@ -522,7 +525,7 @@ __host__ __device__ inline int SummaryWords(int words) { return (words + kWarp *
 
 __host__ __device__ inline size_t ColumnSlabBytes(int words, int rows_cap, int hash_slots, size_t value_size) {
   return Round16(static_cast<size_t>(words) * 4) + Round16(static_cast<size_t>(SummaryWords(words)) * 4) +
-         Round16(static_cast<size_t>(rows_cap) * 4) + Round16(static_cast<size_t>(hash_slots) * 4) +
+         Round16(static_cast<size_t>(rows_cap) * 2) + Round16(static_cast<size_t>(hash_slots) * 4) +
          Round16(static_cast<size_t>(hash_slots) * value_size) + 2 * Round16(kWarp * sizeof(double));
 }
 
@@ -613,9 +616,10 @@ __device__ __forceinline__ void MarkRow(uint32_t* bm, uint32_t* summary, int off
   if (old == 0u) atomicOr(&summary[w >> 5], 1u << (w & 31));
 }
 
-// Reads the marked rows back in ascending order (into rows[] unless null),
+// Reads the marked rows back in ascending order, as 16-bit offsets from the
+// window start (a window spans at most 65,536 rows), into rows[] unless null,
 // clearing both levels; returns the warp-uniform count.
-__device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, int32_t lo, int32_t* rows, int lane) {
+__device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, uint16_t* rows, int lane) {
   int total = 0;
   for (int s0 = 0; s0 < summary_words; s0 += kWarp) {
     const int s = s0 + lane;
@@ -634,7 +638,7 @@ __device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, int
       uint32_t bits = bm[w];
       bm[w] = 0u;
       if (rows != nullptr) {
-        for (; bits != 0u; bits &= bits - 1u) rows[at++] = lo + (w << 5) + (__ffs(bits) - 1);
+        for (; bits != 0u; bits &= bits - 1u) rows[at++] = static_cast<uint16_t>((w << 5) + (__ffs(bits) - 1));
       }
     }
     summary[s] = 0u;
@@ -657,8 +661,8 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, cons
   base += Round16(static_cast<size_t>(words_cap) * 4);
   uint32_t* summary = reinterpret_cast<uint32_t*>(base);
   base += Round16(static_cast<size_t>(summary_cap) * 4);
-  int32_t* rows = reinterpret_cast<int32_t*>(base);
-  base += Round16(static_cast<size_t>(rows_cap) * 4);
+  uint16_t* rows = reinterpret_cast<uint16_t*>(base);
+  base += Round16(static_cast<size_t>(rows_cap) * 2);
   int32_t* hkeys = reinterpret_cast<int32_t*>(base);
   base += Round16(static_cast<size_t>(hash_slots) * 4);
   T* hvals = reinterpret_cast<T*>(base);
@@ -716,7 +720,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, cons
       }
     }
     __syncwarp();
-    const int count = DrainRows(bm, summary, SummaryWords(words), lo, rows, lane);
+    const int count = DrainRows(bm, summary, SummaryWords(words), rows, lane);
     const int64_t c0 = projection ? 0 : a.c_ptr[col];
     int kept = 0;
     double sq = 0.0;
@@ -728,7 +732,7 @@ __global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, cons
       int32_t row_out = 0;
       T stored = T(0);
       if (r < count) {
-        const int32_t i = rows[r];
+        const int32_t i = lo + static_cast<int32_t>(rows[r]);
         // the storage type's arithmetic: FP64 for double storage, FP32 multiply and accumulate for float storage
         T acc = T(-0.0);
         if constexpr (kEll > 0) {
@@ -988,6 +992,34 @@ void LaunchRowSets(Ctx& ctx, RowSetArgs<T> args, const unsigned long long* host_
   }
 }
 
+// Warps per block of a warp-per-column kernel with `per_warp` bytes of shared
+// memory per warp: the count that keeps the most warps resident per SM (the
+// slab makes shared memory the usual limit, in steps of a block).  Cached per
+// kernel and slab size.
+int WarpsPerBlock(const void* kernel, size_t per_warp) {
+  static std::mutex mutex;
+  static std::map<std::pair<const void*, size_t>, int> chosen;
+  std::lock_guard<std::mutex> lock(mutex);
+  const auto key = std::make_pair(kernel, per_warp);
+  const auto it = chosen.find(key);
+  if (it != chosen.end()) return it->second;
+  int warps = 1;
+  int best_resident = -1;
+  for (int w = 8; w >= 1; --w) {
+    const size_t bytes = per_warp * static_cast<size_t>(w);
+    if (bytes > static_cast<size_t>(200 * 1024)) continue;
+    SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+    int blocks = 0;
+    SPAI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, w * kWarp, bytes));
+    if (blocks * w > best_resident) {
+      best_resident = blocks * w;
+      warps = w;
+    }
+  }
+  chosen[key] = warps;
+  return warps;
+}
+
 // The column path: one launch per populated bitmap bin, over that bin's
 // column list (written by NeedKernel), with the bin's shared-memory layout.
 template <class T>
@@ -998,9 +1030,6 @@ void LaunchColumnProducts(Ctx& ctx, const ColumnArgs<T>& args, const unsigned lo
     if (population == 0) continue;
     const int words_cap = kWordBins[bin];
     const size_t per_warp = ColumnSlabBytes(words_cap, rows_cap, hash_slots, sizeof(T));
-    int warps = static_cast<int>((96 * 1024) / per_warp);
-    warps = warps < 1 ? 1 : (warps > 8 ? 8 : warps);
-    const size_t smem = per_warp * warps;
     void (*kernel)(ColumnArgs<T>, const int32_t*, int64_t, int, int, int) = ColumnProductKernel<T, 0>;
     switch (args.ell_width) {
       case 4: kernel = ColumnProductKernel<T, 4>; break;
@@ -1009,6 +1038,8 @@ void LaunchColumnProducts(Ctx& ctx, const ColumnArgs<T>& args, const unsigned lo
       case 16: kernel = ColumnProductKernel<T, 16>; break;
       default: break;
     }
+    const int warps = WarpsPerBlock(reinterpret_cast<const void*>(kernel), per_warp);
+    const size_t smem = per_warp * static_cast<size_t>(warps);
     SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     const int32_t* list = ctx.sg_bin_cols.data() + static_cast<int64_t>(bin) * args.b.cols;
     kernel<<<GridFor(population * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(args, list, population,
