@@ -650,7 +650,7 @@ __device__ int DrainRows(uint32_t* bm, uint32_t* summary, int summary_words, uin
 
 // kEll: the ELL width of X (compile time, so its loops unroll), 0 without.
 template <class T, int kEll>
-__global__ void __launch_bounds__(256) ColumnProductKernel(ColumnArgs<T> a, const int32_t* __restrict__ cols_list,
+__global__ void __launch_bounds__(256, 5) ColumnProductKernel(ColumnArgs<T> a, const int32_t* __restrict__ cols_list,
                                                            int64_t list_len, int words_cap, int rows_cap,
                                                            int hash_slots) {
   extern __shared__ __align__(16) unsigned char smem[];

@@ -503,7 +503,7 @@ __device__ void KeepLargest(DropSlab& s, int count, int64_t col, int candidates,
 // mt.ptr[j] when symmetric), their number to counts[j]; `overflow` is set
 // when a column exceeds kDropCap (the caller then discards the pass).
 template <class T>
-__global__ void SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric, int64_t topk,
+__global__ void __launch_bounds__(256, 4) SymmetrizeDropKernel(CscView<T> m, CscView<T> mt, bool symmetric, int64_t topk,
                                      int64_t* __restrict__ counts, int32_t* __restrict__ out_idx,
                                      T* __restrict__ out_val, int32_t* __restrict__ overflow) {
   extern __shared__ __align__(16) unsigned char drop_smem[];
