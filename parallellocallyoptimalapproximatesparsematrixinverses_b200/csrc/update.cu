@@ -285,7 +285,7 @@ __device__ int MergeShared(const CscView<T>& y, const CscView<T>& x, int64_t j, 
   return merged;
 }
 
-constexpr int kUnionPadCap = 512;  // longest input column of the single-pass union
+constexpr int kUnionPadCap = 256;  // longest input column of the single-pass union (keeps 8 blocks resident)
 
 // Single-pass union: column j of the result goes to out at y.ptr[j] +
 // x.ptr[j] (an upper bound of its offset); exact zeros are pruned in place
