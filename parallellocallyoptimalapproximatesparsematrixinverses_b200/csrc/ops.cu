@@ -512,7 +512,8 @@ template <class T>
 __global__ void CompactPaddedKernel(const int64_t* __restrict__ base, const int64_t* __restrict__ base2, int64_t cols,
                                     const int64_t* __restrict__ out_ptr, const int32_t* __restrict__ src_idx,
                                     const T* __restrict__ src_val, int32_t* __restrict__ dst_idx,
-                                    T* __restrict__ dst_val) {
+                                    T* __restrict__ dst_val, const T* __restrict__ src_val2,
+                                    int32_t* __restrict__ dst_idx2, T* __restrict__ dst_val2) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
@@ -521,8 +522,13 @@ __global__ void CompactPaddedKernel(const int64_t* __restrict__ base, const int6
     const int64_t to = out_ptr[j];
     const int64_t n = out_ptr[j + 1] - to;
     for (int64_t i = lane; i < n; i += kWarp) {
-      if (dst_idx != nullptr) dst_idx[to + i] = src_idx[from + i];
+      const int32_t r = src_idx[from + i];
+      if (dst_idx != nullptr) dst_idx[to + i] = r;
       dst_val[to + i] = src_val[from + i];
+      if (dst_val2 != nullptr) {
+        dst_idx2[to + i] = r;
+        dst_val2[to + i] = src_val2[from + i];
+      }
     }
   }
 }
@@ -1205,7 +1211,18 @@ template <class T>
 void CompactPadded(Ctx& ctx, const int64_t* base, const int64_t* base2, int64_t cols, const int64_t* out_ptr,
                    const int32_t* src_idx, const T* src_val, int32_t* dst_idx, T* dst_val) {
   CompactPaddedKernel<T><<<GridFor(cols * kWarp, 256), 256, 0, ctx.stream>>>(base, base2, cols, out_ptr, src_idx,
-                                                                            src_val, dst_idx, dst_val);
+                                                                            src_val, dst_idx, dst_val, nullptr,
+                                                                            nullptr, nullptr);
+  SPAI_LAUNCH_CHECK();
+}
+
+template <class T>
+void CompactPaddedPair(Ctx& ctx, const int64_t* base, int64_t cols, const int64_t* out_ptr, const int32_t* src_idx,
+                       const T* src_val, int32_t* dst_idx, T* dst_val, const T* src_val2, int32_t* dst_idx2,
+                       T* dst_val2) {
+  CompactPaddedKernel<T><<<GridFor(cols * kWarp, 256), 256, 0, ctx.stream>>>(base, nullptr, cols, out_ptr, src_idx,
+                                                                            src_val, dst_idx, dst_val, src_val2,
+                                                                            dst_idx2, dst_val2);
   SPAI_LAUNCH_CHECK();
 }
 
@@ -1360,6 +1377,8 @@ void ConvertValues(Ctx& ctx, const S* src, D* dst, int64_t n) {
   template void ScaleColumns<T>(Ctx&, DevCsc<T>&, const double*);                                             \
   template void DropZeros<T>(Ctx&, DevCsc<T>&);                                                               \
   template void BuildEll<T>(Ctx&, const DevCsc<T>&, int, int32_t*, T*);                                         \
+  template void CompactPaddedPair<T>(Ctx&, const int64_t*, int64_t, const int64_t*, const int32_t*, const T*,         \
+                                     int32_t*, T*, const T*, int32_t*, T*);                                      \
   template void CompactPadded<T>(Ctx&, const int64_t*, const int64_t*, int64_t, const int64_t*, const int32_t*,      \
                                  const T*, int32_t*, T*);                                                        \
   template void PruneColumnRelative<T>(Ctx&, DevCsc<T>&);                                                     \

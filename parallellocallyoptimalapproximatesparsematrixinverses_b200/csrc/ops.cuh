@@ -70,6 +70,12 @@ void ScanCountsAsync(Ctx& ctx, const int64_t* counts, int64_t n, int64_t* out);
 // Moves column j of a padded matrix -- out_ptr[j+1] - out_ptr[j] entries
 // starting at base[j] (+ base2[j] when base2 is given) of src -- to
 // out_ptr[j] of dst.  dst_idx may be null (values only).
+// Two padded matrices of one pattern (rows in src_idx) in one pass: a matrix
+// and a second value array, e.g. R and Z = Pr*R.
+template <class T>
+void CompactPaddedPair(Ctx& ctx, const int64_t* base, int64_t cols, const int64_t* out_ptr, const int32_t* src_idx,
+                       const T* src_val, int32_t* dst_idx, T* dst_val, const T* src_val2, int32_t* dst_idx2,
+                       T* dst_val2);
 template <class T>
 void CompactPadded(Ctx& ctx, const int64_t* base, const int64_t* base2, int64_t cols, const int64_t* out_ptr,
                    const int32_t* src_idx, const T* src_val, int32_t* dst_idx, T* dst_val);

@@ -835,7 +835,8 @@ __global__ void __launch_bounds__(256, 5) ColumnProductKernel(ColumnArgs<T> a, c
 // atomic per warp and bin; the fill counters are the bin populations the host
 // reads); block-level reduction of the maxima and of the sum of the bounds.
 template <class T>
-__global__ void __launch_bounds__(256) NeedKernel(CscView<T> x, CscView<T> b, bool add_diag, int64_t* __restrict__ need,
+__global__ void __launch_bounds__(256) NeedKernel(CscView<T> x, const int32_t* __restrict__ x_cols_ell, int ell_width,
+                                                  CscView<T> b, bool add_diag, int64_t* __restrict__ need,
                                                   int64_t* __restrict__ ub, int32_t* __restrict__ win_lo,
                                                   int32_t* __restrict__ win_words, int32_t* __restrict__ bin_cols,
                                                   unsigned long long* __restrict__ maxima) {
@@ -858,12 +859,29 @@ __global__ void __launch_bounds__(256) NeedKernel(CscView<T> x, CscView<T> b, bo
       int32_t hi = add_diag ? static_cast<int32_t>(j) : -1;
       for (int64_t p = bs; p < be; ++p) {
         const int32_t k = b.idx[p];
-        const int64_t xs = x.ptr[k];
-        const int64_t xe = x.ptr[k + 1];
-        if (xe > xs) {
-          u += xe - xs;
-          lo = min(lo, x.idx[xs]);
-          hi = max(hi, x.idx[xe - 1]);
+        if (ell_width > 0) {
+          // the ELL copy of X(:,k): its rows in ascending order, then -1 padding
+          const int4* e = reinterpret_cast<const int4*>(x_cols_ell + static_cast<int64_t>(k) * ell_width);
+          for (int q = 0; q < ell_width / 4; ++q) {
+            const int4 r4 = e[q];
+            const int32_t r[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+              if (r[t] >= 0) {
+                ++u;
+                lo = min(lo, r[t]);
+                hi = max(hi, r[t]);
+              }
+            }
+          }
+        } else {
+          const int64_t xs = x.ptr[k];
+          const int64_t xe = x.ptr[k + 1];
+          if (xe > xs) {
+            u += xe - xs;
+            lo = min(lo, x.idx[xs]);
+            hi = max(hi, x.idx[xe - 1]);
+          }
         }
       }
       int words = 0;
@@ -1070,7 +1088,8 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
   ctx.sg_maxima.Reserve(kMaximaSlots, ctx.stream);
   ctx.sg_bin_cols.Reserve(static_cast<size_t>(kWordBinCount + 1) * static_cast<size_t>(cols), ctx.stream);
   SPAI_CUDA(cudaMemsetAsync(ctx.sg_maxima.data(), 0, kMaximaSlots * sizeof(unsigned long long), ctx.stream));
-  NeedKernel<T><<<GridFor(cols, 256), 256, 0, ctx.stream>>>(View(x_csc), View(b), residual,
+  NeedKernel<T><<<GridFor(cols, 256), 256, 0, ctx.stream>>>(View(x_csc), extras.x_cols_ell, extras.ell_width, View(b),
+                                                            residual,
                                                                    ctx.sg_need.data(), ctx.sg_counts.data(),
                                                                    ctx.sg_win_lo.data(), ctx.sg_win_words.data(),
                                                                    ctx.sg_bin_cols.data(), ctx.sg_maxima.data());
@@ -1155,17 +1174,19 @@ bool Spgemm(Ctx& ctx, const DevCsc<T>& x_csc, const DevCsc<T>& x_csr, const DevC
       double bytes = 2.0 * MatrixBytes<T>(nnz, cols);
       if (want_z) bytes += 2.0 * static_cast<double>(nnz) * (sizeof(T) + sizeof(int32_t));
       prof::Scope scope(ctx.stream, "spgemm_compact", bytes);
-      CompactPadded(ctx, ctx.sg_ub_ptr.data(), static_cast<const int64_t*>(nullptr), cols, result.ptr.data(),
-                    ctx.sg_pad_idx.data(), pad_val, result.idx.data(), result.val.data());
       if (want_z) {
         DevCsc<T> z;
         z.Shape(result.rows, cols, ctx.stream);
         z.ReserveNnz(nnz, ctx.stream);
         SPAI_CUDA(cudaMemcpyAsync(z.ptr.data(), result.ptr.data(), sizeof(int64_t) * (cols + 1),
                                   cudaMemcpyDeviceToDevice, ctx.stream));
-        CompactPadded(ctx, ctx.sg_ub_ptr.data(), static_cast<const int64_t*>(nullptr), cols, z.ptr.data(),
-                      ctx.sg_pad_idx.data(), pad_z, z.idx.data(), z.val.data());
+        CompactPaddedPair(ctx, ctx.sg_ub_ptr.data(), cols, result.ptr.data(), ctx.sg_pad_idx.data(), pad_val,
+                          result.idx.data(), result.val.data(), static_cast<const T*>(pad_z), z.idx.data(),
+                          z.val.data());
         c_z->Swap(z);
+      } else {
+        CompactPadded(ctx, ctx.sg_ub_ptr.data(), static_cast<const int64_t*>(nullptr), cols, result.ptr.data(),
+                      ctx.sg_pad_idx.data(), pad_val, result.idx.data(), result.val.data());
       }
     }
     c.Swap(result);
