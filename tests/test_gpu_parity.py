@@ -146,3 +146,22 @@ def test_fp64_reference_cpu_configuration(require_gpu, topk):
     want_hist, want_status = pyoracle.pcg(a, msym, b, 2000, 1e-8, order=pyoracle.ORDER_DEVICE)
     assert status == want_status == 1
     assert np.array_equal(hist.view(np.int64), want_hist.view(np.int64))
+
+
+@pytest.mark.parametrize("family,name", [("global_spai", "mr"), ("inner_outer", "lomr")])
+def test_fp64_dense_column_global_hash_fallback(require_gpu, family, name):
+    """A column with far more candidate rows than the shared-memory hash bins
+    hold (about 630,000) over a window of 70,000 rows: the generic SpGEMM's
+    hash in global memory, the two-pass union and no dropping (so the dense
+    column survives every step)."""
+    from scipy import sparse
+    n = 70_000
+    A = problems.random_banded_spd(n, half_width=2, extra=2, seed=6)
+    dense = np.random.default_rng(12).uniform(-1.0, 1.0, n) * 1e-4
+    M0 = sparse.lil_matrix(problems.diagonal_inverse(A))
+    M0[:, 0] = dense[:, None]
+    M0 = sparse.csc_matrix(M0)
+    M0.sort_indices()
+    got, want = _run_both(family, name, A, M0, None, max_iterations=2, tolerance=1e-12, max_density=1.0,
+                          enable_dropping=False)
+    assert_same_result(got, want, f"{family}.{name} dense column")
