@@ -129,6 +129,36 @@ int64_t spai_pcg_device_noalloc(int64_t n, int64_t a_nnz, const double* a_values
                                 int64_t max_iterations, double tolerance, int64_t refresh_period, void* stream,
                                 double* history, int64_t* status, char* error, int64_t error_capacity);
 
+/* ---- Adjoints (reverse mode).  No counterpart in the reference; they
+ * differentiate what the reference computes. ---- */
+
+/* f(A, M) = ||I - A M||_F^2 -- the square of the residual norm the reference
+ * records (methods_common.cpp:112-122) -- and its gradient with respect to the
+ * stored values of M and of A.  A and M: n x n CSC in the reference's
+ * MatrixData, canonical (offsets from 0 to nnz, rows strictly increasing in
+ * every column).  On return *loss = f and, unless NULL,
+ *   grad_m[p] = -2 (A^T R)(i, j)  for M's stored entry p = (i, j)  (nnz(M) doubles),
+ *   grad_a[q] = -2 (R M^T)(i, k)  for A's stored entry q = (i, k)  (nnz(A) doubles),
+ * with R = I - A M; every product in FP64, its terms summed in ascending k.
+ * device: CUDA ordinal, -1 for the current device.  Returns 0, or -1 with `error`. */
+int64_t spai_residual_adjoint(struct MatrixData A, struct MatrixData M, int64_t device, double* loss,
+                              double* grad_m, double* grad_a, char* error, int64_t error_capacity);
+
+/* Reverse mode of spai_pcg (x = A^-1 b for symmetric positive definite CSR A):
+ * given x (the forward solution, n doubles) and grad_x = dL/dx, solves
+ * A lambda = grad_x with the forward's preconditioner and settings (the same
+ * arithmetic as spai_pcg with b = grad_x) and writes, unless NULL,
+ *   grad_b[i] = lambda_i                                   (n doubles),
+ *   grad_a[q] = -(lambda_i * x_j) for A's CSR entry q = (i, j)  (nnz(A) doubles).
+ * This is the implicit-function adjoint: the gradient of the exact solution
+ * map, which the computed x approximates to the solve's tolerance.  history
+ * (params.max_iterations doubles) may be NULL; returns the adjoint solve's
+ * history length and sets *status as spai_pcg does, or -1 with `error`. */
+int64_t spai_pcg_adjoint(int64_t n, const double* a_values, const int64_t* a_indices, const int64_t* a_offsets,
+                         const double* m_values, const int64_t* m_indices, const int64_t* m_offsets, const double* x,
+                         const double* grad_x, PcgParams params, double* grad_b, double* grad_a, double* history,
+                         int64_t* status, char* error, int64_t error_capacity);
+
 /* y = A x for CSR A (backward_error.pyx:56-66 `matvec`); returns 0, or -1 with `error`. */
 int64_t spai_matvec(int64_t n, const double* values, const int64_t* indices, const int64_t* offsets,
                     const double* x, double* y, int64_t device, char* error, int64_t error_capacity);

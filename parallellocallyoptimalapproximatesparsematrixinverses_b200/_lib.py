@@ -81,7 +81,7 @@ EXPORTED_SYMBOLS = (
     "spai_run_ex", "spai_pcg", "spai_matvec", "spai_session_create", "spai_session_run", "spai_session_history",
     "spai_session_result", "spai_session_set_rhs", "spai_session_pcg", "spai_session_destroy",
     "spai_kernel_launches", "spai_session_stream", "spai_profile_enable", "spai_profile_reset",
-    "spai_profile_read", "spai_pcg_device_noalloc",
+    "spai_profile_read", "spai_pcg_device_noalloc", "spai_residual_adjoint", "spai_pcg_adjoint",
 )
 
 _lib = None
@@ -134,6 +134,11 @@ def _declare(lib) -> None:
                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_void_p, _i64, _f64, _i64, ctypes.c_void_p, _pf64, _pi64,
                                             ctypes.c_char_p, _i64]
+    lib.spai_residual_adjoint.restype = _i64
+    lib.spai_residual_adjoint.argtypes = [MatrixData, MatrixData, _i64, _pf64, _pf64, _pf64, ctypes.c_char_p, _i64]
+    lib.spai_pcg_adjoint.restype = _i64
+    lib.spai_pcg_adjoint.argtypes = [_i64, _pf64, _pi64, _pi64, _pf64, _pi64, _pi64, _pf64, _pf64, PcgParams, _pf64,
+                                     _pf64, _pf64, _pi64, ctypes.c_char_p, _i64]
 
 
 def load():

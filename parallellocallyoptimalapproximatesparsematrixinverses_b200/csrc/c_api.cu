@@ -15,6 +15,7 @@
 
 #include "../../include/methods_c_api.h"
 #include "../../include/spai_b200.h"
+#include "adjoint.cuh"
 #include "device.cuh"
 #include "ops.cuh"
 #include "pcg.cuh"
@@ -204,9 +205,49 @@ void CheckPcgParams(int64_t n, const PcgParams& p) {
 
 int64_t FinishPcg(const PcgResult& r, int64_t capacity, double* history, int64_t* status) {
   const int64_t count = static_cast<int64_t>(r.history.size());
-  for (int64_t i = 0; i < count && i < capacity; ++i) history[i] = r.history[i];
+  if (history != nullptr) {
+    for (int64_t i = 0; i < count && i < capacity; ++i) history[i] = r.history[i];
+  }
   if (status != nullptr) *status = r.status;
   return count;
+}
+
+// Uploads CSR M as params ask (FP64 or FP32, optionally its symmetric part)
+// and runs PCG from x = 0 on the device vectors rhs -> x.
+void PcgOnDevice(Ctx& ctx, int64_t n, const DevCsc<double>& a, const double* m_values, const int64_t* m_indices,
+                 const int64_t* m_offsets, const PcgParams& params, const double* rhs, double* x,
+                 PcgResult& result) {
+  PcgOptions opt;
+  opt.max_iterations = params.max_iterations;
+  opt.tolerance = params.tolerance;
+  opt.refresh_period = params.refresh_period;
+  if (params.m_precision == 1) {
+    DevCsc<float> m;
+    UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
+    if (params.symmetric_part) SymmetricPart(ctx, m);
+    RunPcg(ctx, a, m, rhs, x, opt, result);
+  } else {
+    DevCsc<double> m;
+    UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
+    if (params.symmetric_part) SymmetricPart(ctx, m);
+    RunPcg(ctx, a, m, rhs, x, opt, result);
+  }
+}
+
+// The adjoint entry points index their gradients by stored entry, so they
+// take canonical CSC only: offsets from 0 to nnz, rows strictly increasing
+// inside every column (what methods.pyx:82-86 hands the reference).
+void CheckCanonicalCsc(const HostCsc& h, const char* name) {
+  if (h.ptr[0] != 0 || h.ptr[h.cols] != h.nnz) {
+    throw std::invalid_argument(std::string(name) + ": column offsets must run from 0 to nnz");
+  }
+  for (int64_t j = 0; j < h.cols; ++j) {
+    for (int64_t p = h.ptr[j] + 1; p < h.ptr[j + 1]; ++p) {
+      if (h.idx[p] <= h.idx[p - 1]) {
+        throw std::invalid_argument(std::string(name) + ": row indices must be strictly increasing in every column");
+      }
+    }
+  }
 }
 
 }  // namespace
@@ -292,27 +333,92 @@ int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, co
     bd.Reserve(static_cast<size_t>(n), ctx.stream);
     xd.Reserve(static_cast<size_t>(n), ctx.stream);
     SPAI_CUDA(cudaMemcpyAsync(bd.data(), b, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.stream));
-    spai::PcgOptions opt;
-    opt.max_iterations = params.max_iterations;
-    opt.tolerance = params.tolerance;
-    opt.refresh_period = params.refresh_period;
     spai::PcgResult result;
-    if (params.m_precision == 1) {
-      spai::DevCsc<float> m;
-      spai::UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
-      if (params.symmetric_part) spai::SymmetricPart(ctx, m);
-      spai::RunPcg(ctx, a, m, bd.data(), xd.data(), opt, result);
-    } else {
-      spai::DevCsc<double> m;
-      spai::UploadCsr(ctx, n, m_values, m_indices, m_offsets, m);
-      if (params.symmetric_part) spai::SymmetricPart(ctx, m);
-      spai::RunPcg(ctx, a, m, bd.data(), xd.data(), opt, result);
-    }
+    spai::PcgOnDevice(ctx, n, a, m_values, m_indices, m_offsets, params, bd.data(), xd.data(), result);
     if (x_out != nullptr) {
       SPAI_CUDA(cudaMemcpyAsync(x_out, xd.data(), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx.stream));
     }
     ctx.Sync();
     return spai::FinishPcg(result, params.max_iterations, history, status);
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_pcg_adjoint(int64_t n, const double* a_values, const int64_t* a_indices, const int64_t* a_offsets,
+                         const double* m_values, const int64_t* m_indices, const int64_t* m_offsets, const double* x,
+                         const double* grad_x, PcgParams params, double* grad_b, double* grad_a, double* history,
+                         int64_t* status, char* error, int64_t error_capacity) {
+  try {
+    spai::CheckPcgParams(n, params);
+    if (grad_x == nullptr) throw std::invalid_argument("grad_x must not be null");
+    if (grad_a != nullptr && x == nullptr) throw std::invalid_argument("x must not be null when grad_a is requested");
+    spai::CtxGuard guard(spai::ResolveDevice(params.device));
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevCsc<double> a;
+    spai::UploadCsr(ctx, n, a_values, a_indices, a_offsets, a);
+    spai::DevBuf<double> gd;
+    spai::DevBuf<double> lambda;
+    gd.Reserve(static_cast<size_t>(n), ctx.stream);
+    lambda.Reserve(static_cast<size_t>(n), ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(gd.data(), grad_x, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.stream));
+    // A symmetric: A^T lambda = grad_x is the forward's own solve
+    spai::PcgResult result;
+    spai::PcgOnDevice(ctx, n, a, m_values, m_indices, m_offsets, params, gd.data(), lambda.data(), result);
+    if (grad_b != nullptr) {
+      SPAI_CUDA(cudaMemcpyAsync(grad_b, lambda.data(), sizeof(double) * n, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    spai::DevBuf<double> xd;
+    spai::DevBuf<double> ga;
+    if (grad_a != nullptr && a.nnz > 0) {
+      xd.Reserve(static_cast<size_t>(n), ctx.stream);
+      ga.Reserve(static_cast<size_t>(a.nnz), ctx.stream);
+      SPAI_CUDA(cudaMemcpyAsync(xd.data(), x, sizeof(double) * n, cudaMemcpyHostToDevice, ctx.stream));
+      spai::NegativeOuterOnRows(ctx, a, lambda.data(), xd.data(), ga.data());
+      SPAI_CUDA(cudaMemcpyAsync(grad_a, ga.data(), sizeof(double) * a.nnz, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    ctx.Sync();
+    return spai::FinishPcg(result, params.max_iterations, history, status);
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_residual_adjoint(MatrixData A, MatrixData M, int64_t device, double* loss, double* grad_m,
+                              double* grad_a, char* error, int64_t error_capacity) {
+  try {
+    const spai::HostCsc a = spai::CheckedMatrix(A);
+    const spai::HostCsc m = spai::CheckedMatrix(M);
+    if (a.rows != a.cols || m.rows != a.rows || m.cols != a.cols) {
+      throw std::invalid_argument("A and M must be square and of the same size");
+    }
+    spai::CheckCanonicalCsc(a, "A");
+    spai::CheckCanonicalCsc(m, "M");
+    if (loss == nullptr) throw std::invalid_argument("loss must not be null");
+    spai::CtxGuard guard(spai::ResolveDevice(device));
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevBuf<int64_t> stage_idx;
+    spai::DevBuf<double> stage_val;
+    spai::DevCsc<double> ad;
+    spai::DevCsc<double> md;
+    spai::UploadCsc(ctx, a, ad, stage_idx, stage_val);
+    spai::UploadCsc(ctx, m, md, stage_idx, stage_val);
+    spai::DevBuf<double> gm;
+    spai::DevBuf<double> ga;
+    if (grad_m != nullptr) gm.Reserve(static_cast<size_t>(m.nnz), ctx.stream);
+    if (grad_a != nullptr) ga.Reserve(static_cast<size_t>(a.nnz), ctx.stream);
+    spai::ResidualAdjoint(ctx, ad, md, loss, grad_m != nullptr ? gm.data() : nullptr,
+                          grad_a != nullptr ? ga.data() : nullptr);
+    if (grad_m != nullptr) {
+      SPAI_CUDA(cudaMemcpyAsync(grad_m, gm.data(), sizeof(double) * m.nnz, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    if (grad_a != nullptr) {
+      SPAI_CUDA(cudaMemcpyAsync(grad_a, ga.data(), sizeof(double) * a.nnz, cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    ctx.Sync();
+    return 0;
   } catch (const std::exception& ex) {
     spai::CopyError(ex.what(), error, error_capacity);
     return -1;

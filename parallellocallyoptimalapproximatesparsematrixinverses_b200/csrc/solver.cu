@@ -99,7 +99,8 @@ __global__ void WidenIndexKernel(const int32_t* __restrict__ src, int64_t* __res
   }
 }
 
-// Uploads a host CSC (int64 indices, f64 values) as DevCsc<T>.
+}  // namespace
+
 template <class T>
 void UploadCsc(Ctx& ctx, const HostCsc& h, DevCsc<T>& d, DevBuf<int64_t>& stage_idx, DevBuf<double>& stage_val) {
   d.Shape(h.rows, h.cols, ctx.stream);
@@ -130,6 +131,11 @@ void UploadCsc(Ctx& ctx, const HostCsc& h, DevCsc<T>& d, DevBuf<int64_t>& stage_
   // the pageable host arrays must stay valid until the copies finish
   ctx.Sync();
 }
+
+template void UploadCsc<double>(Ctx&, const HostCsc&, DevCsc<double>&, DevBuf<int64_t>&, DevBuf<double>&);
+template void UploadCsc<float>(Ctx&, const HostCsc&, DevCsc<float>&, DevBuf<int64_t>&, DevBuf<double>&);
+
+namespace {
 
 template <class T>
 class Solver final : public SolverBase {

@@ -86,6 +86,11 @@ class SolverBase {
 
 std::unique_ptr<SolverBase> MakeSolver(Ctx& ctx, const SolveOptions& options);
 
+// Uploads a host CSC (int64 indices, f64 values, offsets rebased to start at
+// 0) as DevCsc<T> (T = double or float); stage_* are scratch.  Synchronises.
+template <class T>
+void UploadCsc(Ctx& ctx, const HostCsc& h, DevCsc<T>& d, DevBuf<int64_t>& stage_idx, DevBuf<double>& stage_val);
+
 // Validation shared by the C entry points (reference methods_c_api.cpp:16-40,
 // methods_common.cpp:12-48); throws std::invalid_argument with the reference's messages.
 HostCsc CheckedMatrix(const MatrixData& data);

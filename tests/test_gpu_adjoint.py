@@ -1,0 +1,130 @@
+"""Device adjoints through the C ABI: bit for bit against the adjoint oracle
+(FP64, same summation orders), and the torch autograd wrappers against
+central finite differences of the device forward."""
+import numpy as np
+import pytest
+from scipy import sparse
+
+from oracle import adjoint_oracle
+from parallellocallyoptimalapproximatesparsematrixinverses_b200 import adjoint, backward_error, global_spai, problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _m_from_mr(A, topk):
+    r = global_spai.mr(A, M0=problems.diagonal_inverse(A), max_iterations=4, tolerance=1e-14,
+                       max_density=topk / A.shape[0], topk_per_column=topk)
+    return adjoint_oracle.canonical_csc(r.M)
+
+
+CASES = {
+    # a built SPAI M: non-symmetric pattern, top-5 per column
+    "laplacian_16_mr": lambda: (problems.laplacian_2d(16), 5),
+    # variable coefficients
+    "diffusion_20_mr": lambda: (problems.diffusion_2d(20, 1.0, 4), 7),
+    # long-range couplings: windows wider than the bitmap kernels take
+    "banded_wide": lambda: (problems.random_banded_spd(20_000, half_width=2, extra=2, seed=9), 0),
+}
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_residual_adjoint_bit_exact(require_gpu, case):
+    A, topk = CASES[case]()
+    A = adjoint_oracle.canonical_csc(A)
+    M = _m_from_mr(A, topk) if topk else adjoint_oracle.canonical_csc(problems.diagonal_inverse(A))
+    loss, grad_m, grad_a = adjoint.residual_adjoint(A, M)
+    want_loss, want_m, want_a = adjoint_oracle.residual_adjoint(A, M)
+    assert loss == want_loss
+    assert np.array_equal(grad_m.indices, M.indices) and np.array_equal(grad_a.indices, A.indices)
+    assert np.array_equal(grad_m.data, want_m)
+    assert np.array_equal(grad_a.data, want_a)
+    assert np.abs(grad_m.data).max() > 0
+
+
+def test_pcg_adjoint_bit_exact(require_gpu):
+    A = sparse.csr_matrix(problems.diffusion_2d(24, 1.0, 5))
+    A.sort_indices()
+    M = sparse.csr_matrix(problems.diagonal_inverse(A))
+    rng = np.random.default_rng(2)
+    x_t = rng.standard_normal(A.shape[0])
+    b = A @ x_t
+    _, status, x = backward_error.pcg(A.data, A.indices, A.indptr, M.data, M.indices, M.indptr, b, 3000, 1, 1e-10,
+                                      return_x=True)
+    assert status == 1
+    g = 2.0 * (x - x_t)
+    grad_b, grad_a, history, status = adjoint.pcg_adjoint(A.data, A.indices, A.indptr, M.data, M.indices,
+                                                          M.indptr, x, g, 3000, 1e-10)
+    want_b, want_a, want_history, want_status = adjoint_oracle.pcg_adjoint(A, M, x, g, 3000, 1e-10)
+    assert status == want_status == 1
+    assert np.array_equal(history.view(np.int64), want_history.view(np.int64))
+    assert np.array_equal(grad_b, want_b)
+    assert np.array_equal(grad_a, want_a)
+    # the adjoint solve is the forward's own arithmetic with b = grad_x
+    _, _, lam = backward_error.pcg(A.data, A.indices, A.indptr, M.data, M.indices, M.indptr, g, 3000, 1, 1e-10,
+                                   return_x=True)
+    assert np.array_equal(grad_b, lam)
+
+
+def _symmetric_direction(A_csr, rng):
+    upper = sparse.triu(A_csr, format="csr")
+    upper.data = rng.standard_normal(upper.nnz)
+    d = sparse.csr_matrix(upper + sparse.triu(upper, k=1).T)
+    d.sort_indices()
+    assert np.array_equal(d.indices, A_csr.indices) and np.array_equal(d.indptr, A_csr.indptr)
+    return d.data
+
+
+def test_pcg_autograd_matches_finite_differences(require_gpu):
+    # variable-coefficient 5-point operator; x_t ~ N(0, 1), b = A x_t + 0.01 N(0, 1); L = ||x - x_t||^2
+    import torch
+    A = sparse.csr_matrix(problems.diffusion_2d(64, 1.0, 11))
+    A.sort_indices()
+    M = sparse.csr_matrix(problems.diagonal_inverse(A))
+    rng = np.random.default_rng(12)
+    x_t = torch.from_numpy(rng.standard_normal(A.shape[0]))
+    b0 = A @ x_t.numpy() + 0.01 * rng.standard_normal(A.shape[0])
+    solve = dict(a_indices=A.indices, a_offsets=A.indptr, m_values=M.data, m_indices=M.indices,
+                 m_offsets=M.indptr, max_iterations=20_000, tolerance=1e-13)
+
+    def loss(a_values, b):
+        x = adjoint.pcg_solve(a_values, b, **solve)
+        return torch.sum((x - x_t) ** 2)
+
+    a = torch.from_numpy(A.data.copy()).requires_grad_(True)
+    b = torch.from_numpy(b0.copy()).requires_grad_(True)
+    loss(a, b).backward()
+    scale = np.abs(A.data).max()
+    for _ in range(16):
+        da = torch.from_numpy(_symmetric_direction(A, rng))
+        db = torch.from_numpy(rng.standard_normal(A.shape[0]))
+        # the step where truncation (h^2) and solve error balance, found with the
+        # oracle PCG (the device's arithmetic): worst relative gap 5e-8 over these 16
+        h = 1e-8 * scale
+        with torch.no_grad():
+            fd = (loss(a + h * da, b + h * db) - loss(a - h * da, b - h * db)).item() / (2 * h)
+        got = (a.grad @ da + b.grad @ db).item()
+        assert got == pytest.approx(fd, rel=1e-6)
+
+
+def test_residual_objective_autograd(require_gpu):
+    import torch
+    A = adjoint_oracle.canonical_csc(problems.diffusion_2d(12, 1.0, 3))
+    M = _m_from_mr(A, 6)
+    a = torch.from_numpy(A.data.copy()).requires_grad_(True)
+    m = torch.from_numpy(M.data.copy()).requires_grad_(True)
+    a_pattern, m_pattern = (A.indptr, A.indices), (M.indptr, M.indices)
+    f = adjoint.residual_objective(a, m, a_pattern, m_pattern)
+    (3.0 * f).backward()
+    _, want_m, want_a = adjoint_oracle.residual_adjoint(A, M)
+    assert np.array_equal(m.grad.numpy(), 3.0 * want_m)
+    assert np.array_equal(a.grad.numpy(), 3.0 * want_a)
+    rng = np.random.default_rng(5)
+    for _ in range(4):
+        da = torch.from_numpy(rng.standard_normal(A.nnz))
+        dm = torch.from_numpy(rng.standard_normal(M.nnz))
+        h = 1e-6
+        with torch.no_grad():
+            fp = adjoint.residual_objective(a + h * da, m + h * dm, a_pattern, m_pattern).item()
+            fm = adjoint.residual_objective(a - h * da, m - h * dm, a_pattern, m_pattern).item()
+        got = ((a.grad @ da + m.grad @ dm) / 3.0).item()
+        assert got == pytest.approx((fp - fm) / (2 * h), rel=1e-6)
