@@ -84,6 +84,19 @@ enum {
 struct Result spai_run_ex(int64_t method, struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
                           struct MethodParams params, const SpaiExtParams* ext);
 
+/* Global MR on `count` independent systems in one batch: A[b] (and M0[b]
+ * when params.use_initial_m) are the reference's MatrixData, each square.  On
+ * the device the systems form one block-diagonal problem, so every kernel
+ * launch covers the whole batch, while step lengths, norms, stop rules and
+ * histories stay per system: results[b] is what spai_global_mr would return
+ * for system b alone (same bits in FP64).  Pr is diag(A[b])^-1
+ * (params.use_preconditioner must be 0) and dropping, when enabled, must be
+ * per column (ext->topk_per_column > 0).  Returns 0 with `count` Results to
+ * release with free_mem each, or -1 with `error` and every results[b] empty. */
+int64_t spai_mr_batched(int64_t count, const struct MatrixData* A, const struct MatrixData* M0,
+                        struct MethodParams params, const SpaiExtParams* ext, struct Result* results, char* error,
+                        int64_t error_capacity);
+
 typedef struct PcgParams {
   int64_t max_iterations; /* length limit of the history, initial entry included (backward_error.pyx:69-72) */
   double tolerance;       /* relative residual ||r|| / ||b|| */

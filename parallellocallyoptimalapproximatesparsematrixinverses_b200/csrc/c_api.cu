@@ -346,6 +346,94 @@ int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, co
   }
 }
 
+int64_t spai_mr_batched(int64_t count, const MatrixData* A, const MatrixData* M0, MethodParams params,
+                        const SpaiExtParams* ext, Result* results, char* error, int64_t error_capacity) {
+  try {
+    if (count <= 0 || A == nullptr || results == nullptr) {
+      throw std::invalid_argument("count must be positive and A, results non-null");
+    }
+    for (int64_t b = 0; b < count; ++b) results[b] = Result{};
+    if (params.use_initial_m != 0 && M0 == nullptr) throw std::invalid_argument("use_initial_m is set but M0 is null");
+    if (params.use_preconditioner != 0) {
+      throw std::invalid_argument("batched runs use Pr = diag(A)^-1: use_preconditioner must be 0");
+    }
+    const int64_t topk = ext != nullptr ? ext->topk_per_column : 0;
+    if (params.enable_dropping != 0 && topk <= 0) {
+      throw std::invalid_argument(
+          "batched runs drop per column only: set topk_per_column > 0 or enable_dropping = 0");
+    }
+    // validation per system, with the reference's messages (methods_c_api.cpp:16-40, methods_common.cpp:12-48)
+    std::vector<spai::HostCsc> as(static_cast<size_t>(count));
+    std::vector<spai::HostCsc> ms(static_cast<size_t>(count));
+    std::vector<int64_t> offsets(static_cast<size_t>(count + 1), 0);
+    int64_t nnz_a = 0;
+    int64_t nnz_m = 0;
+    for (int64_t b = 0; b < count; ++b) {
+      as[b] = spai::CheckedMatrix(A[b]);
+      if (params.use_initial_m != 0) ms[b] = spai::CheckedMatrix(M0[b]);
+      spai::ValidateProblem(as[b], params.use_initial_m != 0 ? &ms[b] : nullptr, nullptr, params);
+      offsets[b + 1] = offsets[b] + as[b].cols;
+      nnz_a += as[b].ptr[as[b].cols] - as[b].ptr[0];
+      if (params.use_initial_m != 0) nnz_m += ms[b].ptr[ms[b].cols] - ms[b].ptr[0];
+    }
+    const int64_t n = offsets[count];
+    if (n > static_cast<int64_t>(INT32_MAX)) throw std::invalid_argument("the batch exceeds 2^31 - 1 rows in total");
+    // the block-diagonal matrices, assembled once on the host
+    auto assemble = [&](const std::vector<spai::HostCsc>& parts, int64_t nnz, std::vector<int64_t>& ptr,
+                        std::vector<int64_t>& idx, std::vector<double>& val) {
+      ptr.assign(static_cast<size_t>(n + 1), 0);
+      idx.resize(static_cast<size_t>(nnz));
+      val.resize(static_cast<size_t>(nnz));
+      int64_t at = 0;
+      for (int64_t b = 0; b < count; ++b) {
+        const spai::HostCsc& h = parts[b];
+        for (int64_t j = 0; j < h.cols; ++j) {
+          for (int64_t p = h.ptr[j]; p < h.ptr[j + 1]; ++p) {
+            idx[at] = h.idx[p] + offsets[b];
+            val[at] = h.val[p];
+            ++at;
+          }
+          ptr[offsets[b] + j + 1] = at;
+        }
+      }
+    };
+    std::vector<int64_t> a_ptr, a_idx, m_ptr, m_idx;
+    std::vector<double> a_val, m_val;
+    assemble(as, nnz_a, a_ptr, a_idx, a_val);
+    spai::HostCsc big_a{n, n, nnz_a, a_ptr.data(), a_idx.data(), a_val.data()};
+    spai::HostCsc big_m;
+    if (params.use_initial_m != 0) {
+      assemble(ms, nnz_m, m_ptr, m_idx, m_val);
+      big_m = spai::HostCsc{n, n, nnz_m, m_ptr.data(), m_idx.data(), m_val.data()};
+    }
+    spai::SolveOptions opt;
+    opt.method = spai::Method::kGlobalMr;
+    opt.max_iterations = params.max_iterations;
+    opt.tolerance = params.tolerance;
+    opt.max_density = params.max_density;
+    opt.dropping = params.enable_dropping != 0;
+    if (ext != nullptr) {
+      if (ext->precision != 0 && ext->precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
+      if (ext->reserved != 0) throw std::invalid_argument("SpaiExtParams.reserved must be 0");
+      opt.precision = static_cast<int>(ext->precision);
+      opt.topk = topk;
+    }
+    spai::CtxGuard guard(spai::ResolveDevice(ext != nullptr ? ext->device : -1));
+    auto solver = spai::MakeSolver(guard.ctx, opt);
+    solver->Upload(big_a, params.use_initial_m != 0 ? &big_m : nullptr, nullptr);
+    std::vector<spai::SolveOutput> outputs;
+    solver->RunMrBatched(offsets, outputs);
+    for (int64_t b = 0; b < count; ++b) results[b] = spai::SuccessResult(outputs[b]);
+    return 0;
+  } catch (const std::exception& ex) {
+    if (results != nullptr) {
+      for (int64_t b = 0; b < count; ++b) free_mem(&results[b]);
+    }
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
 int64_t spai_pcg_adjoint(int64_t n, const double* a_values, const int64_t* a_indices, const int64_t* a_offsets,
                          const double* m_values, const int64_t* m_indices, const int64_t* m_offsets, const double* x,
                          const double* grad_x, PcgParams params, double* grad_b, double* grad_a, double* history,

@@ -5,11 +5,13 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <stdexcept>
 #include <limits>
 
 #include "device.cuh"
@@ -106,6 +108,27 @@ struct TreeArgs {
   const double* src2[8];  // when set, level-one terms are src[i] * src2[i]
 };
 
+// The lanes' partial sums of one chunk -> the chunk's sum: a butterfly over
+// the kTreeLanes threads of the block (every thread returns the sum).
+__device__ __forceinline__ double ChunkButterfly(double s, double* shared) {
+  const int t = threadIdx.x;
+  shared[t] = s;
+  __syncthreads();
+#pragma unroll
+  for (int stride = kTreeLanes / 2; stride >= kWarp; stride >>= 1) {
+    const double other = shared[t ^ stride];
+    __syncthreads();
+    s = Add(s, other);
+    shared[t] = s;
+    __syncthreads();
+  }
+#pragma unroll
+  for (int stride = kWarp / 2; stride >= 1; stride >>= 1) {
+    s = Add(s, __shfl_xor_sync(0xffffffffu, s, stride));
+  }
+  return s;
+}
+
 __global__ void TreeChunkKernel(TreeArgs args, int64_t n, double* __restrict__ out, int64_t out_stride) {
   __shared__ double shared[kTreeLanes];
   const double* __restrict__ src = args.src[blockIdx.y];
@@ -126,21 +149,28 @@ __global__ void TreeChunkKernel(TreeArgs args, int64_t n, double* __restrict__ o
       if (i < n) s = Add(s, src[i]);
     }
   }
-  shared[t] = s;
-  __syncthreads();
-#pragma unroll
-  for (int stride = kTreeLanes / 2; stride >= kWarp; stride >>= 1) {
-    const double other = shared[t ^ stride];
-    __syncthreads();
-    s = Add(s, other);
-    shared[t] = s;
-    __syncthreads();
-  }
-#pragma unroll
-  for (int stride = kWarp / 2; stride >= 1; stride >>= 1) {
-    s = Add(s, __shfl_xor_sync(0xffffffffu, s, stride));
-  }
+  s = ChunkButterfly(s, shared);
   if (t == 0) out[blockIdx.y * out_stride + blockIdx.x] = s;
+}
+
+// One level of the tree over many segments at once.  Block b sums
+// src[start[b], end[b]) (at most one chunk, lanes as TreeChunkKernel) into
+// out[dst[b]]; table = start[blocks] | end[blocks] | dst[blocks].
+__global__ void SegmentChunkKernel(TreeArgs args, const int64_t* __restrict__ table, int64_t blocks,
+                                   double* __restrict__ out, int64_t out_stride) {
+  __shared__ double shared[kTreeLanes];
+  const double* __restrict__ src = args.src[blockIdx.y];
+  const int t = threadIdx.x;
+  const int64_t start = table[blockIdx.x];
+  const int64_t end = table[blocks + blockIdx.x];
+  double s = 0.0;
+#pragma unroll
+  for (int m = 0; m < static_cast<int>(kTreeChunk / kTreeLanes); ++m) {
+    const int64_t i = start + t + static_cast<int64_t>(kTreeLanes) * m;
+    if (i < end) s = Add(s, src[i]);
+  }
+  s = ChunkButterfly(s, shared);
+  if (t == 0) out[blockIdx.y * out_stride + table[2 * blocks + blockIdx.x]] = s;
 }
 
 // ---------------------------------------------------------------------------
@@ -1122,6 +1152,89 @@ void TreeDots(Ctx& ctx, const double* const* x, const double* const* y, int arra
     }
     scratch_at += static_cast<size_t>(arrays) * chunks;
     count = chunks;
+  }
+}
+
+void SegmentTree::Build(Ctx& ctx, const std::vector<int64_t>& offsets) {
+  const int64_t segments = static_cast<int64_t>(offsets.size()) - 1;
+  segments_ = segments;
+  final_at_.assign(static_cast<size_t>(segments), -1);
+  levels_.clear();
+  std::vector<int64_t> table;
+  // the segments still being reduced: [lo, hi) in the current level's source
+  std::vector<int64_t> lo(offsets.begin(), offsets.end() - 1);
+  std::vector<int64_t> hi(offsets.begin() + 1, offsets.end());
+  std::vector<int64_t> owner(static_cast<size_t>(segments));
+  for (int64_t s = 0; s < segments; ++s) owner[s] = s;
+  int64_t slots = 0;
+  while (!owner.empty()) {
+    std::vector<int64_t> start;
+    std::vector<int64_t> end;
+    std::vector<int64_t> dst;
+    std::vector<int64_t> next_lo;
+    std::vector<int64_t> next_hi;
+    std::vector<int64_t> next_owner;
+    for (size_t k = 0; k < owner.size(); ++k) {
+      const int64_t len = hi[k] - lo[k];
+      if (len <= 0) continue;  // an empty segment sums to +0.0, as TreeSums gives
+      const int64_t chunks = CeilDiv(len, kTreeChunk);
+      if (chunks == 1) final_at_[owner[k]] = slots;
+      for (int64_t c = 0; c < chunks; ++c) {
+        start.push_back(lo[k] + c * kTreeChunk);
+        end.push_back(std::min(lo[k] + (c + 1) * kTreeChunk, hi[k]));
+        dst.push_back(slots + c);
+      }
+      if (chunks > 1) {
+        next_lo.push_back(slots);
+        next_hi.push_back(slots + chunks);
+        next_owner.push_back(owner[k]);
+      }
+      slots += chunks;
+    }
+    if (!start.empty()) {
+      Level level;
+      level.blocks = static_cast<int64_t>(start.size());
+      level.table_at = static_cast<int64_t>(table.size());
+      table.insert(table.end(), start.begin(), start.end());
+      table.insert(table.end(), end.begin(), end.end());
+      table.insert(table.end(), dst.begin(), dst.end());
+      levels_.push_back(level);
+    }
+    lo.swap(next_lo);
+    hi.swap(next_hi);
+    owner.swap(next_owner);
+  }
+  slots_ = slots;
+  table_.Reserve(table.empty() ? 1 : table.size(), ctx.stream);
+  if (!table.empty()) {
+    SPAI_CUDA(cudaMemcpyAsync(table_.data(), table.data(), sizeof(int64_t) * table.size(), cudaMemcpyHostToDevice,
+                              ctx.stream));
+  }
+  ctx.Sync();
+}
+
+void SegmentTree::Sums(Ctx& ctx, const double* const* partials, int arrays, double* out) {
+  if (arrays > 8) throw std::invalid_argument("SegmentTree::Sums takes at most 8 arrays");
+  values_.Reserve(static_cast<size_t>(arrays) * (slots_ > 0 ? slots_ : 1), ctx.stream);
+  TreeArgs args{};
+  for (size_t l = 0; l < levels_.size(); ++l) {
+    for (int a = 0; a < arrays; ++a) args.src[a] = l == 0 ? partials[a] : values_.data() + a * slots_;
+    dim3 grid(static_cast<unsigned>(levels_[l].blocks), static_cast<unsigned>(arrays));
+    SegmentChunkKernel<<<grid, kTreeLanes, 0, ctx.stream>>>(args, table_.data() + levels_[l].table_at,
+                                                            levels_[l].blocks, values_.data(), slots_);
+    SPAI_LAUNCH_CHECK();
+  }
+  host_.resize(static_cast<size_t>(arrays) * slots_);
+  if (slots_ > 0) {
+    SPAI_CUDA(cudaMemcpyAsync(host_.data(), values_.data(), sizeof(double) * host_.size(), cudaMemcpyDeviceToHost,
+                              ctx.stream));
+  }
+  ctx.Sync();
+  for (int a = 0; a < arrays; ++a) {
+    for (int64_t s = 0; s < segments_; ++s) {
+      const int64_t at = final_at_[s];
+      out[a * segments_ + s] = at < 0 ? 0.0 : host_[a * slots_ + at];
+    }
   }
 }
 

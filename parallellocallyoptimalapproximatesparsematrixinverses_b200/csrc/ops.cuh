@@ -88,6 +88,32 @@ void TreeSums(Ctx& ctx, const double* const* partials, int arrays, int64_t n, in
 void TreeDots(Ctx& ctx, const double* const* x, const double* const* y, int arrays, int64_t n, int slot);
 void FetchScalars(Ctx& ctx, int first_slot, int count, double* out);
 
+// The same tree applied to every segment [offsets[s], offsets[s + 1]) of a
+// per-column array on its own (the diagonal blocks of a batch): each
+// segment's sum has the bits TreeSums gives for that segment alone.  Build
+// once per segmentation; every Sums call is one launch per tree level over
+// all segments and one read-back.
+class SegmentTree {
+ public:
+  void Build(Ctx& ctx, const std::vector<int64_t>& offsets);
+  // out[a * segments + s] = the tree sum of partials[a] over segment s (host), a < arrays <= 8.
+  void Sums(Ctx& ctx, const double* const* partials, int arrays, double* out);
+  int64_t segments() const { return segments_; }
+
+ private:
+  struct Level {
+    int64_t blocks = 0;
+    int64_t table_at = 0;
+  };
+  std::vector<Level> levels_;
+  std::vector<int64_t> final_at_;  // slot of each segment's sum (-1: empty segment)
+  int64_t segments_ = 0;
+  int64_t slots_ = 0;              // per-array slots over all levels
+  DevBuf<int64_t> table_;
+  DevBuf<double> values_;
+  std::vector<double> host_;
+};
+
 // Per-column sequential partial sums (storage order, as Eigen within a column).
 template <class T>
 void ColumnSquares(Ctx& ctx, CscView<T> x, double* partial);

@@ -33,6 +33,24 @@ __device__ __forceinline__ double SafeQuotient(double num, double den) {
   return isfinite(q) ? q : 0.0;
 }
 
+// out[i] = ptr[at[i]]: the column offsets of a matrix at the block boundaries.
+__global__ void GatherOffsetsKernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ at, int64_t count,
+                                    int64_t* __restrict__ out) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[i] = ptr[at[i]];
+  }
+}
+
+// per_column[j] = per_block[block of column j].
+__global__ void BroadcastBlocksKernel(const int32_t* __restrict__ block_of, const double* __restrict__ per_block,
+                                      int64_t n, double* __restrict__ per_column) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    per_column[j] = per_block[block_of[j]];
+  }
+}
+
 // Per-column Inner-Outer step lengths (inner_outer_common.hpp:50-69).
 __global__ void InnerOuterStepKernel(int64_t n, const double* __restrict__ r_az, const double* __restrict__ az_az,
                                      const double* __restrict__ az_aq, const double* __restrict__ aq_aq,
@@ -264,6 +282,205 @@ class Solver final : public SolverBase {
     out.history = history_;
     out.iterations = iterations_;
     out.converged = converged_;
+  }
+
+  // Batched Global MR: the loop of RunMr (minimal_residual.cpp:31-93) per
+  // diagonal block.  Every block follows the single-system arithmetic bit for
+  // bit: the products, unions and drop steps are column-local, and each
+  // block's scalars come from the fixed tree over that block's columns
+  // (SegmentTree).  A block that stops (converged, density limit, breakdown,
+  // iteration limit) has its M copied out at that moment; afterwards it rides
+  // along with step length 0 and its results are no longer read.
+  void RunMrBatched(const std::vector<int64_t>& offsets, std::vector<SolveOutput>& outputs) override {
+    const int64_t blocks = static_cast<int64_t>(offsets.size()) - 1;
+    if (blocks <= 0 || offsets.front() != 0 || offsets.back() != n_) throw std::invalid_argument("bad block offsets");
+    if (!pr_diagonal_) throw std::invalid_argument("batched runs use a diagonal Pr");
+    if (opt_.dropping && opt_.topk <= 0) throw std::invalid_argument("batched runs need top-k dropping or none");
+    SegmentTree tree;
+    tree.Build(ctx_, offsets);
+    std::vector<int32_t> block_of(static_cast<size_t>(n_));
+    for (int64_t b = 0; b < blocks; ++b) {
+      for (int64_t j = offsets[b]; j < offsets[b + 1]; ++j) block_of[j] = static_cast<int32_t>(b);
+    }
+    DevBuf<int32_t> block_of_dev;
+    DevBuf<int64_t> bounds_dev;
+    DevBuf<int64_t> gathered;
+    DevBuf<double> alpha_dev;
+    block_of_dev.Reserve(static_cast<size_t>(n_), ctx_.stream);
+    bounds_dev.Reserve(static_cast<size_t>(blocks + 1), ctx_.stream);
+    gathered.Reserve(static_cast<size_t>(2 * (blocks + 1)), ctx_.stream);
+    alpha_dev.Reserve(static_cast<size_t>(blocks), ctx_.stream);
+    SPAI_CUDA(cudaMemcpyAsync(block_of_dev.data(), block_of.data(), sizeof(int32_t) * n_, cudaMemcpyHostToDevice,
+                              ctx_.stream));
+    SPAI_CUDA(cudaMemcpyAsync(bounds_dev.data(), offsets.data(), sizeof(int64_t) * (blocks + 1),
+                              cudaMemcpyHostToDevice, ctx_.stream));
+    ctx_.Sync();
+
+    outputs.assign(static_cast<size_t>(blocks), SolveOutput());
+    std::vector<char> active(static_cast<size_t>(blocks), 1);
+    int64_t live = blocks;
+    std::vector<double> sums(static_cast<size_t>(2 * blocks));
+    std::vector<int64_t> m_at(static_cast<size_t>(blocks + 1));
+    std::vector<int64_t> z_at(static_cast<size_t>(blocks + 1));
+    std::vector<int> stopping;
+
+    // nnz of M and Z per block: their column offsets at the block boundaries
+    auto fetch_counts = [&]() {
+      const int g = GridFor(blocks + 1, 128);
+      GatherOffsetsKernel<<<g, 128, 0, ctx_.stream>>>(m_.ptr.data(), bounds_dev.data(), blocks + 1, gathered.data());
+      SPAI_LAUNCH_CHECK();
+      GatherOffsetsKernel<<<g, 128, 0, ctx_.stream>>>(z_.ptr.data(), bounds_dev.data(), blocks + 1,
+                                                      gathered.data() + blocks + 1);
+      SPAI_LAUNCH_CHECK();
+      SPAI_CUDA(cudaMemcpyAsync(m_at.data(), gathered.data(), sizeof(int64_t) * (blocks + 1), cudaMemcpyDeviceToHost,
+                                ctx_.stream));
+      SPAI_CUDA(cudaMemcpyAsync(z_at.data(), gathered.data() + blocks + 1, sizeof(int64_t) * (blocks + 1),
+                                cudaMemcpyDeviceToHost, ctx_.stream));
+      ctx_.Sync();
+    };
+    // ||R||_F per block from the column squares the last residual product left
+    auto residual_norms = [&](std::vector<double>& out) {
+      if (!r_squares_ready_) ColumnSquares(ctx_, View(r_), ctx_.Partial(kResidualPartial, n_));
+      const double* parts[1] = {ctx_.Partial(kResidualPartial, n_)};
+      tree.Sums(ctx_, parts, 1, sums.data());
+      out.resize(static_cast<size_t>(blocks));
+      for (int64_t b = 0; b < blocks; ++b) out[b] = std::sqrt(sums[b]);
+    };
+    // M of every block in `stopping` to its output (local indices, FP64 values)
+    auto snapshot = [&]() {
+      if (stopping.empty()) return;
+      fetch_counts();
+      std::vector<int32_t> idx;
+      std::vector<T> val;
+      for (const int b : stopping) {
+        SolveOutput& out = outputs[b];
+        const int64_t c0 = offsets[b];
+        const int64_t cols = offsets[b + 1] - c0;
+        const int64_t p0 = m_at[b];
+        const int64_t nnz = m_at[b + 1] - p0;
+        out.rows = cols;
+        out.cols = cols;
+        out.ptr.resize(static_cast<size_t>(cols + 1));
+        SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), m_.ptr.data() + c0, sizeof(int64_t) * (cols + 1),
+                                  cudaMemcpyDeviceToHost, ctx_.stream));
+        idx.resize(static_cast<size_t>(nnz));
+        val.resize(static_cast<size_t>(nnz));
+        if (nnz > 0) {
+          SPAI_CUDA(cudaMemcpyAsync(idx.data(), m_.idx.data() + p0, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost,
+                                    ctx_.stream));
+          SPAI_CUDA(cudaMemcpyAsync(val.data(), m_.val.data() + p0, sizeof(T) * nnz, cudaMemcpyDeviceToHost,
+                                    ctx_.stream));
+        }
+        ctx_.Sync();
+        for (int64_t j = 0; j <= cols; ++j) out.ptr[j] -= p0;
+        out.idx.resize(static_cast<size_t>(nnz));
+        out.val.resize(static_cast<size_t>(nnz));
+        for (int64_t p = 0; p < nnz; ++p) {
+          out.idx[p] = static_cast<int64_t>(idx[p]) - c0;
+          out.val[p] = static_cast<double>(val[p]);
+        }
+        active[b] = 0;
+        --live;
+      }
+      stopping.clear();
+    };
+    // AppendIteration (result_operations.cpp:53-67) for every live block
+    auto append = [&](const std::vector<double>& residual) {
+      fetch_counts();
+      for (int64_t b = 0; b < blocks; ++b) {
+        if (!active[b]) continue;
+        SolveOutput& out = outputs[b];
+        const double nb = static_cast<double>(offsets[b + 1] - offsets[b]);
+        const double entries = nb * nb;
+        SingleIterationData row;
+        row.iteration = static_cast<int64_t>(out.history.size());
+        out.iterations = row.iteration;
+        row.residual_norm = residual[b];
+        row.density_m = static_cast<double>(m_at[b + 1] - m_at[b]) / entries;
+        row.density_direction = static_cast<double>(z_at[b + 1] - z_at[b]) / entries;
+        out.history.push_back(row);
+        if (row.residual_norm < opt_.tolerance) {
+          out.converged = true;
+          stopping.push_back(static_cast<int>(b));
+        } else if (!opt_.dropping && opt_.max_density < 1.0 && row.density_m >= opt_.max_density) {
+          stopping.push_back(static_cast<int>(b));
+        }
+      }
+      snapshot();
+    };
+    // <Z, Pr A Z> and ||Pr A Z||^2 per block: the fused projection, reduced per block
+    std::vector<double> num(static_cast<size_t>(blocks));
+    std::vector<double> den(static_cast<size_t>(blocks));
+    auto projection = [&]() {
+      double* tt = ctx_.Partial(0, n_);
+      double* bt = ctx_.Partial(1, n_);
+      SpgemmExtras extras = AExtras();
+      extras.row_scale = pr_vec_.data();
+      extras.proj_tt = tt;
+      extras.proj_bt = bt;
+      DevCsc<T> unused;
+      Spgemm(ctx_, A(), a_csr_, z_, unused, Epilogue::kProjection, extras);
+      const double* parts[2] = {bt, tt};
+      tree.Sums(ctx_, parts, 2, sums.data());
+      for (int64_t b = 0; b < blocks; ++b) {
+        num[b] = sums[b];
+        den[b] = sums[blocks + b];
+      }
+    };
+
+    // PrepareStateManager (methods_common.cpp:126-157) on every block
+    Copy(ctx_, m0_, m_);
+    for (DevCsc<T>* x : {&r_, &z_, &p_, &ap_, &az_, &tmp_, &q_}) Empty(*x);
+    InvalidateResidualExtras();
+    symmetric_ = true;
+    if (opt_.dropping) {
+      ApplyDroppingStrategy();
+    } else {
+      Residual();
+    }
+    std::vector<double> residual;
+    residual_norms(residual);
+    ComputeZ();
+    append(residual);
+    if (live > 0) projection();
+    std::vector<double> alpha(static_cast<size_t>(blocks));
+    DevCsc<T> scaled;
+    for (int64_t i = 1; i <= opt_.max_iterations && live > 0; ++i) {
+      for (int64_t b = 0; b < blocks; ++b) {
+        alpha[b] = 0.0;
+        if (!active[b]) continue;
+        const double a = num[b] / den[b];
+        if (!FiniteNonZeroHost(den[b]) || !std::isfinite(a)) {
+          stopping.push_back(static_cast<int>(b));
+        } else {
+          alpha[b] = a;
+        }
+      }
+      snapshot();
+      if (live == 0) break;
+      // M += alpha_b Z per block: Z scaled per column, then the union with
+      // coefficient 1 (the same products and sums as the scalar union)
+      SPAI_CUDA(cudaMemcpyAsync(alpha_dev.data(), alpha.data(), sizeof(double) * blocks, cudaMemcpyHostToDevice,
+                                ctx_.stream));
+      double* alpha_col = ColVec(0);
+      BroadcastBlocksKernel<<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(block_of_dev.data(), alpha_dev.data(), n_,
+                                                                      alpha_col);
+      SPAI_LAUNCH_CHECK();
+      Copy(ctx_, z_, scaled);
+      ScaleColumns(ctx_, scaled, alpha_col);
+      Union(ctx_, m_, false, 1.0, scaled, 1.0, m_, UnionMode::kAxpby);
+      UpdateResiduals([&] { Residual(); }, false);
+      residual_norms(residual);
+      append(residual);
+      if (live == 0) break;
+      ComputeZ();
+      projection();
+    }
+    for (int64_t b = 0; b < blocks; ++b) {
+      if (active[b]) stopping.push_back(static_cast<int>(b));
+    }
+    snapshot();
+    ctx_.Sync();
   }
 
   int64_t iterations() const override { return iterations_; }

@@ -79,6 +79,12 @@ class SolverBase {
   // Device CSR copy of the current M (rows as major), values widened to FP64
   // or kept in FP32 depending on want_fp32; used by the PCG evaluator.
   virtual void ExportMForPcg(void* csr_out, bool want_fp32) = 0;
+  // Global MR on every diagonal block of the uploaded A on its own: block b
+  // is rows and columns [offsets[b], offsets[b + 1]), with Pr = diag(A)^-1 and
+  // per-column top-k or no dropping (the rules that stay inside a block).
+  // Every launch covers all blocks; the step lengths, norms and stop rules
+  // are per block.  outputs[b] gets block b's M (local indices) and history.
+  virtual void RunMrBatched(const std::vector<int64_t>& offsets, std::vector<SolveOutput>& outputs) = 0;
   virtual const void* DeviceA() const = 0;  // DevCsc<double>* when precision == 0, else DevCsc<float>*
   virtual const void* DeviceA64() const = 0;  // DevCsc<double>* (always)
   virtual int64_t n() const = 0;

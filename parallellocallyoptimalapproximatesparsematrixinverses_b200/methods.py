@@ -152,6 +152,36 @@ class GlobalSpaiMethods:
         return _call_method("global_spai", "lomr", A, M0, Pr, max_iterations, tolerance, max_density,
                             enable_dropping, num_threads, **ext)
 
+    def mr_batched(self, As, M0s=None, max_iterations=100, tolerance=1e-9, max_density=0.03, enable_dropping=True,
+                   num_threads=1, topk_per_column=0, precision="fp64", device=-1):
+        """`mr` on many independent systems in one batch (libspai_b200.so
+        spai_mr_batched): one list entry per system, each what `mr` returns
+        for that system alone with Pr = diag(A)^-1.  Dropping, when enabled,
+        must be per column (topk_per_column > 0)."""
+        lib = _lib.load()
+        As = [as_csc(A) for A in As]
+        count = len(As)
+        if count == 0:
+            return []
+        if M0s is not None:
+            if len(M0s) != count:
+                raise ValueError("M0s must have one matrix per system")
+            M0s = [as_csc(M, A.shape) for M, A in zip(M0s, As)]
+        params = _lib.MethodParams(max_iterations, tolerance, max_density, 1 if enable_dropping else 0, num_threads,
+                                   1 if M0s is not None else 0, 0, 2)
+        ext = ext_params(precision, topk_per_column, device)
+        a_data = (_lib.MatrixData * count)(*[matrix_data(A) for A in As])
+        m_data = (_lib.MatrixData * count)(*[matrix_data(M) for M in M0s]) if M0s is not None else None
+        results = (_lib.Result * count)()
+        err = _lib.error_buffer()
+        rc = lib.spai_mr_batched(count, a_data, m_data, params, ctypes.byref(ext), results, err, len(err))
+        if rc != 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        out = []
+        for b in range(count):
+            out.append(result_to_python(results[b]))
+        return out
+
 
 class InnerOuterMethods:
     """Reference methods.pyx:225-254."""

@@ -15,6 +15,10 @@ generators, `numpy.random.default_rng(seed)`).
   absolute row sum.
 * tridiagonal(n): tridiag(-1, 2, -1), the reference's C++ test fixture
   (tests/test.cpp:13-28).
+* diffusion_batch(count, seed, n_min, n_max): many independent systems for
+  batched runs.  Per system: n log-uniform in [n_min, n_max], a 5-point 2-D
+  or 7-point 3-D grid (fair coin) with side round(n^(1/2)) or round(n^(1/3)),
+  log-normal coefficients with sigma 0.5, plus a diagonal shift U(0, 0.1).
 """
 from __future__ import annotations
 
@@ -106,6 +110,25 @@ def random_banded_spd(n: int, half_width: int = 4, extra: int = 6, seed: int = 0
     a.sum_duplicates()
     a.sort_indices()
     return a
+
+
+def diffusion_batch(count: int = 256, seed: int = 0, n_min: int = 1000, n_max: int = 64000):
+    rng = np.random.default_rng(seed)
+    out = []
+    for b in range(count):
+        n = float(np.exp(rng.uniform(np.log(n_min), np.log(n_max))))
+        three_d = bool(rng.integers(0, 2))
+        system_seed = int(rng.integers(0, 2**31 - 1))
+        shift = float(rng.uniform(0.0, 0.1))
+        if three_d:
+            a = diffusion_3d(max(2, int(round(n ** (1.0 / 3.0)))), 0.5, system_seed)
+        else:
+            a = diffusion_2d(max(2, int(round(n ** 0.5))), 0.5, system_seed)
+        a = sparse.csc_matrix(a + shift * sparse.identity(a.shape[0], format="csc"))
+        a.sum_duplicates()
+        a.sort_indices()
+        out.append(a)
+    return out
 
 
 def diagonal_inverse(a) -> sparse.csc_matrix:
