@@ -20,7 +20,8 @@ storage of M, R, Z, A; FP64 reductions; PCG in FP64 with FP32 M-apply), timed
 with CUDA events on the library's stream, inputs resident in HBM, L2 flushed
 before every step.  The same line carries the PCG time to 1e-8, the FP64 step
 for comparison, the end-to-end figure through the C ABI with host buffers,
-the roofline of the dominant kernel and the CPU baseline.
+the roofline of the dominant kernel and the CPU baseline, plus a batched leg
+(256 independent systems in one call, against one call per system).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -60,6 +61,10 @@ def parse_args():
     p.add_argument("--pcg-max-iterations", type=int, default=5000)
     p.add_argument("--skip-cpu-baseline", action="store_true")
     p.add_argument("--skip-e2e", action="store_true")
+    p.add_argument("--skip-batched", action="store_true")
+    p.add_argument("--batch-count", type=int, default=256, help="systems in the batched leg")
+    p.add_argument("--batch-iterations", type=int, default=15)
+    p.add_argument("--batch-topk", type=int, default=10)
     return p.parse_args()
 
 
@@ -343,6 +348,8 @@ def run_ours(args):
         s.close()
 
     if rank == 0 and world == 1:
+        if not args.skip_batched:
+            line["batched"] = batched_leg(args, local)
         if not args.skip_e2e:
             line["e2e"] = e2e(args, A, M0, b)
         if not args.skip_cpu_baseline:
@@ -351,6 +358,41 @@ def run_ours(args):
         print(json.dumps(line), flush=True)
     if group is not None:
         group.destroy_process_group()
+
+
+def batched_leg(args, device):
+    """Many small systems: `global_spai.mr_batched` (one block-diagonal batch,
+    every launch over all systems) against one `global_spai.mr` call per
+    system, both through the public API with host buffers (wall clock; host
+    assembly, uploads and downloads included)."""
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import global_spai, problems
+    systems = problems.diffusion_batch(args.batch_count, seed=0)
+    kw = dict(max_iterations=args.batch_iterations, tolerance=1e-12, max_density=1.0,
+              topk_per_column=args.batch_topk, precision="mixed", device=device)
+    global_spai.mr_batched(systems, **kw)  # warm-up
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        out = global_spai.mr_batched(systems, **kw)
+        times.append(time.perf_counter() - t0)
+    seconds = statistics.mean(times)
+    iterations = sum(r.iterations for r in out)
+    t0 = time.perf_counter()
+    for A in systems:
+        global_spai.mr(A, **kw)
+    one_by_one = time.perf_counter() - t0
+    return {
+        "workload": f"{len(systems)} systems, n log-uniform in [1000, 64000], 2-D 5-pt / 3-D 7-pt, sigma 0.5, "
+                    f"diagonal shift U(0, 0.1); Global MR {args.batch_iterations} it, top-{args.batch_topk}, mixed",
+        "rows": int(sum(A.shape[0] for A in systems)),
+        "nnz": int(sum(A.nnz for A in systems)),
+        "seconds_per_batch": round(seconds, 4),
+        "systems_per_s": round(len(systems) / seconds, 2),
+        "spai_iters_per_s": round(iterations / seconds, 1),
+        "one_call_per_system_seconds": round(one_by_one, 3),
+        "speedup_vs_one_call_per_system": round(one_by_one / seconds, 2),
+        "timing": "wall clock around the public API call, mean of 2 after 1 warm-up",
+    }
 
 
 def e2e(args, A, M0, b):
