@@ -172,6 +172,25 @@ int64_t spai_pcg_adjoint(int64_t n, const double* a_values, const int64_t* a_ind
                          const double* grad_x, PcgParams params, double* grad_b, double* grad_a, double* history,
                          int64_t* status, char* error, int64_t error_capacity);
 
+/* ---- Matrix Market files, read and written natively (host) ---- */
+
+/* Reads a Matrix Market matrix file (coordinate or array; real, integer or
+ * pattern; general, symmetric or skew-symmetric) into the canonical CSC the
+ * reference's loader builds (scripts/common.py:397-402: mmread, tocsc,
+ * sum_duplicates, eliminate_zeros, sort_indices): symmetric entries mirrored,
+ * duplicates summed in file order, explicit zeros removed, rows ascending.
+ * threads <= 0: all hardware threads.  The Result carries rows, cols, nnz,
+ * col_offsets, row_indices and values (history empty); free it with
+ * free_mem.  On failure only error_message is set. */
+struct Result spai_mtx_read(const char* path, int64_t threads);
+
+/* Writes CSC m as "%%MatrixMarket matrix coordinate real general" (or
+ * "symmetric" with only the entries on or below the diagonal; the caller
+ * vouches for the symmetry), 1-based, values with 17 significant digits so
+ * that they read back to the same bits.  Returns 0, or -1 with `error`. */
+int64_t spai_mtx_write(const char* path, struct MatrixData m, int64_t symmetric, char* error,
+                       int64_t error_capacity);
+
 /* y = A x for CSR A (backward_error.pyx:56-66 `matvec`); returns 0, or -1 with `error`. */
 int64_t spai_matvec(int64_t n, const double* values, const int64_t* indices, const int64_t* offsets,
                     const double* x, double* y, int64_t device, char* error, int64_t error_capacity);

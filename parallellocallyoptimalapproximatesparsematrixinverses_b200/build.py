@@ -18,7 +18,7 @@ LIB_PATH = PACKAGE_DIR / "libspai_b200.so"
 BUILD_DIR = PACKAGE_DIR / "_build"
 
 SOURCES = ["ops.cu", "spgemm.cu", "update.cu", "solver.cu", "pcg.cu", "c_api.cu", "profile.cu", "noalloc.cu",
-           "adjoint.cu"]
+           "adjoint.cu", "mtx.cpp"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
