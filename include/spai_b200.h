@@ -66,7 +66,10 @@ typedef struct SpaiExtParams {
   int64_t topk_per_column; /* 0: the reference's global budget max(n, floor(max_density*n^2)) (dropping.cpp:122-224);
                               K > 0: keep at most K entries per column by magnitude (diagonal of M protected) */
   int64_t device;          /* CUDA device ordinal; -1: the calling thread's current device */
-  int64_t reserved;        /* must be 0 */
+  int64_t summation_order; /* 0: the device order (sequential per column, then a fixed 4096-wide tree);
+                              1: the reference's order (min(n, num_threads) column batches, each global sum
+                              sequential through a batch, then over the batches; methods_common.cpp:78-103):
+                              FP64 runs then reproduce the reference's own results bit for bit */
 } SpaiExtParams;
 
 /* Method ids for spai_run_ex / sessions. */

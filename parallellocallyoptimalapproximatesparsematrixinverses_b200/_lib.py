@@ -49,7 +49,7 @@ class Result(ctypes.Structure):
 
 class SpaiExtParams(ctypes.Structure):
     """include/spai_b200.h SpaiExtParams."""
-    _fields_ = [("precision", _i64), ("topk_per_column", _i64), ("device", _i64), ("reserved", _i64)]
+    _fields_ = [("precision", _i64), ("topk_per_column", _i64), ("device", _i64), ("summation_order", _i64)]
 
 
 class PcgParams(ctypes.Structure):

@@ -128,10 +128,14 @@ SolveOptions CheckInputs(int64_t method, const MatrixData& A, const MatrixData& 
   if (ext != nullptr) {
     if (ext->precision != 0 && ext->precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
     if (ext->topk_per_column < 0) throw std::invalid_argument("topk_per_column must be non-negative");
-    if (ext->reserved != 0) throw std::invalid_argument("SpaiExtParams.reserved must be 0");
+    if (ext->summation_order != 0 && ext->summation_order != 1) {
+      throw std::invalid_argument("summation_order must be 0 (device tree) or 1 (the reference's batches)");
+    }
     opt.precision = static_cast<int>(ext->precision);
     opt.topk = ext->topk_per_column;
+    opt.summation = static_cast<int>(ext->summation_order);
   }
+  opt.num_threads = params.num_threads;
   return opt;
 }
 
@@ -414,7 +418,7 @@ int64_t spai_mr_batched(int64_t count, const MatrixData* A, const MatrixData* M0
     opt.dropping = params.enable_dropping != 0;
     if (ext != nullptr) {
       if (ext->precision != 0 && ext->precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
-      if (ext->reserved != 0) throw std::invalid_argument("SpaiExtParams.reserved must be 0");
+      if (ext->summation_order != 0) throw std::invalid_argument("batched runs use the device summation order");
       opt.precision = static_cast<int>(ext->precision);
       opt.topk = topk;
     }

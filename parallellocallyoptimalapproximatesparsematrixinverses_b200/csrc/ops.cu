@@ -299,7 +299,10 @@ struct KeepNonZero {
 template <class T>
 struct KeepAboveLimit {
   double limit;
-  __device__ void Begin(const CscView<T>&, int64_t, int) {}
+  const double* column_limit = nullptr;  // when set: the limit of each column
+  __device__ void Begin(const CscView<T>&, int64_t col, int) {
+    if (column_limit != nullptr) limit = column_limit[col];
+  }
   __device__ bool Keep(int64_t, int64_t, int32_t, T v) const {
     return !(fabs(static_cast<double>(v)) <= limit);
   }
@@ -1361,6 +1364,11 @@ void PruneAbsAtMost(Ctx& ctx, DevCsc<T>& x, double limit) {
 }
 
 template <class T>
+void PruneAbsAtMostPerColumn(Ctx& ctx, DevCsc<T>& x, const double* column_limit) {
+  RunFilter(ctx, x, KeepAboveLimit<T>{0.0, column_limit});
+}
+
+template <class T>
 void KeepTopKPerColumn(Ctx& ctx, DevCsc<T>& x, int64_t k, bool protect_diagonal) {
   KeepTopK<T> pred;
   pred.k = k;
@@ -1496,6 +1504,7 @@ void ConvertValues(Ctx& ctx, const S* src, D* dst, int64_t n) {
                                  const T*, int32_t*, T*);                                                        \
   template void PruneColumnRelative<T>(Ctx&, DevCsc<T>&);                                                     \
   template void PruneAbsAtMost<T>(Ctx&, DevCsc<T>&, double);                                                  \
+  template void PruneAbsAtMostPerColumn<T>(Ctx&, DevCsc<T>&, const double*);                                  \
   template void KeepTopKPerColumn<T>(Ctx&, DevCsc<T>&, int64_t, bool);                                        \
   template void GlobalDropByScore<T>(Ctx&, DevCsc<T>&, const double*, bool, int64_t);                         \
   template void Transpose<T>(Ctx&, const DevCsc<T>&, DevCsc<T>&);                                             \

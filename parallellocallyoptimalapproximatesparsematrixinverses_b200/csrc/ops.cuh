@@ -172,6 +172,9 @@ void PruneColumnRelative(Ctx& ctx, DevCsc<T>& m);
 // keep iff !(|v| <= limit)   (dropping.cpp:182-185 with limit = ||X||_F * eps)
 template <class T>
 void PruneAbsAtMost(Ctx& ctx, DevCsc<T>& x, double limit);
+// the same with a limit per column (device array of x.cols values)
+template <class T>
+void PruneAbsAtMostPerColumn(Ctx& ctx, DevCsc<T>& x, const double* column_limit);
 // keep the k largest (|v|, row) per column; the diagonal is always kept (and
 // counts toward k) when protect_diagonal.
 template <class T>

@@ -33,6 +33,51 @@ __device__ __forceinline__ double SafeQuotient(double num, double den) {
   return isfinite(q) ? q : 0.0;
 }
 
+// The reference's summation order: thread per column batch, sequential over
+// the batch's columns in storage order (AccSquares / AccDot of a batch).
+template <class T>
+__global__ void BatchSquaresKernel(CscView<T> x, const int64_t* __restrict__ first, int64_t batches,
+                                   double* __restrict__ out) {
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < batches;
+       b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int64_t p = x.ptr[first[b]]; p < x.ptr[first[b + 1]]; ++p) {
+      const double v = static_cast<double>(x.val[p]);
+      s = Add(s, Mul(v, v));
+    }
+    out[b] = s;
+  }
+}
+
+template <class T>
+__global__ void BatchDotsKernel(CscView<T> x, CscView<T> y, const int64_t* __restrict__ first, int64_t batches,
+                                double* __restrict__ out) {
+  for (int64_t b = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; b < batches;
+       b += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double s = 0.0;
+    for (int64_t j = first[b]; j < first[b + 1]; ++j) {
+      int64_t p = x.ptr[j];
+      int64_t q = y.ptr[j];
+      const int64_t pe = x.ptr[j + 1];
+      const int64_t qe = y.ptr[j + 1];
+      while (p < pe && q < qe) {
+        const int32_t rp = x.idx[p];
+        const int32_t rq = y.idx[q];
+        if (rp == rq) {
+          s = Add(s, Mul(static_cast<double>(x.val[p]), static_cast<double>(y.val[q])));
+          ++p;
+          ++q;
+        } else if (rp < rq) {
+          ++p;
+        } else {
+          ++q;
+        }
+      }
+    }
+    out[b] = s;
+  }
+}
+
 // out[i] = ptr[at[i]]: the column offsets of a matrix at the block boundaries.
 __global__ void GatherOffsetsKernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ at, int64_t count,
                                     int64_t* __restrict__ out) {
@@ -170,6 +215,7 @@ class Solver final : public SolverBase {
     }
     Transpose(ctx_, A(), a_csr_);
     BuildAEll(a);
+    if (ReferenceOrder()) InitReferenceBatches();
     // ||A e_k||^2 per column (methods_common.cpp:65-76)
     col_norm2_.Reserve(static_cast<size_t>(n_), ctx_.stream);
     if (opt_.dropping) {
@@ -631,6 +677,7 @@ class Solver final : public SolverBase {
 
   // ---- reductions ----------------------------------------------------------
   double Dot(const DevCsc<T>& x, const DevCsc<T>& y) {
+    if (ReferenceOrder()) return BatchTotal(BatchSums(&x, &y));
     double* part = ctx_.Partial(0, n_);
     ColumnDots(ctx_, View(x), View(y), part);
     const double* parts[1] = {part};
@@ -641,6 +688,7 @@ class Solver final : public SolverBase {
   }
 
   double SquaredNorm(const DevCsc<T>& x) {
+    if (ReferenceOrder()) return BatchTotal(BatchSums(&x, nullptr));
     if (&x == &r_ && r_squares_ready_) {
       const double* ready[1] = {ctx_.Partial(kResidualPartial, n_)};
       TreeSums(ctx_, ready, 1, n_, 0);
@@ -655,6 +703,56 @@ class Solver final : public SolverBase {
     double out;
     FetchScalars(ctx_, 0, 1, &out);
     return out;
+  }
+
+  // ---- the reference's summation order (opt_.summation == 1) --------------
+  bool ReferenceOrder() const { return opt_.summation == 1; }
+
+  // InitializeBatches (methods_common.cpp:78-103): batch i holds columns
+  // [n i / count, n (i + 1) / count) with count = min(n, num_threads).
+  void InitReferenceBatches() {
+    const int64_t count = std::min<int64_t>(n_, std::max<int64_t>(1, opt_.num_threads));
+    batch_first_.assign(static_cast<size_t>(count + 1), 0);
+    for (int64_t i = 0; i <= count; ++i) batch_first_[i] = n_ * i / count;
+    std::vector<int32_t> batch_of(static_cast<size_t>(n_));
+    for (int64_t b = 0; b < count; ++b) {
+      for (int64_t j = batch_first_[b]; j < batch_first_[b + 1]; ++j) batch_of[j] = static_cast<int32_t>(b);
+    }
+    batch_first_dev_.Reserve(static_cast<size_t>(count + 1), ctx_.stream);
+    batch_of_dev_.Reserve(static_cast<size_t>(n_), ctx_.stream);
+    batch_sums_.Reserve(static_cast<size_t>(count), ctx_.stream);
+    SPAI_CUDA(cudaMemcpyAsync(batch_first_dev_.data(), batch_first_.data(), sizeof(int64_t) * (count + 1),
+                              cudaMemcpyHostToDevice, ctx_.stream));
+    SPAI_CUDA(cudaMemcpyAsync(batch_of_dev_.data(), batch_of.data(), sizeof(int32_t) * n_, cudaMemcpyHostToDevice,
+                              ctx_.stream));
+    ctx_.Sync();
+  }
+
+  // Per-batch sums of squares of x (y null) or of the products x * y on the
+  // common pattern, each sequential through its batch.
+  std::vector<double> BatchSums(const DevCsc<T>* x, const DevCsc<T>* y) {
+    const int64_t count = static_cast<int64_t>(batch_first_.size()) - 1;
+    const int grid = GridFor(count, 64);
+    if (y == nullptr) {
+      BatchSquaresKernel<T><<<grid, 64, 0, ctx_.stream>>>(View(*x), batch_first_dev_.data(), count,
+                                                          batch_sums_.data());
+    } else {
+      BatchDotsKernel<T><<<grid, 64, 0, ctx_.stream>>>(View(*x), View(*y), batch_first_dev_.data(), count,
+                                                       batch_sums_.data());
+    }
+    SPAI_LAUNCH_CHECK();
+    std::vector<double> out(static_cast<size_t>(count));
+    SPAI_CUDA(cudaMemcpyAsync(out.data(), batch_sums_.data(), sizeof(double) * count, cudaMemcpyDeviceToHost,
+                              ctx_.stream));
+    ctx_.Sync();
+    return out;
+  }
+
+  // the batches' partial sums added in batch order (the reference's reduction over batches)
+  static double BatchTotal(const std::vector<double>& partial) {
+    double total = 0.0;
+    for (const double v : partial) total += v;
+    return total;
   }
 
   // ---- sparse updates (sparse_operations.cpp:22-49) ------------------------
@@ -716,8 +814,23 @@ class Solver final : public SolverBase {
   bool DropForMatrixType(DevCsc<T>& x) {
     if (!opt_.dropping) return false;
     const int64_t original = x.nnz;
-    const double limit = std::sqrt(SquaredNorm(x)) * kEpsilon;
-    PruneAbsAtMost(ctx_, x, limit);
+    if (ReferenceOrder()) {
+      // the reference prunes a direction per column batch, against that batch's norm (dropping.cpp:177-190)
+      const std::vector<double> squares = BatchSums(&x, nullptr);
+      std::vector<double> limit(squares.size());
+      for (size_t b = 0; b < squares.size(); ++b) limit[b] = std::sqrt(squares[b]) * kEpsilon;
+      batch_limit_.Reserve(limit.size(), ctx_.stream);
+      SPAI_CUDA(cudaMemcpyAsync(batch_limit_.data(), limit.data(), sizeof(double) * limit.size(),
+                                cudaMemcpyHostToDevice, ctx_.stream));
+      double* column_limit = ColVec(1);
+      BroadcastBlocksKernel<<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(batch_of_dev_.data(), batch_limit_.data(),
+                                                                      n_, column_limit);
+      SPAI_LAUNCH_CHECK();
+      PruneAbsAtMostPerColumn(ctx_, x, column_limit);
+    } else {
+      const double limit = std::sqrt(SquaredNorm(x)) * kEpsilon;
+      PruneAbsAtMost(ctx_, x, limit);
+    }
     if (opt_.topk > 0) {
       KeepTopKPerColumn(ctx_, x, opt_.topk, false);
       return x.nnz != original;
@@ -801,7 +914,7 @@ class Solver final : public SolverBase {
 
   // num = <Z, Pr A Z>, den = ||Pr A Z||^2 (minimal_residual.cpp:44-52,78-88)
   void MrProjection(double& num, double& den) {
-    if (pr_diagonal_) {
+    if (pr_diagonal_ && !ReferenceOrder()) {
       double* tt = ctx_.Partial(0, n_);
       double* bt = ctx_.Partial(1, n_);
       SpgemmExtras extras = AExtras();
@@ -851,22 +964,33 @@ class Solver final : public SolverBase {
       MulA(p_, ap_);
       MulA(z_, az_);
       MulPr(az_, tmp_);
-      double* parts_buf[5];
-      for (int k = 0; k < 5; ++k) parts_buf[k] = ctx_.Partial(k, n_);
-      ColumnDots(ctx_, View(az_), View(tmp_), parts_buf[0]);
-      ColumnDots(ctx_, View(z_), View(az_), parts_buf[1]);
-      int arrays = 2;
-      if (i > 1) {
-        MulPr(ap_, tmp_);
-        ColumnDots(ctx_, View(ap_), View(tmp_), parts_buf[2]);
-        ColumnDots(ctx_, View(az_), View(tmp_), parts_buf[3]);
-        ColumnDots(ctx_, View(z_), View(ap_), parts_buf[4]);
-        arrays = 5;
-      }
-      const double* parts[5] = {parts_buf[0], parts_buf[1], parts_buf[2], parts_buf[3], parts_buf[4]};
-      TreeSums(ctx_, parts, arrays, n_, 0);
       double s[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-      FetchScalars(ctx_, 0, arrays, s);
+      if (ReferenceOrder()) {
+        s[0] = Dot(az_, tmp_);
+        s[1] = Dot(z_, az_);
+        if (i > 1) {
+          MulPr(ap_, tmp_);
+          s[2] = Dot(ap_, tmp_);
+          s[3] = Dot(az_, tmp_);
+          s[4] = Dot(z_, ap_);
+        }
+      } else {
+        double* parts_buf[5];
+        for (int k = 0; k < 5; ++k) parts_buf[k] = ctx_.Partial(k, n_);
+        ColumnDots(ctx_, View(az_), View(tmp_), parts_buf[0]);
+        ColumnDots(ctx_, View(z_), View(az_), parts_buf[1]);
+        int arrays = 2;
+        if (i > 1) {
+          MulPr(ap_, tmp_);
+          ColumnDots(ctx_, View(ap_), View(tmp_), parts_buf[2]);
+          ColumnDots(ctx_, View(az_), View(tmp_), parts_buf[3]);
+          ColumnDots(ctx_, View(z_), View(ap_), parts_buf[4]);
+          arrays = 5;
+        }
+        const double* parts[5] = {parts_buf[0], parts_buf[1], parts_buf[2], parts_buf[3], parts_buf[4]};
+        TreeSums(ctx_, parts, arrays, n_, 0);
+        FetchScalars(ctx_, 0, arrays, s);
+      }
       const double az_praz = s[0];
       const double z_az = s[1];
       const double ap_prap = s[2];
@@ -1001,6 +1125,11 @@ class Solver final : public SolverBase {
   bool r_squares_ready_ = false;  // Partial(kResidualPartial) holds R's column squares
   bool z_fused_ready_ = false;
   static constexpr int kResidualPartial = 7;
+  std::vector<int64_t> batch_first_;  // reference order: first column of every batch, then n
+  DevBuf<int64_t> batch_first_dev_;
+  DevBuf<int32_t> batch_of_dev_;      // batch of every column
+  DevBuf<double> batch_sums_;
+  DevBuf<double> batch_limit_;
   std::vector<SingleIterationData> history_;
   double initial_residual_ = 0.0;
   int64_t iterations_ = 0;

@@ -46,6 +46,13 @@ struct SolveOptions {
   int64_t inner_iterations = 2;
   int64_t topk = 0;       // 0: reference global budget; K > 0: per-column top-K by magnitude
   int precision = 0;      // 0: FP64 storage, 1: FP32 storage with FP64 reductions
+  // 0: the device order -- sequential inside a column, then the fixed
+  // 4096-wide tree across columns.  1: the reference's order -- columns in
+  // min(n, num_threads) batches (methods_common.cpp:78-103,135-136), each
+  // global sum sequential through a batch's columns in storage order, then
+  // over the batches -- which reproduces the reference's recorded histories.
+  int summation = 0;
+  int64_t num_threads = 1;
 };
 
 struct SolveOutput {

@@ -9,8 +9,10 @@ methods.pyx:182-258) on top of libspai_b200.so.
 Same arguments, defaults, conversions (scipy -> canonical int64 CSC, methods.pyx:74-98)
 and error behaviour (RuntimeError with the library's message, methods.pyx:128-130)
 as the reference.  Extra keyword arguments select the device-only forms:
-precision ("fp64" | "mixed"), topk_per_column (0 = the reference's global budget)
-and device (CUDA ordinal, -1 = current).
+precision ("fp64" | "mixed"), topk_per_column (0 = the reference's global budget),
+device (CUDA ordinal, -1 = current) and summation ("device" | "reference": the
+reference's num_threads column batches and summation order, which reproduces
+its recorded results bit for bit in FP64).
 """
 from __future__ import annotations
 
@@ -29,6 +31,9 @@ HISTORY_DTYPE = np.dtype([
 ])
 
 PRECISIONS = {"fp64": 0, "mixed": 1}
+# "device": per-column sums and the fixed tree; "reference": the reference's
+# num_threads column batches, summed in its order (its recorded results, bit for bit)
+SUMMATIONS = {"device": 0, "reference": 1}
 
 
 class OutputResult:
@@ -105,14 +110,17 @@ def method_params(A_csc, M0, Pr, max_iterations, tolerance, max_density, enable_
                              1 if M0 is not None else 0, 1 if Pr is not None else 0, inner_iterations)
 
 
-def ext_params(precision="fp64", topk_per_column=0, device=-1) -> _lib.SpaiExtParams:
+def ext_params(precision="fp64", topk_per_column=0, device=-1, summation="device") -> _lib.SpaiExtParams:
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
-    return _lib.SpaiExtParams(PRECISIONS[precision], int(topk_per_column), int(device), 0)
+    if summation not in SUMMATIONS:
+        raise ValueError(f"summation must be one of {sorted(SUMMATIONS)}")
+    return _lib.SpaiExtParams(PRECISIONS[precision], int(topk_per_column), int(device), SUMMATIONS[summation])
 
 
 def _call_method(family, name, A, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
-                 inner_iterations=2, precision="fp64", topk_per_column=0, device=-1) -> OutputResult:
+                 inner_iterations=2, precision="fp64", topk_per_column=0, device=-1,
+                 summation="device") -> OutputResult:
     """methods.pyx:147-179 plus the extension knobs."""
     lib = _lib.load()
     A_csc = as_csc(A)
@@ -121,13 +129,13 @@ def _call_method(family, name, A, M0, Pr, max_iterations, tolerance, max_density
     params = method_params(A_csc, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
                            inner_iterations)
     method_id = _lib.METHOD_IDS[(family, name)]
-    if precision == "fp64" and not topk_per_column and device == -1:
+    if precision == "fp64" and not topk_per_column and device == -1 and summation == "device":
         # the reference's own entry points (methods_c_api.h:48-56)
         entry = {0: lib.spai_global_cg, 1: lib.spai_global_mr, 2: lib.spai_global_lomr,
                  3: lib.inner_outer_mr, 4: lib.inner_outer_lomr}[method_id]
         result = entry(matrix_data(A_csc), matrix_data(M0_csc), matrix_data(Pr_csc), params)
     else:
-        ext = ext_params(precision, topk_per_column, device)
+        ext = ext_params(precision, topk_per_column, device, summation)
         result = lib.spai_run_ex(method_id, matrix_data(A_csc), matrix_data(M0_csc), matrix_data(Pr_csc), params,
                                  ctypes.byref(ext))
     return result_to_python(result)
