@@ -433,9 +433,11 @@ def e2e(args, A, M0, b):
         r = global_spai.mr(A_csc, M0=M0_csc, max_iterations=args.spai_iterations, tolerance=1e-12,
                            max_density=float(args.topk) / n, precision="mixed", topk_per_column=args.topk)
         t1 = time.perf_counter()
-        M_csr = sparse.csr_matrix(r.M)
-        hist, status = backward_error.pcg(a_arrays[0], a_arrays[1], a_arrays[2], M_csr.data, M_csr.indices,
-                                          M_csr.indptr, b_pinned, args.pcg_max_iterations, 1, args.pcg_tolerance,
+        # M's CSC arrays read as CSR are M^T, whose symmetric part (M^T + M)/2 is the
+        # preconditioner asked for: the same entries, the same bits, no host transpose
+        M_csc = r.M
+        hist, status = backward_error.pcg(a_arrays[0], a_arrays[1], a_arrays[2], M_csc.data, M_csc.indices,
+                                          M_csc.indptr, b_pinned, args.pcg_max_iterations, 1, args.pcg_tolerance,
                                           refresh_period=args.pcg_refresh, m_precision="mixed", symmetric_part=True)
         t2 = time.perf_counter()
         if rep == 0:
@@ -444,7 +446,7 @@ def e2e(args, A, M0, b):
         times_pcg.append(t2 - t1)
         h2d = (A_csc.indptr.nbytes + A_csc.indices.nbytes + A_csc.data.nbytes + M0_csc.indptr.nbytes
                + M0_csc.indices.nbytes + M0_csc.data.nbytes + sum(x.nbytes for x in a_arrays)
-               + M_csr.data.nbytes + M_csr.indices.nbytes + M_csr.indptr.nbytes + b_pinned.nbytes)
+               + M_csc.data.nbytes + 8 * M_csc.indices.size + 8 * M_csc.indptr.size + b_pinned.nbytes)
         d2h = (r.M.indptr.nbytes + r.M.indices.nbytes + r.M.data.nbytes + r.history.nbytes
                + 8 * args.pcg_max_iterations)
     spai_s = statistics.median(times_spai)

@@ -72,6 +72,12 @@ typedef struct SpaiExtParams {
                               FP64 runs then reproduce the reference's own results bit for bit */
 } SpaiExtParams;
 
+/* Release one array of a Result (col_offsets / row_indices: int64; values:
+ * double) on its own, for callers that keep the arrays beyond the Result
+ * (set the Result's field to NULL before free_mem). */
+void spai_free_int64_array(int64_t* array);
+void spai_free_double_array(double* array);
+
 /* Method ids for spai_run_ex / sessions. */
 enum {
   SPAI_GLOBAL_CG = 0,

@@ -82,7 +82,7 @@ EXPORTED_SYMBOLS = (
     "spai_session_result", "spai_session_set_rhs", "spai_session_pcg", "spai_session_destroy",
     "spai_kernel_launches", "spai_session_stream", "spai_profile_enable", "spai_profile_reset",
     "spai_profile_read", "spai_pcg_device_noalloc", "spai_residual_adjoint", "spai_pcg_adjoint",
-    "spai_mr_batched", "spai_mtx_read", "spai_mtx_write",
+    "spai_mr_batched", "spai_mtx_read", "spai_mtx_write", "spai_free_int64_array", "spai_free_double_array",
 )
 
 _lib = None
@@ -135,6 +135,10 @@ def _declare(lib) -> None:
                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                             ctypes.c_void_p, _i64, _f64, _i64, ctypes.c_void_p, _pf64, _pi64,
                                             ctypes.c_char_p, _i64]
+    lib.spai_free_int64_array.restype = None
+    lib.spai_free_int64_array.argtypes = [ctypes.c_void_p]
+    lib.spai_free_double_array.restype = None
+    lib.spai_free_double_array.argtypes = [ctypes.c_void_p]
     lib.spai_mtx_read.restype = Result
     lib.spai_mtx_read.argtypes = [ctypes.c_char_p, _i64]
     lib.spai_mtx_write.restype = _i64

@@ -76,6 +76,31 @@ Result SuccessResult(const SolveOutput& s) {
   return out;
 }
 
+// The same Result, filled from the device without an intermediate host copy.
+Result SolverResult(SolverBase& solver) {
+  const std::vector<SingleIterationData>& history = solver.history();
+  const int64_t n = solver.n();
+  const int64_t nnz = solver.m_nnz();
+  std::unique_ptr<int64_t[]> ptr(new int64_t[n + 1]);
+  std::unique_ptr<int64_t[]> idx(new int64_t[nnz]);
+  std::unique_ptr<double[]> val(new double[nnz]);
+  std::unique_ptr<SingleIterationData[]> hist(new SingleIterationData[history.size()]);
+  solver.DownloadM(ptr.get(), idx.get(), val.get());
+  for (size_t i = 0; i < history.size(); ++i) hist[i] = history[i];
+  Result out{};
+  out.rows = n;
+  out.cols = n;
+  out.nnz = nnz;
+  out.iterations = solver.iterations();
+  out.converged = solver.converged() ? 1 : 0;
+  out.history_size = static_cast<int64_t>(history.size());
+  out.col_offsets = ptr.release();
+  out.row_indices = idx.release();
+  out.values = val.release();
+  out.history = hist.release();
+  return out;
+}
+
 int ResolveDevice(int64_t requested) {
   int count = 0;
   const cudaError_t err = cudaGetDeviceCount(&count);
@@ -148,9 +173,7 @@ Result RunMethod(int64_t method, MatrixData A, MatrixData M0, MatrixData Pr, Met
     auto solver = MakeSolver(guard.ctx, opt);
     solver->Upload(in.a, in.has_m0 ? &in.m0 : nullptr, in.has_pr ? &in.pr : nullptr);
     solver->Run();
-    SolveOutput out;
-    solver->Download(out);
-    return SuccessResult(out);
+    return SolverResult(*solver);
   } catch (const std::exception& ex) {
     return ErrorResult(ex.what());
   } catch (...) {
@@ -158,7 +181,22 @@ Result RunMethod(int64_t method, MatrixData A, MatrixData M0, MatrixData Pr, Met
   }
 }
 
+// dst[i] = src[i] as int32; *bad = 1 when an index is outside [0, limit).
+__global__ void NarrowCheckedKernel(const int64_t* __restrict__ src, int32_t* __restrict__ dst, int64_t n,
+                                    int64_t limit, int32_t* __restrict__ bad) {
+  bool out_of_range = false;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t v = src[i];
+    out_of_range |= v < 0 || v >= limit;
+    dst[i] = static_cast<int32_t>(v);
+  }
+  if (__any_sync(0xffffffffu, out_of_range) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+}
+
 // Host CSR (int64) -> device row-compressed DevCsc (rows as major dimension).
+// The offsets are checked on the host; the column indices go up as int64 and
+// are narrowed and range-checked on the device.
 template <class T>
 void UploadCsr(Ctx& ctx, int64_t n, const double* values, const int64_t* indices, const int64_t* offsets,
                DevCsc<T>& out) {
@@ -167,16 +205,18 @@ void UploadCsr(Ctx& ctx, int64_t n, const double* values, const int64_t* indices
     if (offsets[i] > offsets[i + 1]) throw std::invalid_argument("CSR offsets must be non-decreasing");
   }
   const int64_t nnz = offsets[n];
-  std::vector<int32_t> idx(nnz);
-  for (int64_t k = 0; k < nnz; ++k) {
-    if (indices[k] < 0 || indices[k] >= n) throw std::invalid_argument("CSR column index out of range");
-    idx[k] = static_cast<int32_t>(indices[k]);
-  }
   out.Shape(n, n, ctx.stream);
   out.ReserveNnz(nnz, ctx.stream);
   SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), offsets, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, ctx.stream));
   if (nnz > 0) {
-    SPAI_CUDA(cudaMemcpyAsync(out.idx.data(), idx.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx.stream));
+    DevBuf<int64_t> wide;
+    wide.Reserve(static_cast<size_t>(nnz), ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(wide.data(), indices, sizeof(int64_t) * nnz, cudaMemcpyHostToDevice, ctx.stream));
+    int32_t* bad = ctx.flags.data() + 3;
+    SPAI_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx.stream));
+    NarrowCheckedKernel<<<GridFor(nnz, 256), 256, 0, ctx.stream>>>(wide.data(), out.idx.data(), nnz, n, bad);
+    SPAI_LAUNCH_CHECK();
+    SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 3, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
     if constexpr (sizeof(T) == sizeof(double)) {
       SPAI_CUDA(cudaMemcpyAsync(out.val.data(), values, sizeof(double) * nnz, cudaMemcpyHostToDevice, ctx.stream));
     } else {
@@ -186,6 +226,8 @@ void UploadCsr(Ctx& ctx, int64_t n, const double* values, const int64_t* indices
       ConvertValues<double, T>(ctx, stage.data(), out.val.data(), nnz);
       ctx.Sync();
     }
+    ctx.Sync();
+    if (ctx.host_flags[3] != 0) throw std::invalid_argument("CSR column index out of range");
   }
   ctx.Sync();
 }
@@ -316,6 +358,10 @@ void free_mem(Result* result) {
   result->history = nullptr;
   result->error_message = nullptr;
 }
+
+void spai_free_int64_array(int64_t* array) { delete[] array; }
+
+void spai_free_double_array(double* array) { delete[] array; }
 
 Result spai_run_ex(int64_t method, MatrixData A, MatrixData M0, MatrixData Pr, MethodParams params,
                    const SpaiExtParams* ext) {
@@ -582,10 +628,9 @@ int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* con
 int64_t spai_session_history(SpaiSession* session, SingleIterationData* out, int64_t capacity) {
   if (session == nullptr) return 0;
   try {
-    spai::SolveOutput full;
-    session->solver->Download(full);
-    const int64_t count = static_cast<int64_t>(full.history.size());
-    for (int64_t i = 0; i < count && i < capacity; ++i) out[i] = full.history[i];
+    const std::vector<SingleIterationData>& history = session->solver->history();
+    const int64_t count = static_cast<int64_t>(history.size());
+    for (int64_t i = 0; i < count && i < capacity; ++i) out[i] = history[i];
     return count;
   } catch (...) {
     return 0;
@@ -595,9 +640,7 @@ int64_t spai_session_history(SpaiSession* session, SingleIterationData* out, int
 Result spai_session_result(SpaiSession* session) {
   try {
     if (session == nullptr) throw std::invalid_argument("null session");
-    spai::SolveOutput out;
-    session->solver->Download(out);
-    return spai::SuccessResult(out);
+    return spai::SolverResult(*session->solver);
   } catch (const std::exception& ex) {
     return spai::ErrorResult(ex.what());
   }

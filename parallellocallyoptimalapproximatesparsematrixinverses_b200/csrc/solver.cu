@@ -302,33 +302,37 @@ class Solver final : public SolverBase {
     out.ptr.resize(m_.cols + 1);
     out.idx.resize(m_.nnz);
     out.val.resize(m_.nnz);
-    SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), m_.ptr.data(), sizeof(int64_t) * (m_.cols + 1), cudaMemcpyDeviceToHost,
+    DownloadM(out.ptr.data(), out.idx.data(), out.val.data());
+    out.history = history_;
+    out.iterations = iterations_;
+    out.converged = converged_;
+  }
+
+  void DownloadM(int64_t* ptr, int64_t* idx, double* val) override {
+    SPAI_CUDA(cudaMemcpyAsync(ptr, m_.ptr.data(), sizeof(int64_t) * (m_.cols + 1), cudaMemcpyDeviceToHost,
                               ctx_.stream));
     if (m_.nnz > 0) {
       DevBuf<int64_t> wide;
       wide.Reserve(static_cast<size_t>(m_.nnz), ctx_.stream);
       WidenIndexKernel<<<GridFor(m_.nnz, 256), 256, 0, ctx_.stream>>>(m_.idx.data(), wide.data(), m_.nnz);
       SPAI_LAUNCH_CHECK();
-      SPAI_CUDA(cudaMemcpyAsync(out.idx.data(), wide.data(), sizeof(int64_t) * m_.nnz, cudaMemcpyDeviceToHost,
-                                ctx_.stream));
+      SPAI_CUDA(cudaMemcpyAsync(idx, wide.data(), sizeof(int64_t) * m_.nnz, cudaMemcpyDeviceToHost, ctx_.stream));
       if constexpr (std::is_same<T, double>::value) {
-        SPAI_CUDA(cudaMemcpyAsync(out.val.data(), m_.val.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost,
-                                  ctx_.stream));
+        SPAI_CUDA(cudaMemcpyAsync(val, m_.val.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost, ctx_.stream));
         ctx_.Sync();
       } else {
         DevBuf<double> widev;
         widev.Reserve(static_cast<size_t>(m_.nnz), ctx_.stream);
         ConvertValues<T, double>(ctx_, m_.val.data(), widev.data(), m_.nnz);
-        SPAI_CUDA(cudaMemcpyAsync(out.val.data(), widev.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost,
-                                  ctx_.stream));
+        SPAI_CUDA(cudaMemcpyAsync(val, widev.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost, ctx_.stream));
         ctx_.Sync();
       }
     }
     ctx_.Sync();
-    out.history = history_;
-    out.iterations = iterations_;
-    out.converged = converged_;
   }
+
+  const std::vector<SingleIterationData>& history() const override { return history_; }
+  bool converged() const override { return converged_; }
 
   // Batched Global MR: the loop of RunMr (minimal_residual.cpp:31-93) per
   // diagonal block.  Every block follows the single-system arithmetic bit for

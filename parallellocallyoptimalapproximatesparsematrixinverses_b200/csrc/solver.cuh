@@ -81,6 +81,10 @@ class SolverBase {
   virtual void Run() = 0;
   // Copies M (as FP64, int64 indices) and the history to the host.
   virtual void Download(SolveOutput& out) = 0;
+  // Copies M straight into host arrays of n() + 1 (ptr) and m_nnz() (idx, val) entries.
+  virtual void DownloadM(int64_t* ptr, int64_t* idx, double* val) = 0;
+  virtual const std::vector<SingleIterationData>& history() const = 0;
+  virtual bool converged() const = 0;
   virtual int64_t iterations() const = 0;
   virtual int64_t m_nnz() const = 0;
   // Device CSR copy of the current M (rows as major), values widened to FP64

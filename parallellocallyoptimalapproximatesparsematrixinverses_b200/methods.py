@@ -84,20 +84,46 @@ def history_array(rows, count) -> np.ndarray:
     return history
 
 
+class _LibraryArray:
+    """Owner of one array of a Result: numpy views of it keep this object
+    alive, and the last one to go releases the array through the library."""
+
+    def __init__(self, address, count, typestr, release):
+        self.address = address
+        self._release = release
+        self.__array_interface__ = {"data": (address, False), "shape": (count,), "typestr": typestr, "version": 3}
+
+    def __del__(self):
+        try:
+            self._release(self.address)
+        except Exception:  # interpreter shutdown: the process frees the memory
+            pass
+
+
+def adopt_matrix(result: _lib.Result) -> sparse.csc_matrix:
+    """M of a successful Result as a scipy CSC matrix whose arrays are the
+    library's own (no copy); clears the Result's matrix fields, so that
+    free_mem releases only the rest."""
+    lib = _lib.load()
+    arrays = []
+    for field, typestr, count, release in (("col_offsets", "<i8", result.cols + 1, lib.spai_free_int64_array),
+                                           ("row_indices", "<i8", result.nnz, lib.spai_free_int64_array),
+                                           ("values", "<f8", result.nnz, lib.spai_free_double_array)):
+        address = ctypes.cast(getattr(result, field), ctypes.c_void_p).value
+        setattr(result, field, None)
+        arrays.append(np.asarray(_LibraryArray(address, count, typestr, release)))
+    indptr, indices, values = arrays
+    return sparse.csc_matrix((values, indices, indptr), shape=(result.rows, result.cols))
+
+
 def result_to_python(result: _lib.Result) -> OutputResult:
-    """Copies a Result into numpy/scipy and always frees it (methods.pyx:119-144)."""
+    """Turns a Result into numpy/scipy and always frees it (methods.pyx:119-144);
+    M keeps the library's arrays instead of copying them."""
     lib = _lib.load()
     try:
         if result.error_message:
             raise RuntimeError(result.error_message.decode("utf-8", "replace"))
-        indptr = np.ctypeslib.as_array(result.col_offsets, shape=(result.cols + 1,)).copy()
-        if result.nnz:
-            indices = np.ctypeslib.as_array(result.row_indices, shape=(result.nnz,)).copy()
-            values = np.ctypeslib.as_array(result.values, shape=(result.nnz,)).copy()
-        else:
-            indices = np.empty(0, dtype=np.int64)
-            values = np.empty(0, dtype=np.float64)
-        M = sparse.csc_matrix((values, indices, indptr), shape=(result.rows, result.cols))
+        M = adopt_matrix(result)
         history = history_array(result.history, result.history_size)
         return OutputResult(M, result.iterations, bool(result.converged), history)
     finally:

@@ -21,7 +21,7 @@ import numpy as np
 from scipy import sparse
 
 from . import _lib
-from .methods import as_csc, matrix_data
+from .methods import adopt_matrix, as_csc, matrix_data
 
 
 def load_matrix(path, threads: int = 0) -> sparse.csc_matrix:
@@ -31,14 +31,7 @@ def load_matrix(path, threads: int = 0) -> sparse.csc_matrix:
     try:
         if result.error_message:
             raise RuntimeError(result.error_message.decode("utf-8", "replace"))
-        indptr = np.ctypeslib.as_array(result.col_offsets, shape=(result.cols + 1,)).copy()
-        if result.nnz:
-            indices = np.ctypeslib.as_array(result.row_indices, shape=(result.nnz,)).copy()
-            values = np.ctypeslib.as_array(result.values, shape=(result.nnz,)).copy()
-        else:
-            indices = np.empty(0, np.int64)
-            values = np.empty(0, np.float64)
-        m = sparse.csc_matrix((values, indices, indptr), shape=(result.rows, result.cols))
+        m = adopt_matrix(result)
         m.has_sorted_indices = True
         return m
     finally:

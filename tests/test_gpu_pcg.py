@@ -46,3 +46,34 @@ def test_matvec_matches_scipy(require_gpu):
     x = np.random.default_rng(3).standard_normal(A.shape[0])
     y = backward_error.matvec(A.data, A.indices, A.indptr, x, 1)
     assert np.allclose(y, A @ x, rtol=1e-14, atol=1e-14)
+
+
+def test_pcg_symmetric_part_of_the_transpose_is_the_same(require_gpu):
+    # CSC arrays of M read as CSR are M^T; with symmetric_part the preconditioner
+    # (M + M^T)/2 is the same either way, bit for bit
+    A = _csr(problems.diffusion_2d(20, 1.0, 8))
+    rng = np.random.default_rng(4)
+    M = sparse.csr_matrix(problems.diagonal_inverse(A) + 0.01 * sparse.random(A.shape[0], A.shape[0], 0.01,
+                                                                               random_state=rng))
+    M.sort_indices()
+    Mc = sparse.csc_matrix(M)
+    Mc.sort_indices()
+    b, _ = problems.solution_rhs(A, seed=2)
+    h1, s1 = backward_error.pcg(A.data, A.indices, A.indptr, M.data, M.indices, M.indptr, b, 500, 1, 1e-8,
+                                symmetric_part=True)
+    h2, s2 = backward_error.pcg(A.data, A.indices, A.indptr, Mc.data, Mc.indices, Mc.indptr, b, 500, 1, 1e-8,
+                                symmetric_part=True)
+    assert s1 == s2 and np.array_equal(h1.view(np.int64), h2.view(np.int64))
+
+
+def test_pcg_rejects_an_out_of_range_column(require_gpu):
+    A = _csr(problems.laplacian_2d(6))
+    M = _csr(problems.diagonal_inverse(A))
+    bad = A.indices.astype(np.int64)
+    bad[7] = A.shape[0] + 2
+    with pytest.raises(RuntimeError, match="CSR column index out of range"):
+        backward_error.pcg(A.data, bad, A.indptr, M.data, M.indices, M.indptr, np.ones(A.shape[0]), 50, 1, 1e-8)
+    # the library stays usable
+    hist, status = backward_error.pcg(A.data, A.indices, A.indptr, M.data, M.indices, M.indptr,
+                                      np.ones(A.shape[0]), 50, 1, 1e-8)
+    assert status == 1
