@@ -40,11 +40,15 @@ void CountLaunch();
 // is handed to the next allocation on s that fits it (at least the request,
 // at most twice it): stream order makes the reuse safe without events, and
 // the iteration loop, whose buffers recur at similar sizes every step, stops
-// calling the allocator.  CacheFlush frees a stream's blocks (before the
+// calling the allocator.  CacheFlush frees a stream's blocks; CacheRetire
+// hands them to the next calls on the same device instead (both before the
 // stream is destroyed).
 void* CacheTake(cudaStream_t stream, size_t bytes, size_t* capacity_bytes);
 void CacheGive(cudaStream_t stream, void* block, size_t bytes);
 void CacheFlush(cudaStream_t stream);
+// After `stream` has been synchronised: its blocks join a pool of idle blocks
+// of `device` that later streams on the device take from before allocating.
+void CacheRetire(cudaStream_t stream, int device);
 
 #define SPAI_LAUNCH_CHECK()          \
   do {                               \

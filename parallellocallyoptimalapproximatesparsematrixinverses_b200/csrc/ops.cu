@@ -984,25 +984,45 @@ struct CachedBlock {
   size_t bytes;
 };
 constexpr size_t kCacheBlocksPerStream = 64;
+constexpr size_t kRetiredBlocksPerDevice = 128;
 std::mutex g_cache_mutex;
 std::map<cudaStream_t, std::vector<CachedBlock>> g_block_cache;
-}  // namespace
+// Blocks of finished contexts (their streams synchronised, so idle), per
+// device: any later context on the device takes them before the allocator.
+std::map<int, std::vector<CachedBlock>> g_retired;
 
-void* CacheTake(cudaStream_t stream, size_t bytes, size_t* capacity_bytes) {
-  std::lock_guard<std::mutex> lock(g_cache_mutex);
-  auto it = g_block_cache.find(stream);
-  if (it == g_block_cache.end()) return nullptr;
-  std::vector<CachedBlock>& blocks = it->second;
+// Index of the smallest block in `blocks` that holds `bytes` without wasting
+// more than half of itself, or blocks.size().
+size_t BestFit(const std::vector<CachedBlock>& blocks, size_t bytes) {
   size_t best = blocks.size();
   for (size_t i = 0; i < blocks.size(); ++i) {
     const size_t b = blocks[i].bytes;
     if (b >= bytes && b <= 2 * bytes + (size_t{1} << 20) && (best == blocks.size() || b < blocks[best].bytes)) best = i;
   }
-  if (best == blocks.size()) return nullptr;
-  void* p = blocks[best].ptr;
-  *capacity_bytes = blocks[best].bytes;
-  blocks.erase(blocks.begin() + static_cast<std::ptrdiff_t>(best));
+  return best;
+}
+
+void* TakeAt(std::vector<CachedBlock>& blocks, size_t at, size_t* capacity_bytes) {
+  void* p = blocks[at].ptr;
+  *capacity_bytes = blocks[at].bytes;
+  blocks.erase(blocks.begin() + static_cast<std::ptrdiff_t>(at));
   return p;
+}
+}  // namespace
+
+void* CacheTake(cudaStream_t stream, size_t bytes, size_t* capacity_bytes) {
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  auto it = g_block_cache.find(stream);
+  if (it != g_block_cache.end()) {
+    const size_t at = BestFit(it->second, bytes);
+    if (at < it->second.size()) return TakeAt(it->second, at, capacity_bytes);
+  }
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess) return nullptr;
+  auto retired = g_retired.find(device);
+  if (retired == g_retired.end()) return nullptr;
+  const size_t at = BestFit(retired->second, bytes);
+  return at < retired->second.size() ? TakeAt(retired->second, at, capacity_bytes) : nullptr;
 }
 
 void CacheGive(cudaStream_t stream, void* block, size_t bytes) {
@@ -1024,6 +1044,32 @@ void CacheFlush(cudaStream_t stream) {
   g_block_cache.erase(it);
 }
 
+void CacheRetire(cudaStream_t stream, int device) {
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  auto it = g_block_cache.find(stream);
+  if (it == g_block_cache.end()) return;
+  std::vector<CachedBlock>& retired = g_retired[device];
+  for (const CachedBlock& b : it->second) retired.push_back(b);
+  g_block_cache.erase(it);
+  // keep the newest blocks; the oldest go back to the pool (the stream is idle)
+  while (retired.size() > kRetiredBlocksPerDevice) {
+    cudaFreeAsync(retired.front().ptr, stream);
+    retired.erase(retired.begin());
+  }
+}
+
+namespace {
+// Pinned read-back slots of finished contexts, reused by the next ones
+// (cudaMallocHost is slow and cudaFreeHost synchronises the device).
+struct PinnedSlots {
+  double* scalars;
+  int64_t* counts;
+  int32_t* flags;
+};
+std::mutex g_pinned_mutex;
+std::vector<PinnedSlots> g_pinned;
+}  // namespace
+
 void Ctx::Init(int device_ordinal) {
   device = device_ordinal;
   SPAI_CUDA(cudaSetDevice(device));
@@ -1033,9 +1079,20 @@ void Ctx::Init(int device_ordinal) {
   SPAI_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
   uint64_t threshold = UINT64_MAX;
   SPAI_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
-  SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_scalars), sizeof(double) * kScalarSlots));
-  SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_counts), sizeof(int64_t) * 8));
-  SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_flags), sizeof(int32_t) * 8));
+  {
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    if (!g_pinned.empty()) {
+      host_scalars = g_pinned.back().scalars;
+      host_counts = g_pinned.back().counts;
+      host_flags = g_pinned.back().flags;
+      g_pinned.pop_back();
+    }
+  }
+  if (host_scalars == nullptr) {
+    SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_scalars), sizeof(double) * kScalarSlots));
+    SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_counts), sizeof(int64_t) * 8));
+    SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_flags), sizeof(int32_t) * 8));
+  }
   scalars.Reserve(kScalarSlots, stream);
   select_state.Reserve(4, stream);
   histogram.Reserve(256, stream);
@@ -1075,14 +1132,16 @@ void Ctx::Destroy() {
   pad_idx.Release();
   pad_val.Release();
   if (stream != nullptr) {
-    CacheFlush(stream);
+    // every block of the stream is idle after the synchronisation above
+    CacheRetire(stream, device);
     cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
     stream = nullptr;
   }
-  if (host_scalars != nullptr) cudaFreeHost(host_scalars);
-  if (host_counts != nullptr) cudaFreeHost(host_counts);
-  if (host_flags != nullptr) cudaFreeHost(host_flags);
+  if (host_scalars != nullptr) {
+    std::lock_guard<std::mutex> lock(g_pinned_mutex);
+    g_pinned.push_back(PinnedSlots{host_scalars, host_counts, host_flags});
+  }
   host_scalars = nullptr;
   host_counts = nullptr;
   host_flags = nullptr;
