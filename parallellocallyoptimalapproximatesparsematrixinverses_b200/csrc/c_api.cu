@@ -46,33 +46,22 @@ Result ErrorResult(const std::string& message) {
   return out;
 }
 
-// GetSuccessResult (methods_c_api.cpp:66-114): host arrays allocated with new[].
-Result SuccessResult(const SolveOutput& s) {
+// GetSuccessResult (methods_c_api.cpp:66-114): host arrays allocated with
+// new[]; M's arrays are taken over from the SolveOutput.
+Result SuccessResult(SolveOutput&& s) {
+  std::unique_ptr<SingleIterationData[]> hist(new SingleIterationData[s.history.size()]);
+  for (size_t i = 0; i < s.history.size(); ++i) hist[i] = s.history[i];
   Result out{};
   out.rows = s.rows;
   out.cols = s.cols;
-  out.nnz = static_cast<int64_t>(s.idx.size());
+  out.nnz = s.nnz;
   out.iterations = s.iterations;
   out.converged = s.converged ? 1 : 0;
   out.history_size = static_cast<int64_t>(s.history.size());
-  try {
-    out.col_offsets = new int64_t[s.cols + 1];
-    out.row_indices = new int64_t[out.nnz];
-    out.values = new double[out.nnz];
-    out.history = new SingleIterationData[s.history.size()];
-  } catch (...) {
-    delete[] out.col_offsets;
-    delete[] out.row_indices;
-    delete[] out.values;
-    delete[] out.history;
-    throw;
-  }
-  std::memcpy(out.col_offsets, s.ptr.data(), sizeof(int64_t) * (s.cols + 1));
-  if (out.nnz > 0) {
-    std::memcpy(out.row_indices, s.idx.data(), sizeof(int64_t) * out.nnz);
-    std::memcpy(out.values, s.val.data(), sizeof(double) * out.nnz);
-  }
-  for (size_t i = 0; i < s.history.size(); ++i) out.history[i] = s.history[i];
+  out.col_offsets = s.ptr.release();
+  out.row_indices = s.idx.release();
+  out.values = s.val.release();
+  out.history = hist.release();
   return out;
 }
 
@@ -473,7 +462,7 @@ int64_t spai_mr_batched(int64_t count, const MatrixData* A, const MatrixData* M0
     solver->Upload(big_a, params.use_initial_m != 0 ? &big_m : nullptr, nullptr);
     std::vector<spai::SolveOutput> outputs;
     solver->RunMrBatched(offsets, outputs);
-    for (int64_t b = 0; b < count; ++b) results[b] = spai::SuccessResult(outputs[b]);
+    for (int64_t b = 0; b < count; ++b) results[b] = spai::SuccessResult(std::move(outputs[b]));
     return 0;
   } catch (const std::exception& ex) {
     if (results != nullptr) {
@@ -614,9 +603,7 @@ int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* con
     session->solver->Run();
     if (iterations != nullptr) *iterations = session->solver->iterations();
     if (nnz_m != nullptr) *nnz_m = session->solver->m_nnz();
-    spai::SolveOutput out;
-    // only the history is needed here; M stays on the device
-    if (converged != nullptr) *converged = 0;
+    if (converged != nullptr) *converged = session->solver->converged() ? 1 : 0;
     session->history.clear();
     return 0;
   } catch (const std::exception& ex) {

@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <stdexcept>
+#include <thread>
 #include <limits>
 
 #include "device.cuh"
@@ -1069,6 +1070,71 @@ struct PinnedSlots {
 std::mutex g_pinned_mutex;
 std::vector<PinnedSlots> g_pinned;
 }  // namespace
+
+namespace {
+// Pinned staging buffers for downloads, reused across calls (pinning memory
+// is slow); each call takes one for its duration.
+constexpr size_t kStageBytes = size_t{32} << 20;
+std::mutex g_stage_mutex;
+std::vector<void*> g_stages;
+
+// f(first, last) over [0, n) in up to `parts` contiguous pieces, one thread each.
+template <class F>
+void HostParallel(int64_t n, int parts, F f) {
+  if (parts <= 1 || n < (int64_t{1} << 16)) {
+    f(int64_t{0}, n);
+    return;
+  }
+  std::vector<std::thread> pool;
+  for (int k = 0; k < parts; ++k) {
+    const int64_t first = n * k / parts;
+    const int64_t last = n * (k + 1) / parts;
+    pool.emplace_back(f, first, last);
+  }
+  for (auto& t : pool) t.join();
+}
+}  // namespace
+
+template <class T>
+void DownloadWiden(Ctx& ctx, const int32_t* idx_dev, const T* val_dev, int64_t n, int64_t index_offset,
+                   int64_t* idx_host, double* val_host) {
+  if (n <= 0) return;
+  void* stage = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_stage_mutex);
+    if (!g_stages.empty()) {
+      stage = g_stages.back();
+      g_stages.pop_back();
+    }
+  }
+  if (stage == nullptr) SPAI_CUDA(cudaMallocHost(&stage, kStageBytes));
+  struct Return {
+    void* p;
+    ~Return() {
+      std::lock_guard<std::mutex> lock(g_stage_mutex);
+      g_stages.push_back(p);
+    }
+  } give_back{stage};
+  const int64_t per_chunk = static_cast<int64_t>(kStageBytes / (sizeof(int32_t) + sizeof(T)));
+  int32_t* stage_idx = static_cast<int32_t*>(stage);
+  T* stage_val = reinterpret_cast<T*>(static_cast<unsigned char*>(stage) + sizeof(int32_t) * per_chunk);
+  const int threads = static_cast<int>(std::min(8u, std::max(1u, std::thread::hardware_concurrency())));
+  for (int64_t first = 0; first < n; first += per_chunk) {
+    const int64_t count = std::min(per_chunk, n - first);
+    SPAI_CUDA(cudaMemcpyAsync(stage_idx, idx_dev + first, sizeof(int32_t) * count, cudaMemcpyDeviceToHost, ctx.stream));
+    SPAI_CUDA(cudaMemcpyAsync(stage_val, val_dev + first, sizeof(T) * count, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.Sync();
+    HostParallel(count, threads, [&](int64_t a, int64_t b) {
+      for (int64_t i = a; i < b; ++i) {
+        idx_host[first + i] = static_cast<int64_t>(stage_idx[i]) - index_offset;
+        val_host[first + i] = static_cast<double>(stage_val[i]);
+      }
+    });
+  }
+}
+
+template void DownloadWiden<double>(Ctx&, const int32_t*, const double*, int64_t, int64_t, int64_t*, double*);
+template void DownloadWiden<float>(Ctx&, const int32_t*, const float*, int64_t, int64_t, int64_t*, double*);
 
 void Ctx::Init(int device_ordinal) {
   device = device_ordinal;

@@ -114,6 +114,14 @@ class SegmentTree {
   std::vector<double> host_;
 };
 
+// Host copies of a device index array (int32, minus index_offset, widened to
+// int64) and value array (T, widened to double), n entries each, through a
+// pinned staging buffer reused across calls and widened by several host
+// threads.  Synchronises the stream.
+template <class T>
+void DownloadWiden(Ctx& ctx, const int32_t* idx_dev, const T* val_dev, int64_t n, int64_t index_offset,
+                   int64_t* idx_host, double* val_host);
+
 // Per-column sequential partial sums (storage order, as Eigen within a column).
 template <class T>
 void ColumnSquares(Ctx& ctx, CscView<T> x, double* partial);

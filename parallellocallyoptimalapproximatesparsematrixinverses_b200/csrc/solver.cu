@@ -155,13 +155,6 @@ __global__ void NarrowIndexKernel(const int64_t* __restrict__ src, int32_t* __re
   }
 }
 
-__global__ void WidenIndexKernel(const int32_t* __restrict__ src, int64_t* __restrict__ dst, int64_t n) {
-  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    dst[i] = static_cast<int64_t>(src[i]);
-  }
-}
-
 }  // namespace
 
 template <class T>
@@ -297,12 +290,8 @@ class Solver final : public SolverBase {
   }
 
   void Download(SolveOutput& out) override {
-    out.rows = m_.rows;
-    out.cols = m_.cols;
-    out.ptr.resize(m_.cols + 1);
-    out.idx.resize(m_.nnz);
-    out.val.resize(m_.nnz);
-    DownloadM(out.ptr.data(), out.idx.data(), out.val.data());
+    out.Allocate(m_.rows, m_.cols, m_.nnz);
+    DownloadM(out.ptr.get(), out.idx.get(), out.val.get());
     out.history = history_;
     out.iterations = iterations_;
     out.converged = converged_;
@@ -311,23 +300,7 @@ class Solver final : public SolverBase {
   void DownloadM(int64_t* ptr, int64_t* idx, double* val) override {
     SPAI_CUDA(cudaMemcpyAsync(ptr, m_.ptr.data(), sizeof(int64_t) * (m_.cols + 1), cudaMemcpyDeviceToHost,
                               ctx_.stream));
-    if (m_.nnz > 0) {
-      DevBuf<int64_t> wide;
-      wide.Reserve(static_cast<size_t>(m_.nnz), ctx_.stream);
-      WidenIndexKernel<<<GridFor(m_.nnz, 256), 256, 0, ctx_.stream>>>(m_.idx.data(), wide.data(), m_.nnz);
-      SPAI_LAUNCH_CHECK();
-      SPAI_CUDA(cudaMemcpyAsync(idx, wide.data(), sizeof(int64_t) * m_.nnz, cudaMemcpyDeviceToHost, ctx_.stream));
-      if constexpr (std::is_same<T, double>::value) {
-        SPAI_CUDA(cudaMemcpyAsync(val, m_.val.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost, ctx_.stream));
-        ctx_.Sync();
-      } else {
-        DevBuf<double> widev;
-        widev.Reserve(static_cast<size_t>(m_.nnz), ctx_.stream);
-        ConvertValues<T, double>(ctx_, m_.val.data(), widev.data(), m_.nnz);
-        SPAI_CUDA(cudaMemcpyAsync(val, widev.data(), sizeof(double) * m_.nnz, cudaMemcpyDeviceToHost, ctx_.stream));
-        ctx_.Sync();
-      }
-    }
+    DownloadWiden<T>(ctx_, m_.idx.data(), m_.val.data(), m_.nnz, 0, idx, val);
     ctx_.Sync();
   }
 
@@ -366,7 +339,8 @@ class Solver final : public SolverBase {
                               cudaMemcpyHostToDevice, ctx_.stream));
     ctx_.Sync();
 
-    outputs.assign(static_cast<size_t>(blocks), SolveOutput());
+    outputs.clear();
+    outputs.resize(static_cast<size_t>(blocks));
     std::vector<char> active(static_cast<size_t>(blocks), 1);
     int64_t live = blocks;
     std::vector<double> sums(static_cast<size_t>(2 * blocks));
@@ -400,35 +374,18 @@ class Solver final : public SolverBase {
     auto snapshot = [&]() {
       if (stopping.empty()) return;
       fetch_counts();
-      std::vector<int32_t> idx;
-      std::vector<T> val;
       for (const int b : stopping) {
         SolveOutput& out = outputs[b];
         const int64_t c0 = offsets[b];
         const int64_t cols = offsets[b + 1] - c0;
         const int64_t p0 = m_at[b];
         const int64_t nnz = m_at[b + 1] - p0;
-        out.rows = cols;
-        out.cols = cols;
-        out.ptr.resize(static_cast<size_t>(cols + 1));
-        SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), m_.ptr.data() + c0, sizeof(int64_t) * (cols + 1),
+        out.Allocate(cols, cols, nnz);
+        SPAI_CUDA(cudaMemcpyAsync(out.ptr.get(), m_.ptr.data() + c0, sizeof(int64_t) * (cols + 1),
                                   cudaMemcpyDeviceToHost, ctx_.stream));
-        idx.resize(static_cast<size_t>(nnz));
-        val.resize(static_cast<size_t>(nnz));
-        if (nnz > 0) {
-          SPAI_CUDA(cudaMemcpyAsync(idx.data(), m_.idx.data() + p0, sizeof(int32_t) * nnz, cudaMemcpyDeviceToHost,
-                                    ctx_.stream));
-          SPAI_CUDA(cudaMemcpyAsync(val.data(), m_.val.data() + p0, sizeof(T) * nnz, cudaMemcpyDeviceToHost,
-                                    ctx_.stream));
-        }
+        DownloadWiden<T>(ctx_, m_.idx.data() + p0, m_.val.data() + p0, nnz, c0, out.idx.get(), out.val.get());
         ctx_.Sync();
         for (int64_t j = 0; j <= cols; ++j) out.ptr[j] -= p0;
-        out.idx.resize(static_cast<size_t>(nnz));
-        out.val.resize(static_cast<size_t>(nnz));
-        for (int64_t p = 0; p < nnz; ++p) {
-          out.idx[p] = static_cast<int64_t>(idx[p]) - c0;
-          out.val[p] = static_cast<double>(val[p]);
-        }
         active[b] = 0;
         --live;
       }

@@ -55,15 +55,27 @@ struct SolveOptions {
   int64_t num_threads = 1;
 };
 
+// M on the host in the arrays the C ABI hands out (new[], released by
+// free_mem), so a Result takes them over without a copy.
 struct SolveOutput {
   int64_t rows = 0;
   int64_t cols = 0;
-  std::vector<int64_t> ptr;
-  std::vector<int64_t> idx;
-  std::vector<double> val;
+  int64_t nnz = 0;
+  std::unique_ptr<int64_t[]> ptr;  // cols + 1
+  std::unique_ptr<int64_t[]> idx;  // nnz
+  std::unique_ptr<double[]> val;   // nnz
   std::vector<SingleIterationData> history;
   int64_t iterations = 0;
   bool converged = false;
+
+  void Allocate(int64_t r, int64_t c, int64_t count) {
+    rows = r;
+    cols = c;
+    nnz = count;
+    ptr.reset(new int64_t[c + 1]);
+    idx.reset(new int64_t[count]);
+    val.reset(new double[count]);
+  }
 };
 
 struct IterationTimes {
