@@ -204,7 +204,16 @@ class Solver final : public SolverBase {
     DevBuf<double> stage_val;
     UploadCsc(ctx_, a, a64_, stage_idx, stage_val);
     if constexpr (!std::is_same<T, double>::value) {
-      UploadCsc(ctx_, a, a_, stage_idx, stage_val);
+      // the FP32 copy from the FP64 one already in HBM (same rounding as from the host values)
+      a_.Shape(a64_.rows, a64_.cols, ctx_.stream);
+      a_.ReserveNnz(a64_.nnz, ctx_.stream);
+      SPAI_CUDA(cudaMemcpyAsync(a_.ptr.data(), a64_.ptr.data(), sizeof(int64_t) * (a64_.cols + 1),
+                                cudaMemcpyDeviceToDevice, ctx_.stream));
+      if (a64_.nnz > 0) {
+        SPAI_CUDA(cudaMemcpyAsync(a_.idx.data(), a64_.idx.data(), sizeof(int32_t) * a64_.nnz,
+                                  cudaMemcpyDeviceToDevice, ctx_.stream));
+        ConvertValues<double, T>(ctx_, a64_.val.data(), a_.val.data(), a64_.nnz);
+      }
     }
     Transpose(ctx_, A(), a_csr_);
     BuildAEll(a);

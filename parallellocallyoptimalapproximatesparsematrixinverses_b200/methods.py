@@ -113,7 +113,12 @@ def adopt_matrix(result: _lib.Result) -> sparse.csc_matrix:
         setattr(result, field, None)
         arrays.append(np.asarray(_LibraryArray(address, count, typestr, release)))
     indptr, indices, values = arrays
-    return sparse.csc_matrix((values, indices, indptr), shape=(result.rows, result.cols))
+    # assigned, not passed to the constructor: scipy would scan the indices and
+    # copy them down to int32; the library's columns are sorted and duplicate-free
+    m = sparse.csc_matrix((result.rows, result.cols), dtype=np.float64)
+    m.data, m.indices, m.indptr = values, indices, indptr
+    m.has_canonical_format = True
+    return m
 
 
 def result_to_python(result: _lib.Result) -> OutputResult:
