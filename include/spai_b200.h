@@ -213,6 +213,23 @@ typedef struct SpaiSession SpaiSession;
 SpaiSession* spai_session_create(int64_t method, struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
                                  struct MethodParams params, const SpaiExtParams* ext, char* error,
                                  int64_t error_capacity);
+/* The same with the problem already in DEVICE memory (for example the arrays
+ * of a torch sparse CSC tensor on the GPU), with no host round trip: A (and
+ * M0 when params.use_initial_m) as canonical CSC -- int64 col_offsets (n + 1)
+ * running from 0 to nnz, int64 row_indices strictly increasing in every
+ * column, FP64 values -- on the session's device, checked there.  Pr is
+ * diag(A)^-1 (params.use_preconditioner must be 0).  The caller's arrays are
+ * read during the call only; finish writing them before calling. */
+SpaiSession* spai_session_create_device(int64_t method, int64_t n, int64_t a_nnz, const int64_t* a_col_offsets,
+                                        const int64_t* a_row_indices, const double* a_values, int64_t m0_nnz,
+                                        const int64_t* m0_col_offsets, const int64_t* m0_row_indices,
+                                        const double* m0_values, struct MethodParams params,
+                                        const SpaiExtParams* ext, char* error, int64_t error_capacity);
+/* M of the last run into DEVICE arrays on the session's device: col_offsets
+ * (n + 1 int64), row_indices and values (capacity >= nnz(M) int64 / double).
+ * Returns nnz(M) (the copies are complete), or -1 with `error`. */
+int64_t spai_session_result_device(SpaiSession* session, int64_t* col_offsets, int64_t* row_indices, double* values,
+                                   int64_t capacity, char* error, int64_t error_capacity);
 /* Runs the method from M0 on the resident problem; M stays on the device.
  * Returns 0 (sets *iterations, *converged, *nnz_m), or -1 with `error`. */
 int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* converged, int64_t* nnz_m,

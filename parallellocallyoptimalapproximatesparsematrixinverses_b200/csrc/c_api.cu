@@ -596,6 +596,103 @@ SpaiSession* spai_session_create(int64_t method, MatrixData A, MatrixData M0, Ma
   }
 }
 
+SpaiSession* spai_session_create_device(int64_t method, int64_t n, int64_t a_nnz, const int64_t* a_col_offsets,
+                                        const int64_t* a_row_indices, const double* a_values, int64_t m0_nnz,
+                                        const int64_t* m0_col_offsets, const int64_t* m0_row_indices,
+                                        const double* m0_values, MethodParams params, const SpaiExtParams* ext,
+                                        char* error, int64_t error_capacity) {
+  SpaiSession* session = nullptr;
+  try {
+    if (method < 0 || method > 4) throw std::invalid_argument("unknown method id");
+    // GetCompressedSparseMatrix (methods_c_api.cpp:16-40) on the sizes; the arrays are checked on the device
+    if (n <= 0 || a_nnz <= 0) throw std::invalid_argument("Sparse matrix dimensions and nnz must be positive");
+    if (params.use_initial_m != 0 && m0_nnz <= 0) {
+      throw std::invalid_argument("Sparse matrix dimensions and nnz must be positive");
+    }
+    if (n > static_cast<int64_t>(INT32_MAX)) {
+      throw std::invalid_argument("Sparse matrix dimensions exceed the 32-bit row index range of the device layout");
+    }
+    if (params.use_preconditioner != 0) {
+      throw std::invalid_argument("device sessions use Pr = diag(A)^-1: use_preconditioner must be 0");
+    }
+    if (method >= 3 && params.inner_iterations <= 0) throw std::invalid_argument("inner_iterations must be positive");
+    spai::HostCsc shape_a;
+    shape_a.rows = shape_a.cols = n;
+    shape_a.nnz = a_nnz;
+    spai::HostCsc shape_m = shape_a;
+    shape_m.nnz = m0_nnz;
+    spai::ValidateProblem(shape_a, params.use_initial_m != 0 ? &shape_m : nullptr, nullptr, params);
+    spai::Inputs unused;
+    MatrixData none{};
+    spai::SolveOptions opt;
+    {
+      // the option checks of the host entry points, on a placeholder matrix
+      const int64_t ptr[2] = {0, 1};
+      const int64_t idx[1] = {0};
+      const double val[1] = {1.0};
+      const MatrixData one{1, 1, 1, ptr, idx, val};
+      MethodParams p = params;
+      p.use_initial_m = 0;
+      p.use_preconditioner = 0;
+      p.max_density = 1.0;
+      opt = spai::CheckInputs(method, one, none, none, p, ext, unused);
+      opt.max_density = params.max_density;
+      opt.num_threads = params.num_threads;
+    }
+    const int device = spai::ResolveDevice(ext != nullptr ? ext->device : -1);
+    SPAI_CUDA(cudaSetDevice(device));
+    auto check = [&](const void* ptr, size_t bytes, const char* name) {
+      if (bytes == 0) return;
+      cudaPointerAttributes attr{};
+      if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+        cudaGetLastError();
+        throw std::invalid_argument(std::string(name) + " is not a pointer CUDA knows");
+      }
+      if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) {
+        throw std::invalid_argument(std::string(name) + " must point to device memory");
+      }
+      if (attr.type == cudaMemoryTypeDevice && attr.device != device) {
+        throw std::invalid_argument(std::string(name) + " lives on another device than the session's");
+      }
+    };
+    check(a_col_offsets, sizeof(int64_t) * (n + 1), "A col_offsets");
+    check(a_row_indices, sizeof(int64_t) * a_nnz, "A row_indices");
+    check(a_values, sizeof(double) * a_nnz, "A values");
+    spai::DeviceCscInput a{n, a_nnz, a_col_offsets, a_row_indices, a_values};
+    spai::DeviceCscInput m0{n, m0_nnz, m0_col_offsets, m0_row_indices, m0_values};
+    if (params.use_initial_m != 0) {
+      check(m0_col_offsets, sizeof(int64_t) * (n + 1), "M0 col_offsets");
+      check(m0_row_indices, sizeof(int64_t) * m0_nnz, "M0 row_indices");
+      check(m0_values, sizeof(double) * m0_nnz, "M0 values");
+    }
+    session = new SpaiSession();
+    session->ctx.Init(device);
+    session->options = opt;
+    session->n = n;
+    session->solver = spai::MakeSolver(session->ctx, opt);
+    session->solver->UploadDevice(a, params.use_initial_m != 0 ? &m0 : nullptr);
+    return session;
+  } catch (const std::exception& ex) {
+    delete session;
+    spai::CopyError(ex.what(), error, error_capacity);
+    return nullptr;
+  }
+}
+
+int64_t spai_session_result_device(SpaiSession* session, int64_t* col_offsets, int64_t* row_indices, double* values,
+                                   int64_t capacity, char* error, int64_t error_capacity) {
+  try {
+    if (session == nullptr) throw std::invalid_argument("null session");
+    const int64_t nnz = session->solver->m_nnz();
+    if (capacity < nnz) throw std::invalid_argument("capacity is smaller than nnz(M)");
+    session->solver->ExportMDevice(col_offsets, row_indices, values);
+    return nnz;
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
 int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* converged, int64_t* nnz_m, char* error,
                          int64_t error_capacity) {
   try {

@@ -78,6 +78,87 @@ __global__ void BatchDotsKernel(CscView<T> x, CscView<T> y, const int64_t* __res
   }
 }
 
+// Canonical device CSC (int64 offsets and rows) -> int32 rows in dst, with
+// *bad |= 1 for offsets that do not run from 0 to nnz or decrease, and
+// |= 2 for rows out of [0, n) or not strictly increasing in a column.
+__global__ void CheckNarrowCscKernel(int64_t n, int64_t nnz, const int64_t* __restrict__ ptr,
+                                     const int64_t* __restrict__ idx, int32_t* __restrict__ dst,
+                                     int32_t* __restrict__ bad) {
+  int flags = 0;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = ptr[j];
+    const int64_t e = ptr[j + 1];
+    if ((j == 0 && b != 0) || (j == n - 1 && e != nnz) || e < b || b < 0 || e > nnz) {
+      flags |= 1;
+      continue;
+    }
+    int64_t previous = -1;
+    for (int64_t p = b; p < e; ++p) {
+      const int64_t r = idx[p];
+      if (r < 0 || r >= n || r <= previous) flags |= 2;
+      previous = r;
+      dst[p] = static_cast<int32_t>(r);
+    }
+  }
+  if (flags != 0) atomicOr(bad, flags);
+}
+
+// The longest column of x and the longest row (the longest column of its
+// transpose) into out[0] (out zeroed by the caller).
+__global__ void LongestKernel(const int64_t* __restrict__ ptr_a, const int64_t* __restrict__ ptr_b, int64_t n,
+                              unsigned long long* __restrict__ out) {
+  unsigned long long m = 0;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const unsigned long long a = static_cast<unsigned long long>(ptr_a[j + 1] - ptr_a[j]);
+    const unsigned long long b = static_cast<unsigned long long>(ptr_b[j + 1] - ptr_b[j]);
+    m = a > m ? a : m;
+    m = b > m ? b : m;
+  }
+  if (m != 0ull) atomicMax(out, m);
+}
+
+// pr[j] = 1 / A(j, j) (methods_common.cpp:50-63); *bad |= 1 for a missing,
+// non-positive or non-finite diagonal, |= 2 for a non-finite inverse.
+template <class T>
+__global__ void DiagonalInverseKernel(CscView<double> a, T* __restrict__ pr, int32_t* __restrict__ bad) {
+  int flags = 0;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < a.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    int64_t lo = a.ptr[j];
+    int64_t hi = a.ptr[j + 1];
+    while (lo < hi) {
+      const int64_t mid = lo + ((hi - lo) >> 1);
+      if (a.idx[mid] < j) {
+        lo = mid + 1;
+      } else {
+        hi = mid;
+      }
+    }
+    const double d = (lo < a.ptr[j + 1] && a.idx[lo] == j) ? a.val[lo] : 0.0;
+    if (!isfinite(d) || d <= 0.0) {
+      flags |= 1;
+      continue;
+    }
+    const double inverse = __ddiv_rn(1.0, d);
+    if (!isfinite(inverse)) flags |= 2;
+    pr[j] = static_cast<T>(inverse);
+  }
+  if (flags != 0) atomicOr(bad, flags);
+}
+
+// int32 rows and T values -> int64 and FP64 (device to device).
+template <class T>
+__global__ void WidenKernel(const int32_t* __restrict__ idx, const T* __restrict__ val, int64_t n,
+                            int64_t* __restrict__ idx_out, double* __restrict__ val_out) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    idx_out[i] = static_cast<int64_t>(idx[i]);
+    val_out[i] = static_cast<double>(val[i]);
+  }
+}
+
 // out[i] = ptr[at[i]]: the column offsets of a matrix at the block boundaries.
 __global__ void GatherOffsetsKernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ at, int64_t count,
                                     int64_t* __restrict__ out) {
@@ -203,71 +284,49 @@ class Solver final : public SolverBase {
     DevBuf<int64_t> stage_idx;
     DevBuf<double> stage_val;
     UploadCsc(ctx_, a, a64_, stage_idx, stage_val);
-    if constexpr (!std::is_same<T, double>::value) {
-      // the FP32 copy from the FP64 one already in HBM (same rounding as from the host values)
-      a_.Shape(a64_.rows, a64_.cols, ctx_.stream);
-      a_.ReserveNnz(a64_.nnz, ctx_.stream);
-      SPAI_CUDA(cudaMemcpyAsync(a_.ptr.data(), a64_.ptr.data(), sizeof(int64_t) * (a64_.cols + 1),
-                                cudaMemcpyDeviceToDevice, ctx_.stream));
-      if (a64_.nnz > 0) {
-        SPAI_CUDA(cudaMemcpyAsync(a_.idx.data(), a64_.idx.data(), sizeof(int32_t) * a64_.nnz,
-                                  cudaMemcpyDeviceToDevice, ctx_.stream));
-        ConvertValues<double, T>(ctx_, a64_.val.data(), a_.val.data(), a64_.nnz);
-      }
-    }
-    Transpose(ctx_, A(), a_csr_);
-    BuildAEll(a);
-    if (ReferenceOrder()) InitReferenceBatches();
-    // ||A e_k||^2 per column (methods_common.cpp:65-76)
-    col_norm2_.Reserve(static_cast<size_t>(n_), ctx_.stream);
-    if (opt_.dropping) {
-      ColumnSquares(ctx_, View(a64_), col_norm2_.data());
-    } else {
-      SPAI_CUDA(cudaMemsetAsync(col_norm2_.data(), 0, sizeof(double) * n_, ctx_.stream));
-    }
+    SetUpFromA();
     // preconditioner (methods_common.cpp:105-110)
     pr_diagonal_ = true;
-    std::vector<double> diag(n_);
     if (pr != nullptr) {
       pr_diagonal_ = IsFullDiagonal(*pr);
       if (pr_diagonal_) {
-        for (int64_t j = 0; j < n_; ++j) diag[j] = pr->val[pr->ptr[j]];
+        std::vector<T> host(n_);
+        for (int64_t j = 0; j < n_; ++j) host[j] = static_cast<T>(pr->val[pr->ptr[j]]);
+        pr_vec_.Reserve(static_cast<size_t>(n_), ctx_.stream);
+        SPAI_CUDA(cudaMemcpyAsync(pr_vec_.data(), host.data(), sizeof(T) * n_, cudaMemcpyHostToDevice, ctx_.stream));
+        ctx_.Sync();
       } else {
         UploadCsc(ctx_, *pr, pr_, stage_idx, stage_val);
         Transpose(ctx_, pr_, pr_csr_);
       }
     } else {
-      for (int64_t j = 0; j < n_; ++j) diag[j] = DiagonalEntry(a, j);
-      for (int64_t j = 0; j < n_; ++j) {
-        if (!std::isfinite(diag[j]) || diag[j] <= 0.0) {
-          throw std::invalid_argument("A has an invalid diagonal entry; provide Pr explicitly");
-        }
-      }
-      for (int64_t j = 0; j < n_; ++j) {
-        const double inverse = 1.0 / diag[j];
-        if (!std::isfinite(inverse)) {
-          throw std::invalid_argument("A diagonal cannot be inverted safely; provide Pr explicitly");
-        }
-        diag[j] = inverse;
-      }
-    }
-    if (pr_diagonal_) {
-      std::vector<T> host(n_);
-      for (int64_t j = 0; j < n_; ++j) host[j] = static_cast<T>(diag[j]);
-      pr_vec_.Reserve(static_cast<size_t>(n_), ctx_.stream);
-      SPAI_CUDA(cudaMemcpyAsync(pr_vec_.data(), host.data(), sizeof(T) * n_, cudaMemcpyHostToDevice, ctx_.stream));
-      ctx_.Sync();
+      DiagonalInversePreconditioner();
     }
     // M0 (methods_common.cpp:78-103): given, or the identity
     if (m0 != nullptr) {
       UploadCsc(ctx_, *m0, m0_, stage_idx, stage_val);
     } else {
-      m0_.Shape(n_, n_, ctx_.stream);
-      m0_.ReserveNnz(n_, ctx_.stream);
-      IdentityKernel<<<GridFor(n_ + 1, 256), 256, 0, ctx_.stream>>>(n_, m0_.ptr.data(), m0_.idx.data());
-      SPAI_LAUNCH_CHECK();
-      FillKernel<T><<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(m0_.val.data(), n_, T(1));
-      SPAI_LAUNCH_CHECK();
+      IdentityM0();
+    }
+    ctx_.Sync();
+  }
+
+  void UploadDevice(const DeviceCscInput& a, const DeviceCscInput* m0) override {
+    n_ = a.n;
+    CopyCheckedFromDevice(a, a64_, "A");
+    SetUpFromA();
+    pr_diagonal_ = true;
+    DiagonalInversePreconditioner();
+    if (m0 != nullptr) {
+      DevCsc<double> m64;
+      CopyCheckedFromDevice(*m0, m64, "M0");
+      if constexpr (std::is_same<T, double>::value) {
+        m0_.Swap(m64);
+      } else {
+        ConvertCsc(m64, m0_);
+      }
+    } else {
+      IdentityM0();
     }
     ctx_.Sync();
   }
@@ -310,6 +369,16 @@ class Solver final : public SolverBase {
     SPAI_CUDA(cudaMemcpyAsync(ptr, m_.ptr.data(), sizeof(int64_t) * (m_.cols + 1), cudaMemcpyDeviceToHost,
                               ctx_.stream));
     DownloadWiden<T>(ctx_, m_.idx.data(), m_.val.data(), m_.nnz, 0, idx, val);
+    ctx_.Sync();
+  }
+
+  void ExportMDevice(int64_t* ptr, int64_t* idx, double* val) override {
+    SPAI_CUDA(cudaMemcpyAsync(ptr, m_.ptr.data(), sizeof(int64_t) * (m_.cols + 1), cudaMemcpyDeviceToDevice,
+                              ctx_.stream));
+    if (m_.nnz > 0) {
+      WidenKernel<T><<<GridFor(m_.nnz, 256), 256, 0, ctx_.stream>>>(m_.idx.data(), m_.val.data(), m_.nnz, idx, val);
+      SPAI_LAUNCH_CHECK();
+    }
     ctx_.Sync();
   }
 
@@ -526,8 +595,8 @@ class Solver final : public SolverBase {
   }
 
  private:
-  template <class D>
-  void ConvertCsc(const DevCsc<T>& src, DevCsc<D>& dst) {
+  template <class S, class D>
+  void ConvertCsc(const DevCsc<S>& src, DevCsc<D>& dst) {
     dst.Shape(src.rows, src.cols, ctx_.stream);
     dst.ReserveNnz(src.nnz, ctx_.stream);
     SPAI_CUDA(cudaMemcpyAsync(dst.ptr.data(), src.ptr.data(), sizeof(int64_t) * (src.cols + 1),
@@ -535,7 +604,7 @@ class Solver final : public SolverBase {
     if (src.nnz > 0) {
       SPAI_CUDA(cudaMemcpyAsync(dst.idx.data(), src.idx.data(), sizeof(int32_t) * src.nnz, cudaMemcpyDeviceToDevice,
                                 ctx_.stream));
-      ConvertValues<T, D>(ctx_, src.val.data(), dst.val.data(), src.nnz);
+      ConvertValues<S, D>(ctx_, src.val.data(), dst.val.data(), src.nnz);
     }
   }
 
@@ -555,24 +624,87 @@ class Solver final : public SolverBase {
     return true;
   }
 
-  static double DiagonalEntry(const HostCsc& a, int64_t j) {
-    const int64_t* begin = a.idx + a.ptr[j];
-    const int64_t* end = a.idx + a.ptr[j + 1];
-    const int64_t* it = std::lower_bound(begin, end, j);
-    if (it != end && *it == j) return a.val[it - a.idx];
-    return 0.0;
+  // Everything that follows from A in HBM (a64_ set): the FP32 copy, the
+  // row-compressed copy, the ELL copies, the reference batches and ||A e_k||^2.
+  void SetUpFromA() {
+    if constexpr (!std::is_same<T, double>::value) {
+      // the FP32 copy from the FP64 one already in HBM (same rounding as from the host values)
+      ConvertCsc(a64_, a_);
+    }
+    Transpose(ctx_, A(), a_csr_);
+    BuildAEll();
+    if (ReferenceOrder()) InitReferenceBatches();
+    // ||A e_k||^2 per column (methods_common.cpp:65-76)
+    col_norm2_.Reserve(static_cast<size_t>(n_), ctx_.stream);
+    if (opt_.dropping) {
+      ColumnSquares(ctx_, View(a64_), col_norm2_.data());
+    } else {
+      SPAI_CUDA(cudaMemsetAsync(col_norm2_.data(), 0, sizeof(double) * n_, ctx_.stream));
+    }
+  }
+
+  // Pr = diag(A)^-1 on the device, with the reference's messages for a bad diagonal.
+  void DiagonalInversePreconditioner() {
+    pr_vec_.Reserve(static_cast<size_t>(n_), ctx_.stream);
+    int32_t* bad = ctx_.flags.data() + 4;
+    SPAI_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx_.stream));
+    DiagonalInverseKernel<T><<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(View(a64_), pr_vec_.data(), bad);
+    SPAI_LAUNCH_CHECK();
+    SPAI_CUDA(cudaMemcpyAsync(ctx_.host_flags + 4, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx_.stream));
+    ctx_.Sync();
+    if (ctx_.host_flags[4] & 1) throw std::invalid_argument("A has an invalid diagonal entry; provide Pr explicitly");
+    if (ctx_.host_flags[4] & 2) {
+      throw std::invalid_argument("A diagonal cannot be inverted safely; provide Pr explicitly");
+    }
+  }
+
+  void IdentityM0() {
+    m0_.Shape(n_, n_, ctx_.stream);
+    m0_.ReserveNnz(n_, ctx_.stream);
+    IdentityKernel<<<GridFor(n_ + 1, 256), 256, 0, ctx_.stream>>>(n_, m0_.ptr.data(), m0_.idx.data());
+    SPAI_LAUNCH_CHECK();
+    FillKernel<T><<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(m0_.val.data(), n_, T(1));
+    SPAI_LAUNCH_CHECK();
+  }
+
+  // A canonical CSC in device memory -> out (int32 rows), checked on the device.
+  void CopyCheckedFromDevice(const DeviceCscInput& in, DevCsc<double>& out, const char* name) {
+    out.Shape(in.n, in.n, ctx_.stream);
+    out.ReserveNnz(in.nnz, ctx_.stream);
+    SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), in.col_offsets, sizeof(int64_t) * (in.n + 1), cudaMemcpyDeviceToDevice,
+                              ctx_.stream));
+    if (in.nnz > 0) {
+      SPAI_CUDA(cudaMemcpyAsync(out.val.data(), in.values, sizeof(double) * in.nnz, cudaMemcpyDeviceToDevice,
+                                ctx_.stream));
+    }
+    int32_t* bad = ctx_.flags.data() + 5;
+    SPAI_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx_.stream));
+    CheckNarrowCscKernel<<<GridFor(in.n, 128), 128, 0, ctx_.stream>>>(in.n, in.nnz, in.col_offsets, in.row_indices,
+                                                                      out.idx.data(), bad);
+    SPAI_LAUNCH_CHECK();
+    SPAI_CUDA(cudaMemcpyAsync(ctx_.host_flags + 5, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx_.stream));
+    ctx_.Sync();
+    if (ctx_.host_flags[5] & 1) {
+      throw std::invalid_argument(std::string(name) + ": column offsets must run from 0 to nnz without decreasing");
+    }
+    if (ctx_.host_flags[5] & 2) {
+      throw std::invalid_argument(std::string(name) +
+                                  ": row indices must lie in [0, n) and increase strictly in every column");
+    }
   }
 
   // ELL copies of A when no row or column of A holds more than kMaxEllWidth entries.
-  void BuildAEll(const HostCsc& a) {
+  void BuildAEll() {
     ell_width_ = 0;
-    int64_t longest = 0;
-    std::vector<int64_t> row_len(static_cast<size_t>(a.rows), 0);
-    for (int64_t j = 0; j < a.cols; ++j) {
-      longest = std::max(longest, a.ptr[j + 1] - a.ptr[j]);
-      for (int64_t p = a.ptr[j]; p < a.ptr[j + 1]; ++p) ++row_len[static_cast<size_t>(a.idx[p])];
-    }
-    for (const int64_t len : row_len) longest = std::max(longest, len);
+    // the longest column of A and of its transpose (the longest row)
+    unsigned long long* longest_dev = ctx_.select_state.data() + 3;
+    SPAI_CUDA(cudaMemsetAsync(longest_dev, 0, sizeof(unsigned long long), ctx_.stream));
+    LongestKernel<<<GridFor(n_, 256), 256, 0, ctx_.stream>>>(A().ptr.data(), a_csr_.ptr.data(), n_, longest_dev);
+    SPAI_LAUNCH_CHECK();
+    SPAI_CUDA(cudaMemcpyAsync(ctx_.host_counts + 2, longest_dev, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                              ctx_.stream));
+    ctx_.Sync();
+    const int64_t longest = ctx_.host_counts[2];
     if (longest > kMaxEllWidth) return;
     const int width = static_cast<int>(std::max<int64_t>(4, (longest + 3) / 4 * 4));
     const size_t slots = static_cast<size_t>(n_) * static_cast<size_t>(width);

@@ -83,16 +83,30 @@ struct IterationTimes {
   double iterate_ms = 0.0;
 };
 
+// A canonical n x n CSC in device memory (offsets from 0 to nnz, rows
+// strictly increasing in every column), int64 indices and FP64 values.
+struct DeviceCscInput {
+  int64_t n = 0;
+  int64_t nnz = 0;
+  const int64_t* col_offsets = nullptr;
+  const int64_t* row_indices = nullptr;
+  const double* values = nullptr;
+};
+
 class SolverBase {
  public:
   virtual ~SolverBase() = default;
   // Host-to-device upload and one-time setup (row-compressed A, column norms,
   // preconditioner).  m0 / pr may be null (identity / diag(A)^-1).
   virtual void Upload(const HostCsc& a, const HostCsc* m0, const HostCsc* pr) = 0;
+  // The same from device memory (checked on the device); Pr = diag(A)^-1.
+  virtual void UploadDevice(const DeviceCscInput& a, const DeviceCscInput* m0) = 0;
   // Runs the method from M0; may be called repeatedly.
   virtual void Run() = 0;
   // Copies M (as FP64, int64 indices) and the history to the host.
   virtual void Download(SolveOutput& out) = 0;
+  // Copies M into DEVICE arrays of n() + 1 (ptr) and m_nnz() (idx, val) entries (int64, FP64); synchronises.
+  virtual void ExportMDevice(int64_t* ptr, int64_t* idx, double* val) = 0;
   // Copies M straight into host arrays of n() + 1 (ptr) and m_nnz() (idx, val) entries.
   virtual void DownloadM(int64_t* ptr, int64_t* idx, double* val) = 0;
   virtual const std::vector<SingleIterationData>& history() const = 0;

@@ -263,6 +263,62 @@ class Session:
             raise RuntimeError(err.value.decode("utf-8", "replace"))
         self._handle = ctypes.c_void_p(handle)
         self.n = self._A.shape[0]
+        self._nnz = 0
+
+    @classmethod
+    def from_torch(cls, family, name, A, M0=None, max_iterations=100, tolerance=1e-9, max_density=0.03,
+                   enable_dropping=True, num_threads=1, inner_iterations=2, precision="fp64", topk_per_column=0,
+                   summation="device"):
+        """A session on the GPU arrays of torch sparse CSC tensors -- A, and M0
+        when given -- with no host round trip (spai_session_create_device):
+        float64 values on one CUDA device, rows sorted and unique in every
+        column (checked on the device).  Pr is diag(A)^-1."""
+        import torch
+        tensors = [A] + ([M0] if M0 is not None else [])
+        for t in tensors:
+            if t.layout != torch.sparse_csc or not t.is_cuda or t.dtype != torch.float64:
+                raise ValueError("A and M0 must be float64 torch.sparse_csc tensors on a CUDA device")
+            if t.shape[0] != t.shape[1] or t.shape != A.shape or t.device != A.device:
+                raise ValueError("A and M0 must be square, of one size and on one device")
+        arrays = [(t.ccol_indices().to(torch.int64).contiguous(), t.row_indices().to(torch.int64).contiguous(),
+                   t.values().contiguous()) for t in tensors]
+        torch.cuda.synchronize(A.device)  # the arrays are complete before the library reads them on its stream
+        self = cls.__new__(cls)
+        self._lib = _lib.load()
+        n = A.shape[0]
+        params = _lib.MethodParams(max_iterations, tolerance, max_density, 1 if enable_dropping else 0, num_threads,
+                                   1 if M0 is not None else 0, 0, inner_iterations)
+        ext = ext_params(precision, topk_per_column, A.device.index, summation)
+        a_ptr, a_idx, a_val = arrays[0]
+        m_ptr, m_idx, m_val = arrays[1] if M0 is not None else (None, None, None)
+        err = _lib.error_buffer()
+        handle = self._lib.spai_session_create_device(
+            _lib.METHOD_IDS[(family, name)], n, a_val.numel(), a_ptr.data_ptr(), a_idx.data_ptr(), a_val.data_ptr(),
+            m_val.numel() if m_val is not None else 0, m_ptr.data_ptr() if m_ptr is not None else None,
+            m_idx.data_ptr() if m_idx is not None else None, m_val.data_ptr() if m_val is not None else None,
+            params, ctypes.byref(ext), err, len(err))
+        if not handle:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        self._handle = ctypes.c_void_p(handle)
+        self.n = n
+        self._nnz = 0
+        self._device = A.device
+        return self
+
+    def result_torch(self):
+        """M of the last run as a float64 torch.sparse_csc tensor on the
+        session's device (spai_session_result_device; no host round trip)."""
+        import torch
+        device = getattr(self, "_device", None) or torch.device("cuda", torch.cuda.current_device())
+        ptr = torch.empty(self.n + 1, dtype=torch.int64, device=device)
+        idx = torch.empty(max(self._nnz, 1), dtype=torch.int64, device=device)
+        val = torch.empty(max(self._nnz, 1), dtype=torch.float64, device=device)
+        err = _lib.error_buffer()
+        nnz = self._lib.spai_session_result_device(self._handle, ptr.data_ptr(), idx.data_ptr(), val.data_ptr(),
+                                                   idx.numel(), err, len(err))
+        if nnz < 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        return torch.sparse_csc_tensor(ptr, idx[:nnz], val[:nnz], size=(self.n, self.n))
 
     def run(self):
         it = ctypes.c_int64(0)
@@ -272,6 +328,8 @@ class Session:
         if self._lib.spai_session_run(self._handle, ctypes.byref(it), ctypes.byref(conv), ctypes.byref(nnz), err,
                                       len(err)) != 0:
             raise RuntimeError(err.value.decode("utf-8", "replace"))
+        self._nnz = nnz.value
+        self.converged = bool(conv.value)
         return it.value, nnz.value
 
     def history(self):
