@@ -119,19 +119,11 @@ struct Inputs {
   bool has_pr = false;
 };
 
-SolveOptions CheckInputs(int64_t method, const MatrixData& A, const MatrixData& M0, const MatrixData& Pr,
-                         const MethodParams& params, const SpaiExtParams* ext, Inputs& in) {
+// The run options from the reference's MethodParams and the extension
+// knobs (the matrices are checked by the callers).
+SolveOptions ParseOptions(int64_t method, const MethodParams& params, const SpaiExtParams* ext) {
   if (method < 0 || method > 4) throw std::invalid_argument("unknown method id");
-  in.a = CheckedMatrix(A);
-  in.has_m0 = params.use_initial_m != 0;
-  if (in.has_m0) in.m0 = CheckedMatrix(M0);
-  in.has_pr = params.use_preconditioner != 0;
-  if (in.has_pr) in.pr = CheckedMatrix(Pr);
-  const bool inner_outer = method >= 3;
-  if (inner_outer && params.inner_iterations <= 0) {
-    throw std::invalid_argument("inner_iterations must be positive");
-  }
-  ValidateProblem(in.a, in.has_m0 ? &in.m0 : nullptr, in.has_pr ? &in.pr : nullptr, params);
+  if (method >= 3 && params.inner_iterations <= 0) throw std::invalid_argument("inner_iterations must be positive");
   SolveOptions opt;
   opt.method = static_cast<Method>(method);
   opt.max_iterations = params.max_iterations;
@@ -139,6 +131,7 @@ SolveOptions CheckInputs(int64_t method, const MatrixData& A, const MatrixData& 
   opt.max_density = params.max_density;
   opt.dropping = params.enable_dropping != 0;
   opt.inner_iterations = params.inner_iterations;
+  opt.num_threads = params.num_threads;
   if (ext != nullptr) {
     if (ext->precision != 0 && ext->precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
     if (ext->topk_per_column < 0) throw std::invalid_argument("topk_per_column must be non-negative");
@@ -149,7 +142,19 @@ SolveOptions CheckInputs(int64_t method, const MatrixData& A, const MatrixData& 
     opt.topk = ext->topk_per_column;
     opt.summation = static_cast<int>(ext->summation_order);
   }
-  opt.num_threads = params.num_threads;
+  return opt;
+}
+
+SolveOptions CheckInputs(int64_t method, const MatrixData& A, const MatrixData& M0, const MatrixData& Pr,
+                         const MethodParams& params, const SpaiExtParams* ext, Inputs& in) {
+  if (method < 0 || method > 4) throw std::invalid_argument("unknown method id");
+  in.a = CheckedMatrix(A);
+  in.has_m0 = params.use_initial_m != 0;
+  if (in.has_m0) in.m0 = CheckedMatrix(M0);
+  in.has_pr = params.use_preconditioner != 0;
+  if (in.has_pr) in.pr = CheckedMatrix(Pr);
+  const SolveOptions opt = ParseOptions(method, params, ext);
+  ValidateProblem(in.a, in.has_m0 ? &in.m0 : nullptr, in.has_pr ? &in.pr : nullptr, params);
   return opt;
 }
 
@@ -615,30 +620,14 @@ SpaiSession* spai_session_create_device(int64_t method, int64_t n, int64_t a_nnz
     if (params.use_preconditioner != 0) {
       throw std::invalid_argument("device sessions use Pr = diag(A)^-1: use_preconditioner must be 0");
     }
-    if (method >= 3 && params.inner_iterations <= 0) throw std::invalid_argument("inner_iterations must be positive");
+    const spai::SolveOptions opt = spai::ParseOptions(method, params, ext);
+    // ValidateProblem reads only the shapes
     spai::HostCsc shape_a;
     shape_a.rows = shape_a.cols = n;
     shape_a.nnz = a_nnz;
     spai::HostCsc shape_m = shape_a;
     shape_m.nnz = m0_nnz;
     spai::ValidateProblem(shape_a, params.use_initial_m != 0 ? &shape_m : nullptr, nullptr, params);
-    spai::Inputs unused;
-    MatrixData none{};
-    spai::SolveOptions opt;
-    {
-      // the option checks of the host entry points, on a placeholder matrix
-      const int64_t ptr[2] = {0, 1};
-      const int64_t idx[1] = {0};
-      const double val[1] = {1.0};
-      const MatrixData one{1, 1, 1, ptr, idx, val};
-      MethodParams p = params;
-      p.use_initial_m = 0;
-      p.use_preconditioner = 0;
-      p.max_density = 1.0;
-      opt = spai::CheckInputs(method, one, none, none, p, ext, unused);
-      opt.max_density = params.max_density;
-      opt.num_threads = params.num_threads;
-    }
     const int device = spai::ResolveDevice(ext != nullptr ? ext->device : -1);
     SPAI_CUDA(cudaSetDevice(device));
     auto check = [&](const void* ptr, size_t bytes, const char* name) {
