@@ -251,6 +251,12 @@ void spai_session_destroy(SpaiSession* session);
  * callers that time the session with their own CUDA events. */
 void* spai_session_stream(SpaiSession* session);
 
+/* Fault injection for tests: after `after` more growing device
+ * reservations, the next one fails as if the device were out of memory (once;
+ * -1 disarms).  The failing call reports the error through its usual error
+ * path and releases what it held; the library stays usable. */
+void spai_inject_allocation_failure(int64_t after);
+
 /* Number of kernels this library has launched since load (diagnostics). */
 int64_t spai_kernel_launches(void);
 

@@ -26,9 +26,16 @@ namespace spai {
 
 namespace {
 std::atomic<int64_t> g_launches{0};
+std::atomic<int64_t> g_fail_after{-1};
 }  // namespace
 
 void CountLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+bool AllocationFailureInjected() {
+  if (g_fail_after.load(std::memory_order_relaxed) < 0) return false;
+  // the reservation that brings the count to zero fails, then the hook disarms
+  return g_fail_after.fetch_sub(1, std::memory_order_relaxed) == 0;
+}
 
 namespace {
 
@@ -107,7 +114,14 @@ int ResolveDevice(int64_t requested) {
 
 struct CtxGuard {
   Ctx ctx;
-  explicit CtxGuard(int device) { ctx.Init(device); }
+  explicit CtxGuard(int device) {
+    try {
+      ctx.Init(device);
+    } catch (...) {
+      ctx.Destroy();  // what Init created so far
+      throw;
+    }
+  }
   ~CtxGuard() { ctx.Destroy(); }
 };
 
@@ -352,6 +366,8 @@ void free_mem(Result* result) {
   result->history = nullptr;
   result->error_message = nullptr;
 }
+
+void spai_inject_allocation_failure(int64_t after) { spai::g_fail_after.store(after, std::memory_order_relaxed); }
 
 void spai_free_int64_array(int64_t* array) { delete[] array; }
 

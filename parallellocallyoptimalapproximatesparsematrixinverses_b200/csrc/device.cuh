@@ -36,6 +36,10 @@ class CudaError : public std::runtime_error {
 // Counts every kernel launch of the library (reported by spai_kernel_launches).
 void CountLaunch();
 
+// Fault injection for tests (spai_inject_allocation_failure): true once,
+// when the armed number of growing reservations has passed.
+bool AllocationFailureInjected();
+
 // Per-stream cache of released device blocks.  A block released on stream s
 // is handed to the next allocation on s that fits it (at least the request,
 // at most twice it): stream order makes the reuse safe without events, and
@@ -89,6 +93,7 @@ class DevBuf {
       stream_ = stream;
       return;
     }
+    if (AllocationFailureInjected()) throw CudaError("CUDA error: injected allocation failure (out of memory)");
     Release();
     const size_t cap = n + n / 4 + 64;
     size_t got = 0;
