@@ -46,3 +46,24 @@ def test_solve_2x2_degenerate_inputs():
     assert np.array_equal(pyoracle.solve_2x2(np.zeros((2, 2)), [1.0, 1.0]), [0.0, 0.0])
     assert np.array_equal(pyoracle.solve_2x2([[np.nan, 0], [0, 1]], [1.0, 1.0]), [0.0, 0.0])
     assert np.array_equal(pyoracle.solve_2x2([[1.0, 0], [0, 1]], [np.inf, 1.0]), [0.0, 0.0])
+
+
+def test_diffusion_batch_is_seeded_and_spd():
+    from scipy import sparse
+
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import problems
+    a = problems.diffusion_batch(count=12, seed=5, n_min=200, n_max=3000)
+    b = problems.diffusion_batch(count=12, seed=5, n_min=200, n_max=3000)
+    assert len(a) == 12
+    for x, y in zip(a, b):
+        assert (x != y).nnz == 0 and x.shape == y.shape
+        n = x.shape[0]
+        assert 100 <= n <= 4000  # rounded grid sides around [n_min, n_max]
+        assert abs(x - x.T).max() == 0.0
+        # diagonally dominant with a positive diagonal: symmetric positive definite
+        off = np.asarray(abs(x).sum(axis=1)).ravel() - np.abs(x.diagonal())
+        assert np.all(x.diagonal() > off)
+        assert x.has_sorted_indices and isinstance(x, sparse.csc_matrix)
+    # both grid kinds appear (5-point rows hold at most 5 entries, 7-point up to 7)
+    widths = {int(np.diff(x.indptr).max()) for x in a}
+    assert widths & {5} and widths & {7}
