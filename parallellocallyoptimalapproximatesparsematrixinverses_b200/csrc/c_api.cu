@@ -113,8 +113,9 @@ int ResolveDevice(int64_t requested) {
 }
 
 struct CtxGuard {
+  DeviceScope scope;  // constructed first, restored last: the caller keeps its current device
   Ctx ctx;
-  explicit CtxGuard(int device) {
+  explicit CtxGuard(int device) : scope(device) {
     try {
       ctx.Init(device);
     } catch (...) {
@@ -603,6 +604,7 @@ SpaiSession* spai_session_create(int64_t method, MatrixData A, MatrixData M0, Ma
     spai::Inputs in;
     const spai::SolveOptions opt = spai::CheckInputs(method, A, M0, Pr, params, ext, in);
     const int device = spai::ResolveDevice(ext != nullptr ? ext->device : -1);
+    spai::DeviceScope scope(device);
     session = new SpaiSession();
     session->ctx.Init(device);
     session->options = opt;
@@ -645,7 +647,7 @@ SpaiSession* spai_session_create_device(int64_t method, int64_t n, int64_t a_nnz
     shape_m.nnz = m0_nnz;
     spai::ValidateProblem(shape_a, params.use_initial_m != 0 ? &shape_m : nullptr, nullptr, params);
     const int device = spai::ResolveDevice(ext != nullptr ? ext->device : -1);
-    SPAI_CUDA(cudaSetDevice(device));
+    spai::DeviceScope scope(device);
     auto check = [&](const void* ptr, size_t bytes, const char* name) {
       if (bytes == 0) return;
       cudaPointerAttributes attr{};
@@ -688,6 +690,7 @@ int64_t spai_session_result_device(SpaiSession* session, int64_t* col_offsets, i
                                    int64_t capacity, char* error, int64_t error_capacity) {
   try {
     if (session == nullptr) throw std::invalid_argument("null session");
+    spai::DeviceScope scope(session->ctx.device);
     const int64_t nnz = session->solver->m_nnz();
     if (capacity < nnz) throw std::invalid_argument("capacity is smaller than nnz(M)");
     session->solver->ExportMDevice(col_offsets, row_indices, values);
@@ -702,6 +705,7 @@ int64_t spai_session_run(SpaiSession* session, int64_t* iterations, int64_t* con
                          int64_t error_capacity) {
   try {
     if (session == nullptr) throw std::invalid_argument("null session");
+    spai::DeviceScope scope(session->ctx.device);
     session->solver->Run();
     if (iterations != nullptr) *iterations = session->solver->iterations();
     if (nnz_m != nullptr) *nnz_m = session->solver->m_nnz();
@@ -729,6 +733,7 @@ int64_t spai_session_history(SpaiSession* session, SingleIterationData* out, int
 Result spai_session_result(SpaiSession* session) {
   try {
     if (session == nullptr) throw std::invalid_argument("null session");
+    spai::DeviceScope scope(session->ctx.device);
     return spai::SolverResult(*session->solver);
   } catch (const std::exception& ex) {
     return spai::ErrorResult(ex.what());
@@ -738,6 +743,7 @@ Result spai_session_result(SpaiSession* session) {
 int64_t spai_session_set_rhs(SpaiSession* session, const double* b, char* error, int64_t error_capacity) {
   try {
     if (session == nullptr) throw std::invalid_argument("null session");
+    spai::DeviceScope scope(session->ctx.device);
     const int64_t n = session->n;
     session->b.Reserve(static_cast<size_t>(n), session->ctx.stream);
     session->x.Reserve(static_cast<size_t>(n), session->ctx.stream);
@@ -760,6 +766,7 @@ int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history
                          char* error, int64_t error_capacity) {
   try {
     if (session == nullptr) throw std::invalid_argument("null session");
+    spai::DeviceScope scope(session->ctx.device);
     if (!session->has_rhs) throw std::invalid_argument("spai_session_set_rhs must be called first");
     spai::CheckPcgParams(session->n, params);
     spai::PcgOptions opt;
@@ -788,7 +795,15 @@ int64_t spai_session_pcg(SpaiSession* session, PcgParams params, double* history
   }
 }
 
-void spai_session_destroy(SpaiSession* session) { delete session; }
+void spai_session_destroy(SpaiSession* session) {
+  if (session == nullptr) return;
+  std::unique_ptr<spai::DeviceScope> scope;  // released after the session, restoring the caller's device
+  try {
+    scope.reset(new spai::DeviceScope(session->ctx.device));
+  } catch (...) {
+  }
+  delete session;
+}
 
 void* spai_session_stream(SpaiSession* session) {
   return session != nullptr ? static_cast<void*>(session->ctx.stream) : nullptr;

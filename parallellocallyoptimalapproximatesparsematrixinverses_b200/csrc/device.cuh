@@ -36,6 +36,29 @@ class CudaError : public std::runtime_error {
 // Counts every kernel launch of the library (reported by spai_kernel_launches).
 void CountLaunch();
 
+// Makes `device` the calling thread's current device for a scope and
+// restores the caller's device afterwards, so that an entry point neither
+// depends on nor changes the caller's choice of device.
+class DeviceScope {
+ public:
+  explicit DeviceScope(int device) {
+    if (cudaGetDevice(&previous_) != cudaSuccess) previous_ = -1;
+    if (device != previous_) {
+      SPAI_CUDA(cudaSetDevice(device));
+      changed_ = previous_ >= 0;
+    }
+  }
+  ~DeviceScope() {
+    if (changed_) cudaSetDevice(previous_);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+
+ private:
+  int previous_ = -1;
+  bool changed_ = false;
+};
+
 // Fault injection for tests (spai_inject_allocation_failure): true once,
 // when the armed number of growing reservations has passed.
 bool AllocationFailureInjected();
@@ -53,6 +76,9 @@ void CacheFlush(cudaStream_t stream);
 // After `stream` has been synchronised: its blocks join a pool of idle blocks
 // of `device` that later streams on the device take from before allocating.
 void CacheRetire(cudaStream_t stream, int device);
+// Records the device a context's stream belongs to (until CacheRetire), so
+// that the stream only ever receives that device's idle blocks.
+void CacheRegisterStream(cudaStream_t stream, int device);
 
 #define SPAI_LAUNCH_CHECK()          \
   do {                               \

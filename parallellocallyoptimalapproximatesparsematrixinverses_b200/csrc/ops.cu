@@ -991,6 +991,8 @@ std::map<cudaStream_t, std::vector<CachedBlock>> g_block_cache;
 // Blocks of finished contexts (their streams synchronised, so idle), per
 // device: any later context on the device takes them before the allocator.
 std::map<int, std::vector<CachedBlock>> g_retired;
+// the device of every live context stream
+std::map<cudaStream_t, int> g_stream_device;
 
 // Index of the smallest block in `blocks` that holds `bytes` without wasting
 // more than half of itself, or blocks.size().
@@ -1018,9 +1020,9 @@ void* CacheTake(cudaStream_t stream, size_t bytes, size_t* capacity_bytes) {
     const size_t at = BestFit(it->second, bytes);
     if (at < it->second.size()) return TakeAt(it->second, at, capacity_bytes);
   }
-  int device = 0;
-  if (cudaGetDevice(&device) != cudaSuccess) return nullptr;
-  auto retired = g_retired.find(device);
+  const auto owner = g_stream_device.find(stream);
+  if (owner == g_stream_device.end()) return nullptr;
+  auto retired = g_retired.find(owner->second);
   if (retired == g_retired.end()) return nullptr;
   const size_t at = BestFit(retired->second, bytes);
   return at < retired->second.size() ? TakeAt(retired->second, at, capacity_bytes) : nullptr;
@@ -1045,8 +1047,14 @@ void CacheFlush(cudaStream_t stream) {
   g_block_cache.erase(it);
 }
 
+void CacheRegisterStream(cudaStream_t stream, int device) {
+  std::lock_guard<std::mutex> lock(g_cache_mutex);
+  g_stream_device[stream] = device;
+}
+
 void CacheRetire(cudaStream_t stream, int device) {
   std::lock_guard<std::mutex> lock(g_cache_mutex);
+  g_stream_device.erase(stream);
   auto it = g_block_cache.find(stream);
   if (it == g_block_cache.end()) return;
   std::vector<CachedBlock>& retired = g_retired[device];
@@ -1141,6 +1149,7 @@ void Ctx::Init(int device_ordinal) {
   SPAI_CUDA(cudaSetDevice(device));
   SPAI_CUDA(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device));
   SPAI_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  CacheRegisterStream(stream, device);
   cudaMemPool_t pool;
   SPAI_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
   uint64_t threshold = UINT64_MAX;
