@@ -1,0 +1,109 @@
+"""Column sharding of the SPAI iteration over several GPUs: the reduction
+that keeps a sharded run bit-identical to a single-GPU run.
+
+Every op of the iteration except the global scalars (and the transpose of
+the drop step) is column-local, so the columns of M, R, Z and P can be split
+into contiguous ranges, one per rank, with A replicated.  A global scalar on
+one GPU is the fixed tree over the per-column partial sums: chunks of 4096
+values, each folded by 256 lanes (lane t adds values t, t + 256, ... in
+order) and a butterfly over the lanes, repeated over the chunk sums until
+one value is left (ops.cu, TreeChunkKernel).  Cutting the columns only at
+multiples of 4096 makes each rank's first-level chunk sums exactly the
+global ones, so
+
+    rank r: chunk sums of its columns           (on its device)
+    all ranks: all_gather of the chunk sums     (n / 4096 values per scalar)
+    every rank: the upper levels of the tree    (the same arithmetic)
+
+gives every rank the single-GPU value, bit for bit, with one small
+all-gather per set of scalars.  `shard_columns` makes such a cut and
+`sharded_tree_sums` does the exchange and the upper levels (torch.distributed;
+NCCL on GPUs, gloo on the host).  `tree_chunk_sums` / `tree_sum` restate the
+device tree on the host for the upper levels.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+TREE_LANES = 256
+TREE_CHUNK = 4096
+
+
+def shard_columns(n: int, world: int, align: int = TREE_CHUNK):
+    """Contiguous column ranges [start, stop) for `world` ranks, cut only at
+    multiples of `align` (the last range takes the remainder); ranks beyond
+    the number of chunks get empty ranges."""
+    if n < 0 or world <= 0 or align <= 0:
+        raise ValueError("n >= 0, world > 0 and align > 0 are required")
+    chunks = -(-n // align)
+    bounds = [min(n, (chunks * r // world) * align) for r in range(world + 1)]
+    bounds[-1] = n
+    return [(bounds[r], bounds[r + 1]) for r in range(world)]
+
+
+def _butterfly(lanes: np.ndarray) -> float:
+    """The lane butterfly of one chunk: strides 128 .. 1, s[t] = s[t] + s[t ^ stride]."""
+    s = lanes.copy()
+    t = np.arange(TREE_LANES)
+    stride = TREE_LANES // 2
+    while stride >= 1:
+        s = s + s[t ^ stride]
+        stride //= 2
+    return float(s[0])
+
+
+def tree_chunk_sums(values) -> np.ndarray:
+    """First level of the fixed tree: one sum per chunk of 4096 values."""
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    count = v.size
+    chunks = -(-count // TREE_CHUNK)
+    out = np.empty(chunks, dtype=np.float64)
+    for c in range(chunks):
+        part = np.zeros(TREE_CHUNK, dtype=np.float64)
+        block = v[c * TREE_CHUNK:(c + 1) * TREE_CHUNK]
+        part[:block.size] = block
+        lanes = np.zeros(TREE_LANES, dtype=np.float64)
+        # lane t adds values t, t + 256, ... in order, starting from +0.0
+        for m in range(TREE_CHUNK // TREE_LANES):
+            lanes = lanes + part[m * TREE_LANES:(m + 1) * TREE_LANES]
+        out[c] = _butterfly(lanes)
+    return out
+
+
+def tree_sum(values) -> float:
+    """The whole fixed tree (+0.0 for no values)."""
+    level = np.ascontiguousarray(values, dtype=np.float64)
+    if level.size == 0:
+        return 0.0
+    while True:
+        level = tree_chunk_sums(level)
+        if level.size == 1:
+            return float(level[0])
+
+
+def sharded_tree_sums(local_chunk_sums, group=None):
+    """Global tree sums from every rank's first-level chunk sums.
+
+    local_chunk_sums: array of shape (scalars, chunks of this rank), the
+    chunk sums of this rank's column range (cut by `shard_columns`).  Returns
+    the `scalars` global sums, identical on every rank and bit-identical to
+    the single-device tree over all columns."""
+    import torch
+    import torch.distributed as dist
+    local = np.ascontiguousarray(np.atleast_2d(local_chunk_sums), dtype=np.float64)
+    world = dist.get_world_size(group)
+    # ranks may hold different chunk counts: exchange the counts, then pad to the longest
+    count = torch.tensor([local.shape[1]], dtype=torch.int64)
+    counts = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+    dist.all_gather(counts, count, group=group)
+    counts = [int(c.item()) for c in counts]
+    longest = max(counts)
+    padded = np.zeros((local.shape[0], longest), dtype=np.float64)
+    padded[:, :local.shape[1]] = local
+    pieces = [torch.zeros((local.shape[0], longest), dtype=torch.float64) for _ in range(world)]
+    dist.all_gather(pieces, torch.from_numpy(padded), group=group)
+    chunk_sums = np.concatenate([p.numpy()[:, :c] for p, c in zip(pieces, counts)], axis=1)
+    out = []
+    for row in chunk_sums:
+        out.append(float(row[0]) if row.size == 1 else (0.0 if row.size == 0 else tree_sum(row)))
+    return out

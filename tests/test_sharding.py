@@ -1,0 +1,72 @@
+"""The sharded reduction of column-sharded runs: the host restatement of the
+device tree against the oracle's tree, and the exchange over 2 and 3 gloo
+ranks giving every rank the single-device value bit for bit."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from oracle import pyoracle
+from parallellocallyoptimalapproximatesparsematrixinverses_b200 import sharding
+
+
+def _values(count, seed):
+    rng = np.random.default_rng(seed)
+    return rng.standard_normal(count) * 10.0 ** rng.integers(-6, 6, count)
+
+
+@pytest.mark.parametrize("count", [0, 1, 255, 4095, 4096, 4097, 3 * 4096 + 17, 70_000])
+def test_host_tree_is_the_device_tree(count):
+    v = _values(count, count)
+    assert sharding.tree_sum(v) == pyoracle.tree_sum(v)
+    assert sharding.tree_sum(v * v) == pyoracle.tree_sum(v * v)
+
+
+@pytest.mark.parametrize("n,world", [(0, 2), (10, 4), (4096, 2), (4097, 2), (70_000, 3), (262_144, 8)])
+def test_shards_cover_the_columns_at_chunk_boundaries(n, world):
+    ranges = sharding.shard_columns(n, world)
+    assert len(ranges) == world
+    assert ranges[0][0] == 0 and ranges[-1][1] == n
+    for (a, b), (c, d) in zip(ranges, ranges[1:]):
+        assert b == c and a <= b
+    for a, _ in ranges:
+        assert a % sharding.TREE_CHUNK == 0 or a == n
+    sizes = [b - a for a, b in ranges]
+    assert max(sizes) - min(sizes) <= sharding.TREE_CHUNK or n < world * sharding.TREE_CHUNK
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _worker(rank, world, port, n, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    a, b = sharding.shard_columns(n, world)[rank]
+    # three per-column partial arrays (e.g. <Z, PrAZ>, ||PrAZ||^2, ||R||^2): this rank's columns only
+    local = np.stack([sharding.tree_chunk_sums(_values(n, seed)[a:b]) if b > a else np.zeros(0)
+                      for seed in (1, 2, 3)])
+    out[rank] = sharding.sharded_tree_sums(local)
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n,world", [(70_000, 2), (20_000, 3), (5_000, 3)])
+def test_sharded_sums_equal_the_single_device_tree(n, world):
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_worker, args=(r, world, port, n, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    want = [pyoracle.tree_sum(_values(n, seed)) for seed in (1, 2, 3)]
+    for r in range(world):
+        assert list(out[r]) == want, f"rank {r}"
