@@ -1,5 +1,5 @@
-"""Column sharding of the SPAI iteration over several GPUs: the reduction
-that keeps a sharded run bit-identical to a single-GPU run.
+"""Column sharding of the SPAI iteration over several GPUs: the exchanges
+that keep a sharded run bit-identical to a single-GPU run.
 
 Every op of the iteration except the global scalars (and the transpose of
 the drop step) is column-local, so the columns of M, R, Z and P can be split
@@ -20,6 +20,12 @@ all-gather per set of scalars.  `shard_columns` makes such a cut and
 `sharded_tree_sums` does the exchange and the upper levels (torch.distributed;
 NCCL on GPUs, gloo on the host).  `tree_chunk_sums` / `tree_sum` restate the
 device tree on the host for the upper levels.
+
+The drop step's symmetrisation 0.5 (M + M^T) needs, in every rank's columns,
+the rows of M that other ranks hold: `sharded_transpose` sends each entry to
+the rank that owns its row with one all-to-all and returns this rank's
+columns of M^T (rows ascending), device-agnostic torch code (NCCL moves
+device tensors directly, over NVLink; no multicast).
 """
 from __future__ import annotations
 
@@ -81,29 +87,77 @@ def tree_sum(values) -> float:
             return float(level[0])
 
 
-def sharded_tree_sums(local_chunk_sums, group=None):
+def sharded_tree_sums(local_chunk_sums, group=None, device=None):
     """Global tree sums from every rank's first-level chunk sums.
 
     local_chunk_sums: array of shape (scalars, chunks of this rank), the
-    chunk sums of this rank's column range (cut by `shard_columns`).  Returns
-    the `scalars` global sums, identical on every rank and bit-identical to
-    the single-device tree over all columns."""
+    chunk sums of this rank's column range (cut by `shard_columns`).  The
+    exchange runs on `device` (a CUDA device under NCCL; the host under
+    gloo).  Returns the `scalars` global sums, identical on every rank and
+    bit-identical to the single-device tree over all columns."""
     import torch
     import torch.distributed as dist
+    device = torch.device("cpu") if device is None else torch.device(device)
     local = np.ascontiguousarray(np.atleast_2d(local_chunk_sums), dtype=np.float64)
     world = dist.get_world_size(group)
     # ranks may hold different chunk counts: exchange the counts, then pad to the longest
-    count = torch.tensor([local.shape[1]], dtype=torch.int64)
-    counts = [torch.zeros(1, dtype=torch.int64) for _ in range(world)]
+    count = torch.tensor([local.shape[1]], dtype=torch.int64, device=device)
+    counts = [torch.zeros(1, dtype=torch.int64, device=device) for _ in range(world)]
     dist.all_gather(counts, count, group=group)
     counts = [int(c.item()) for c in counts]
     longest = max(counts)
     padded = np.zeros((local.shape[0], longest), dtype=np.float64)
     padded[:, :local.shape[1]] = local
-    pieces = [torch.zeros((local.shape[0], longest), dtype=torch.float64) for _ in range(world)]
-    dist.all_gather(pieces, torch.from_numpy(padded), group=group)
-    chunk_sums = np.concatenate([p.numpy()[:, :c] for p, c in zip(pieces, counts)], axis=1)
+    pieces = [torch.zeros((local.shape[0], longest), dtype=torch.float64, device=device) for _ in range(world)]
+    dist.all_gather(pieces, torch.from_numpy(padded).to(device), group=group)
+    chunk_sums = np.concatenate([p.cpu().numpy()[:, :c] for p, c in zip(pieces, counts)], axis=1)
     out = []
     for row in chunk_sums:
         out.append(float(row[0]) if row.size == 1 else (0.0 if row.size == 0 else tree_sum(row)))
     return out
+
+
+def sharded_transpose(col_offsets, row_indices, values, ranges, rank, group=None):
+    """This rank's columns [start, stop) of M^T from this rank's columns of M.
+
+    col_offsets / row_indices / values: the rank's columns of M as CSC (torch
+    tensors; offsets local, from 0, rows global); ranges: every rank's
+    (start, stop), as shard_columns gives.  Returns (col_offsets,
+    row_indices, values) of the rank's columns of M^T, rows ascending in
+    every column, on the inputs' device."""
+    import torch
+    import torch.distributed as dist
+    start, stop = ranges[rank]
+    device = values.device
+    lengths = col_offsets[1:] - col_offsets[:-1]
+    cols = torch.repeat_interleave(torch.arange(start, stop, dtype=torch.int64, device=device), lengths)
+    rows = row_indices.to(torch.int64)
+    # the owner of each entry's row, and the entries grouped by owner (stable, so column order holds)
+    starts = torch.tensor([a for a, _ in ranges[1:]], dtype=torch.int64, device=device)
+    owner = torch.bucketize(rows, starts, right=True)
+    order = torch.argsort(owner, stable=True)
+    rows, cols, vals = rows[order], cols[order], values[order]
+    world = len(ranges)
+    send_counts = torch.bincount(owner, minlength=world).to(torch.int64)
+    recv_counts = torch.empty_like(send_counts)
+    dist.all_to_all_single(recv_counts, send_counts, group=group)
+    send_splits = send_counts.tolist()
+    recv_splits = recv_counts.tolist()
+    total = int(sum(recv_splits))
+    got_rows = torch.empty(total, dtype=torch.int64, device=device)
+    got_cols = torch.empty(total, dtype=torch.int64, device=device)
+    got_vals = torch.empty(total, dtype=values.dtype, device=device)
+    dist.all_to_all_single(got_rows, rows.contiguous(), recv_splits, send_splits, group=group)
+    dist.all_to_all_single(got_cols, cols.contiguous(), recv_splits, send_splits, group=group)
+    dist.all_to_all_single(got_vals, vals.contiguous(), recv_splits, send_splits, group=group)
+    # entry (i, j) of M is entry (j, i) of M^T: column i - start, row j
+    n = int(ranges[-1][1])
+    local_col = got_rows - start
+    key = local_col * max(n, 1) + got_cols
+    order = torch.argsort(key)
+    out_rows = got_cols[order]
+    out_vals = got_vals[order]
+    counts = torch.bincount(local_col, minlength=stop - start)
+    out_ptr = torch.zeros(stop - start + 1, dtype=torch.int64, device=device)
+    out_ptr[1:] = torch.cumsum(counts, 0)
+    return out_ptr, out_rows, out_vals

@@ -70,3 +70,46 @@ def test_sharded_sums_equal_the_single_device_tree(n, world):
     want = [pyoracle.tree_sum(_values(n, seed)) for seed in (1, 2, 3)]
     for r in range(world):
         assert list(out[r]) == want, f"rank {r}"
+
+
+def _transpose_worker(rank, world, port, n, out):
+    import torch
+    import torch.distributed as dist
+    from scipy import sparse
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    m = sparse.random(n, n, density=0.01, random_state=np.random.default_rng(4), format="csc")
+    m = sparse.csc_matrix(m + sparse.identity(n))
+    m.sort_indices()
+    ranges = sharding.shard_columns(n, world, align=64)
+    a, b = ranges[rank]
+    local = m[:, a:b]
+    ptr, rows, vals = sharding.sharded_transpose(torch.tensor(local.indptr, dtype=torch.int64),
+                                                 torch.tensor(local.indices, dtype=torch.int64),
+                                                 torch.tensor(local.data, dtype=torch.float64), ranges, rank)
+    out[rank] = (ptr.numpy(), rows.numpy(), vals.numpy())
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("n,world", [(700, 2), (1000, 3)])
+def test_sharded_transpose_gives_each_rank_its_columns_of_the_transpose(n, world):
+    from scipy import sparse
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_transpose_worker, args=(r, world, port, n, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    m = sparse.random(n, n, density=0.01, random_state=np.random.default_rng(4), format="csc")
+    m = sparse.csc_matrix(m + sparse.identity(n))
+    mt = sparse.csc_matrix(m.T)
+    mt.sort_indices()
+    for r, (a, b) in enumerate(sharding.shard_columns(n, world, align=64)):
+        want = mt[:, a:b]
+        ptr, rows, vals = out[r]
+        assert np.array_equal(ptr, want.indptr) and np.array_equal(rows, want.indices)
+        assert np.array_equal(vals, want.data)
