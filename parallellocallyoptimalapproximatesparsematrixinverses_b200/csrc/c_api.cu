@@ -11,6 +11,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/methods_c_api.h"
@@ -267,6 +268,31 @@ int64_t FinishPcg(const PcgResult& r, int64_t capacity, double* history, int64_t
   return count;
 }
 
+// f(0) .. f(count - 1) on host threads (systems are independent); the error
+// of the first failing system, in system order, is the one rethrown.
+template <class F>
+void ForEachSystem(int64_t count, F f) {
+  const int64_t threads = std::min<int64_t>(count, std::max(1u, std::min(16u, std::thread::hardware_concurrency())));
+  std::vector<std::exception_ptr> errors(static_cast<size_t>(count));
+  std::atomic<int64_t> next{0};
+  auto work = [&]() {
+    for (int64_t b = next.fetch_add(1); b < count; b = next.fetch_add(1)) {
+      try {
+        f(b);
+      } catch (...) {
+        errors[b] = std::current_exception();
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  for (int64_t t = 1; t < threads; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  for (const auto& e : errors) {
+    if (e) std::rethrow_exception(e);
+  }
+}
+
 // Uploads CSR M as params ask (FP64 or FP32, optionally its symmetric part)
 // and runs PCG from x = 0 on the device vectors rhs -> x.
 void PcgOnDevice(Ctx& ctx, int64_t n, const DevCsc<double>& a, const double* m_values, const int64_t* m_indices,
@@ -426,46 +452,55 @@ int64_t spai_mr_batched(int64_t count, const MatrixData* A, const MatrixData* M0
     // validation per system, with the reference's messages (methods_c_api.cpp:16-40, methods_common.cpp:12-48)
     std::vector<spai::HostCsc> as(static_cast<size_t>(count));
     std::vector<spai::HostCsc> ms(static_cast<size_t>(count));
-    std::vector<int64_t> offsets(static_cast<size_t>(count + 1), 0);
-    int64_t nnz_a = 0;
-    int64_t nnz_m = 0;
-    for (int64_t b = 0; b < count; ++b) {
+    const bool has_m0 = params.use_initial_m != 0;
+    spai::ForEachSystem(count, [&](int64_t b) {
       as[b] = spai::CheckedMatrix(A[b]);
-      if (params.use_initial_m != 0) ms[b] = spai::CheckedMatrix(M0[b]);
-      spai::ValidateProblem(as[b], params.use_initial_m != 0 ? &ms[b] : nullptr, nullptr, params);
+      if (has_m0) ms[b] = spai::CheckedMatrix(M0[b]);
+      spai::ValidateProblem(as[b], has_m0 ? &ms[b] : nullptr, nullptr, params);
+    });
+    std::vector<int64_t> offsets(static_cast<size_t>(count + 1), 0);
+    std::vector<int64_t> a_at(static_cast<size_t>(count + 1), 0);
+    std::vector<int64_t> m_at(static_cast<size_t>(count + 1), 0);
+    for (int64_t b = 0; b < count; ++b) {
       offsets[b + 1] = offsets[b] + as[b].cols;
-      nnz_a += as[b].ptr[as[b].cols] - as[b].ptr[0];
-      if (params.use_initial_m != 0) nnz_m += ms[b].ptr[ms[b].cols] - ms[b].ptr[0];
+      a_at[b + 1] = a_at[b] + (as[b].ptr[as[b].cols] - as[b].ptr[0]);
+      if (has_m0) m_at[b + 1] = m_at[b] + (ms[b].ptr[ms[b].cols] - ms[b].ptr[0]);
     }
     const int64_t n = offsets[count];
     if (n > static_cast<int64_t>(INT32_MAX)) throw std::invalid_argument("the batch exceeds 2^31 - 1 rows in total");
-    // the block-diagonal matrices, assembled once on the host
-    auto assemble = [&](const std::vector<spai::HostCsc>& parts, int64_t nnz, std::vector<int64_t>& ptr,
-                        std::vector<int64_t>& idx, std::vector<double>& val) {
-      ptr.assign(static_cast<size_t>(n + 1), 0);
-      idx.resize(static_cast<size_t>(nnz));
-      val.resize(static_cast<size_t>(nnz));
-      int64_t at = 0;
-      for (int64_t b = 0; b < count; ++b) {
-        const spai::HostCsc& h = parts[b];
-        for (int64_t j = 0; j < h.cols; ++j) {
-          for (int64_t p = h.ptr[j]; p < h.ptr[j + 1]; ++p) {
-            idx[at] = h.idx[p] + offsets[b];
-            val[at] = h.val[p];
-            ++at;
-          }
-          ptr[offsets[b] + j + 1] = at;
-        }
-      }
+    // the block-diagonal matrices, assembled once on the host: system b's
+    // columns, rows shifted by its first column, into disjoint ranges
+    struct Assembled {
+      std::unique_ptr<int64_t[]> ptr;
+      std::unique_ptr<int64_t[]> idx;
+      std::unique_ptr<double[]> val;
     };
-    std::vector<int64_t> a_ptr, a_idx, m_ptr, m_idx;
-    std::vector<double> a_val, m_val;
-    assemble(as, nnz_a, a_ptr, a_idx, a_val);
-    spai::HostCsc big_a{n, n, nnz_a, a_ptr.data(), a_idx.data(), a_val.data()};
+    auto assemble = [&](const std::vector<spai::HostCsc>& parts, const std::vector<int64_t>& at) {
+      Assembled out;
+      const int64_t nnz = at[count];
+      out.ptr.reset(new int64_t[n + 1]);
+      out.idx.reset(new int64_t[nnz > 0 ? nnz : 1]);
+      out.val.reset(new double[nnz > 0 ? nnz : 1]);
+      out.ptr[0] = 0;
+      spai::ForEachSystem(count, [&](int64_t b) {
+        const spai::HostCsc& h = parts[b];
+        const int64_t base = h.ptr[0];
+        for (int64_t j = 0; j < h.cols; ++j) out.ptr[offsets[b] + j + 1] = at[b] + (h.ptr[j + 1] - base);
+        const int64_t count_b = h.ptr[h.cols] - base;
+        for (int64_t q = 0; q < count_b; ++q) {
+          out.idx[at[b] + q] = h.idx[base + q] + offsets[b];
+          out.val[at[b] + q] = h.val[base + q];
+        }
+      });
+      return out;
+    };
+    const Assembled big_a_arrays = assemble(as, a_at);
+    spai::HostCsc big_a{n, n, a_at[count], big_a_arrays.ptr.get(), big_a_arrays.idx.get(), big_a_arrays.val.get()};
+    Assembled big_m_arrays;
     spai::HostCsc big_m;
-    if (params.use_initial_m != 0) {
-      assemble(ms, nnz_m, m_ptr, m_idx, m_val);
-      big_m = spai::HostCsc{n, n, nnz_m, m_ptr.data(), m_idx.data(), m_val.data()};
+    if (has_m0) {
+      big_m_arrays = assemble(ms, m_at);
+      big_m = spai::HostCsc{n, n, m_at[count], big_m_arrays.ptr.get(), big_m_arrays.idx.get(), big_m_arrays.val.get()};
     }
     spai::SolveOptions opt;
     opt.method = spai::Method::kGlobalMr;
