@@ -6,9 +6,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 #include <stdexcept>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -1245,20 +1247,42 @@ std::unique_ptr<SolverBase> MakeSolver(Ctx& ctx, const SolveOptions& options) {
   return std::unique_ptr<SolverBase>(new Solver<float>(ctx, options));
 }
 
+namespace {
+// True when pred(i) holds for every i in [0, n); large ranges are split over host threads.
+template <class Pred>
+bool AllOf(int64_t n, Pred pred) {
+  const int64_t parts = n < (int64_t{1} << 20) ? 1 : std::min<int64_t>(8, std::max(1u, std::thread::hardware_concurrency()));
+  if (parts <= 1) {
+    for (int64_t i = 0; i < n; ++i) {
+      if (!pred(i)) return false;
+    }
+    return true;
+  }
+  std::atomic<bool> ok{true};
+  std::vector<std::thread> pool;
+  for (int64_t k = 0; k < parts; ++k) {
+    pool.emplace_back([&, k]() {
+      const int64_t last = n * (k + 1) / parts;
+      for (int64_t i = n * k / parts; i < last && ok.load(std::memory_order_relaxed); ++i) {
+        if (!pred(i)) ok.store(false, std::memory_order_relaxed);
+      }
+    });
+  }
+  for (auto& t : pool) t.join();
+  return ok.load();
+}
+}  // namespace
+
 HostCsc CheckedMatrix(const MatrixData& data) {
   // GetCompressedSparseMatrix (methods_c_api.cpp:16-40)
   if (data.rows <= 0 || data.cols <= 0 || data.nnz <= 0) {
     throw std::invalid_argument("Sparse matrix dimensions and nnz must be positive");
   }
-  for (int64_t i = 0; i < data.cols; ++i) {
-    if (data.col_offsets[i] > data.col_offsets[i + 1]) {
-      throw std::invalid_argument("Sparse matrix column offsets must be non-decreasing");
-    }
+  if (!AllOf(data.cols, [&](int64_t i) { return data.col_offsets[i] <= data.col_offsets[i + 1]; })) {
+    throw std::invalid_argument("Sparse matrix column offsets must be non-decreasing");
   }
-  for (int64_t i = 0; i < data.nnz; ++i) {
-    if (data.row_indices[i] < 0 || data.row_indices[i] >= data.rows) {
-      throw std::invalid_argument("Sparse matrix row idx is out of range");
-    }
+  if (!AllOf(data.nnz, [&](int64_t i) { return data.row_indices[i] >= 0 && data.row_indices[i] < data.rows; })) {
+    throw std::invalid_argument("Sparse matrix row idx is out of range");
   }
   if (data.rows > static_cast<int64_t>(std::numeric_limits<int32_t>::max()) ||
       data.cols > static_cast<int64_t>(std::numeric_limits<int32_t>::max())) {
