@@ -9,7 +9,6 @@ the oracle PCG (reference methods_cython/backward_error.pyx:69-144).
 from __future__ import annotations
 
 import ctypes
-import os
 from pathlib import Path
 
 import numpy as np

@@ -103,7 +103,6 @@ def test_validation_messages_match_reference():
     with pytest.raises(RuntimeError, match="inner_iterations must be positive"):
         inner_outer.mr(A, max_density=1.0, inner_iterations=0)
     with pytest.raises(RuntimeError, match="Initial preconditioner M0 must have the same shape as A"):
-        from parallellocallyoptimalapproximatesparsematrixinverses_b200 import _lib as L  # noqa: F401
         _raw_shape_mismatch(A)
 
 

@@ -8,7 +8,7 @@ import pytest
 from scipy import sparse
 from scipy.sparse import linalg as splinalg
 
-from oracle import adjoint_oracle, pyoracle
+from oracle import adjoint_oracle
 from parallellocallyoptimalapproximatesparsematrixinverses_b200 import _lib, adjoint, problems
 from tests.conftest import cuda_available
 
