@@ -17,6 +17,7 @@ its recorded results bit for bit in FP64).
 from __future__ import annotations
 
 import ctypes
+from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
 from scipy import sparse
@@ -198,14 +199,17 @@ class GlobalSpaiMethods:
         for that system alone with Pr = diag(A)^-1.  Dropping, when enabled,
         must be per column (topk_per_column > 0)."""
         lib = _lib.load()
-        As = [as_csc(A) for A in As]
+        As = list(As)
         count = len(As)
         if count == 0:
             return []
-        if M0s is not None:
-            if len(M0s) != count:
-                raise ValueError("M0s must have one matrix per system")
-            M0s = [as_csc(M, A.shape) for M, A in zip(M0s, As)]
+        if M0s is not None and len(M0s) != count:
+            raise ValueError("M0s must have one matrix per system")
+        # canonical int64 CSC per system; numpy's copies release the GIL, so large batches convert on threads
+        with ThreadPoolExecutor(max_workers=min(8, count)) as pool:
+            As = list(pool.map(as_csc, As))
+            if M0s is not None:
+                M0s = list(pool.map(lambda pair: as_csc(pair[0], pair[1].shape), zip(M0s, As)))
         params = _lib.MethodParams(max_iterations, tolerance, max_density, 1 if enable_dropping else 0, num_threads,
                                    1 if M0s is not None else 0, 0, 2)
         ext = ext_params(precision, topk_per_column, device)
