@@ -21,6 +21,13 @@ all-gather per set of scalars.  `shard_columns` makes such a cut and
 NCCL on GPUs, gloo on the host).  `tree_chunk_sums` / `tree_sum` restate the
 device tree on the host for the upper levels.
 
+The global budget's drop selects the `drop` smallest (score, offset) keys
+over all candidates by a 16-pass radix select (ops.cu, RadixHistKernel /
+RadixDecideKernel).  Sharded, each rank histograms its own candidates and
+one all-reduce of the 256 bins per pass gives every rank the same digit:
+`sharded_drop_cutoff` restates that select with the exchange, offsets being
+the candidates' global column-major positions (rank order = column order).
+
 The drop step's symmetrisation 0.5 (M + M^T) needs, in every rank's columns,
 the rows of M that other ranks hold: `sharded_transpose` sends each entry to
 the rank that owns its row with one all-to-all and returns this rank's
@@ -161,3 +168,51 @@ def sharded_transpose(col_offsets, row_indices, values, ranges, rank, group=None
     out_ptr = torch.zeros(stop - start + 1, dtype=torch.int64, device=device)
     out_ptr[1:] = torch.cumsum(counts, 0)
     return out_ptr, out_rows, out_vals
+
+
+def ordered_bits(scores) -> np.ndarray:
+    """The order-preserving unsigned image of FP64 scores (ops.cu OrderedBits):
+    -0.0 and +0.0 map alike, and unsigned order equals numeric order."""
+    v = np.ascontiguousarray(scores, dtype=np.float64).copy()
+    v[v == 0.0] = 0.0
+    u = v.view(np.uint64)
+    negative = (u >> np.uint64(63)) == np.uint64(1)
+    return np.where(negative, ~u, u | np.uint64(1 << 63))
+
+
+def sharded_drop_cutoff(keys, offset_base: int, drop: int, group=None, device=None):
+    """The cutoff (score bits, offset) of the `drop` smallest keys over all
+    ranks: keys are this rank's ordered score bits (ordered_bits), its
+    candidates holding global offsets offset_base, offset_base + 1, ...  Every
+    rank returns the same pair; a candidate is dropped iff its (bits, offset)
+    <= the cutoff, as on one GPU."""
+    import torch
+    import torch.distributed as dist
+    device = torch.device("cpu") if device is None else torch.device(device)
+    hi = np.ascontiguousarray(keys, dtype=np.uint64)
+    lo = np.arange(offset_base, offset_base + hi.size, dtype=np.uint64)
+    prefix_hi = np.uint64(0)
+    prefix_lo = np.uint64(0)
+    remaining = int(drop)
+    for step in range(16):
+        shift = np.uint64(56 - 8 * (step % 8))
+        if step < 8:
+            mask = np.uint64(0) if step == 0 else np.uint64((0xFFFFFFFFFFFFFFFF << (int(shift) + 8)) & 0xFFFFFFFFFFFFFFFF)
+            match = (hi & mask) == (prefix_hi & mask)
+            digits = ((hi[match] >> shift) & np.uint64(0xFF)).astype(np.int64)
+        else:
+            mask = np.uint64(0) if step == 8 else np.uint64((0xFFFFFFFFFFFFFFFF << (int(shift) + 8)) & 0xFFFFFFFFFFFFFFFF)
+            match = (hi == prefix_hi) & ((lo & mask) == (prefix_lo & mask))
+            digits = ((lo[match] >> shift) & np.uint64(0xFF)).astype(np.int64)
+        local = torch.from_numpy(np.bincount(digits, minlength=256).astype(np.int64)).to(device)
+        dist.all_reduce(local, group=group)
+        hist = local.cpu().numpy()
+        cumulative = np.cumsum(hist)
+        digit = int(np.searchsorted(cumulative, remaining))  # first bin whose running count reaches the rank
+        below = int(cumulative[digit - 1]) if digit > 0 else 0
+        if step < 8:
+            prefix_hi |= np.uint64(digit) << shift
+        else:
+            prefix_lo |= np.uint64(digit) << shift
+        remaining -= below
+    return int(prefix_hi), int(prefix_lo)

@@ -113,3 +113,53 @@ def test_sharded_transpose_gives_each_rank_its_columns_of_the_transpose(n, world
         ptr, rows, vals = out[r]
         assert np.array_equal(ptr, want.indptr) and np.array_equal(rows, want.indices)
         assert np.array_equal(vals, want.data)
+
+
+def _scores(total, seed):
+    rng = np.random.default_rng(seed)
+    s = rng.standard_normal(total) * 10.0 ** rng.integers(-3, 3, total)
+    s[rng.integers(0, total, total // 10)] = 0.0          # ties at zero
+    s[rng.integers(0, total, total // 20)] = -0.0
+    s[rng.integers(0, total, total // 50)] = -np.inf      # non-finite scores map to -inf
+    s[rng.integers(0, total, total // 10)] = 1.5           # more ties
+    return s
+
+
+def _select_worker(rank, world, port, total, drop, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    bounds = [total * r // world for r in range(world + 1)]
+    scores = _scores(total, 9)[bounds[rank]:bounds[rank + 1]]
+    out[rank] = sharding.sharded_drop_cutoff(sharding.ordered_bits(scores), bounds[rank], drop)
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("total,drop,world", [(5_000, 1, 2), (5_000, 2_500, 3), (20_011, 19_000, 2),
+                                              (20_011, 20_011, 3)])
+def test_sharded_drop_cutoff_is_the_single_device_select(total, drop, world):
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    procs = [ctx.Process(target=_select_worker, args=(r, world, port, total, drop, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    bits = sharding.ordered_bits(_scores(total, 9))
+    order = np.lexsort((np.arange(total), bits))  # by (bits, offset)
+    want = (int(bits[order[drop - 1]]), int(order[drop - 1]))
+    for r in range(world):
+        assert tuple(out[r]) == want, f"rank {r}"
+    # exactly `drop` candidates lie at or below the cutoff
+    keys = [(int(b), i) for i, b in enumerate(bits)]
+    assert sum(1 for k in keys if k <= want) == drop
+
+
+def test_ordered_bits_preserve_the_order():
+    v = np.array([-np.inf, -1e300, -2.0, -1e-300, -0.0, 0.0, 1e-300, 3.0, 1e300, np.inf])
+    bits = sharding.ordered_bits(v)
+    assert all(bits[i] <= bits[i + 1] for i in range(len(v) - 1))
+    assert bits[4] == bits[5]
