@@ -88,8 +88,10 @@ enum {
 };
 
 /* One call of any method with the extension knobs; ext may be NULL (FP64,
- * global budget, current device).  Replaces the five reference entry points
- * of methods_c_api.h:48-56 (same inputs, same Result ownership via free_mem). */
+ * global budget, current device and the reference's summation order: what the
+ * five methods_c_api.h entry points run, bit for bit the reference's results).
+ * Replaces the five reference entry points of methods_c_api.h:48-56 (same
+ * inputs, same Result ownership via free_mem). */
 struct Result spai_run_ex(int64_t method, struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
                           struct MethodParams params, const SpaiExtParams* ext);
 
@@ -137,14 +139,17 @@ int64_t spai_pcg(int64_t n, const double* a_values, const int64_t* a_indices, co
  *   (x is overwritten, x0 = 0); history: max_iterations host doubles.
  *   stream: the cudaStream_t to run on (NULL: the default stream).
  * Work vectors live in a fixed device array inside the library (16 MiB), so
- * n is limited to 524,288 rows; larger n returns -1 with an error.  The
- * array's address is looked up on the first call on each device, so make
- * that first call before any stream capture on the device.  Calls that
+ * n is limited to 524,288 rows; larger n returns -1 with an error.  Every
+ * call looks up the array's device address in the current context; the
+ * first call on a device can load the library's device code there, so make
+ * that first call before any stream capture on the device.  The call is
+ * host-synchronous: it returns when the solve is done, and waits for the
+ * stream about three times per iteration to read scalars back.  Calls that
  * overlap on one GPU share the array and race: serialise them per device.
- * Pointers are checked (device memory of the current device, long enough),
- * offsets and indices are checked on the device.  Returns the number of
- * history entries and sets *status as spai_pcg does; -1 with `error` on
- * invalid input or CUDA failure. */
+ * Pointers are checked (device memory of the current device, long enough;
+ * x must not overlap b, A or M), offsets and indices are checked on the
+ * device.  Returns the number of history entries and sets *status as
+ * spai_pcg does; -1 with `error` on invalid input or CUDA failure. */
 int64_t spai_pcg_device_noalloc(int64_t n, int64_t a_nnz, const double* a_values, const int32_t* a_indices,
                                 const int64_t* a_offsets, int64_t m_nnz, const double* m_values,
                                 const int32_t* m_indices, const int64_t* m_offsets, const double* b, double* x,

@@ -148,6 +148,11 @@ SolveOptions ParseOptions(int64_t method, const MethodParams& params, const Spai
   opt.dropping = params.enable_dropping != 0;
   opt.inner_iterations = params.inner_iterations;
   opt.num_threads = params.num_threads;
+  // Without extension knobs (the five methods_c_api.h entry points, or ext ==
+  // NULL) a run is the reference's: FP64, global budget, and its summation
+  // order over min(n, num_threads) column batches, so the drop-in returns the
+  // reference's bits.
+  opt.summation = 1;
   if (ext != nullptr) {
     if (ext->precision != 0 && ext->precision != 1) throw std::invalid_argument("precision must be 0 (FP64) or 1 (mixed)");
     if (ext->topk_per_column < 0) throw std::invalid_argument("topk_per_column must be non-negative");

@@ -11,17 +11,23 @@
 // How it allocates nothing: the four work vectors (r, z, p, A p), the
 // first-level sums of the dot-product tree and the status word live in one
 // fixed array in the library's device data (g_noalloc_scratch below,
-// 16 MiB + 1.1 KiB), which the CUDA module carries.  Its address is looked up
-// once per device, on the first call with that device current
-// (cudaGetSymbolAddress); that first call can load the library's device code
-// on the device and so must come before any stream capture on it.  Problems
-// with more than kNoAllocMaxRows rows are rejected with an error.  The host
-// side uses only stack memory and the caller's buffers; scalars come back
-// through plain device-to-host copies into stack variables.
+// 16 MiB + 1.1 KiB), which the CUDA module carries.  In host code the array's
+// name is only a host-side stand-in, so every call asks the runtime for the
+// array's device address in the current context (cudaGetSymbolAddress, a
+// table lookup once the module is loaded).  Asking on every call, instead of
+// caching the address per device ordinal, keeps the address right after
+// cudaDeviceReset or when the caller makes another context current.  The
+// first call on a device can load the library's device code there and so
+// must come before any stream capture on it.  Problems with more than
+// kNoAllocMaxRows rows are rejected with an error.  The host side uses only
+// stack memory and the caller's buffers; scalars come back through plain
+// device-to-host copies into stack variables, so the call is
+// host-synchronous: it waits for the stream about three times per iteration.
 //
 // Calls share the one scratch array per device: two calls that overlap on the
 // same GPU (different streams, or different host threads) race and corrupt
-// each other's vectors.  Serialise calls per device.
+// each other's vectors.  Serialise calls per device.  x must not overlap b,
+// A or M (x is cleared before r = b is formed); such calls are rejected.
 //
 // The arithmetic is that of spai_pcg with FP64 M (pcg.cu, the reference's
 // methods_cython/backward_error.pyx:69-144): per-row sequential SpMV, the
@@ -60,8 +66,7 @@ static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
-double* g_scratch_of_device[kMaxDevices] = {};
-int g_sm_count_of_device[kMaxDevices] = {};
+int g_sm_count_of_device[kMaxDevices] = {};  // 0 until the device's first call
 
 // Status bits written by the input check.
 constexpr unsigned long long kBadA = 1ull;
@@ -221,19 +226,25 @@ struct NoAllocRun {
   }
 };
 
-// cuMemGetAddressRange, fetched through the runtime (null when unavailable).
+// cuMemGetAddressRange, fetched through the runtime once per process (null
+// when unavailable); resolved under std::call_once before any reader sees it.
 using AddressRangeFn = CUresult (*)(CUdeviceptr*, size_t*, CUdeviceptr);
 AddressRangeFn g_address_range = nullptr;
+std::once_flag g_address_range_once;
 
-void LookUpAddressRange() {
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
-  if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &found) == cudaSuccess &&
-      found == cudaDriverEntryPointSuccess) {
-    g_address_range = reinterpret_cast<AddressRangeFn>(fn);
-  } else {
-    cudaGetLastError();
-  }
+AddressRangeFn AddressRange() {
+  std::call_once(g_address_range_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult found = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &found) ==
+            cudaSuccess &&
+        found == cudaDriverEntryPointSuccess) {
+      g_address_range = reinterpret_cast<AddressRangeFn>(fn);
+    } else {
+      cudaGetLastError();
+    }
+  });
+  return g_address_range;
 }
 
 // True when [ptr, ptr + bytes) is device (or managed) memory usable on
@@ -254,10 +265,11 @@ bool CheckDeviceExtent(const void* ptr, size_t bytes, int device, const char* na
     SetError(error, capacity, "%s lives on device %d but device %d is current", name, attr.device, device);
     return false;
   }
-  if (g_address_range != nullptr) {
+  const AddressRangeFn address_range = AddressRange();
+  if (address_range != nullptr) {
     CUdeviceptr base = 0;
     size_t size = 0;
-    if (g_address_range(&base, &size, reinterpret_cast<CUdeviceptr>(ptr)) != CUDA_SUCCESS) {
+    if (address_range(&base, &size, reinterpret_cast<CUdeviceptr>(ptr)) != CUDA_SUCCESS) {
       SetError(error, capacity, "the allocation holding %s is unknown to the driver", name);
       return false;
     }
@@ -269,29 +281,39 @@ bool CheckDeviceExtent(const void* ptr, size_t bytes, int device, const char* na
   return true;
 }
 
-// The scratch address on the current device, set up on the device's first call.
+// The scratch array's device address in the current context, looked up on
+// every call (never cached: a cached address goes stale when the context is
+// reset or replaced), and the device's SM count, read on its first call.
 double* ScratchOfDevice(int device, int* sm_count, char* error, int64_t capacity) {
+  void* address = nullptr;
+  cudaError_t err = cudaGetSymbolAddress(&address, g_noalloc_scratch);
+  if (err != cudaSuccess || address == nullptr) {
+    cudaGetLastError();
+    SetError(error, capacity, "CUDA error: %s (cudaGetSymbolAddress of the no-alloc scratch)",
+             cudaGetErrorString(err));
+    return nullptr;
+  }
   std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (g_scratch_of_device[device] == nullptr) {
-    void* address = nullptr;
-    cudaError_t err = cudaGetSymbolAddress(&address, g_noalloc_scratch);
-    if (err != cudaSuccess || address == nullptr) {
-      SetError(error, capacity, "CUDA error: %s (cudaGetSymbolAddress of the no-alloc scratch)",
-               cudaGetErrorString(err));
-      return nullptr;
-    }
+  if (g_sm_count_of_device[device] == 0) {
     int sms = 0;
     err = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (err != cudaSuccess) {
+    if (err != cudaSuccess || sms <= 0) {
+      cudaGetLastError();
       SetError(error, capacity, "CUDA error: %s (multiprocessor count)", cudaGetErrorString(err));
       return nullptr;
     }
-    if (g_address_range == nullptr) LookUpAddressRange();
     g_sm_count_of_device[device] = sms;
-    g_scratch_of_device[device] = static_cast<double*>(address);
   }
   *sm_count = g_sm_count_of_device[device];
-  return g_scratch_of_device[device];
+  return static_cast<double*>(address);
+}
+
+// True when the byte ranges [a, a + a_bytes) and [b, b + b_bytes) share a byte.
+bool Overlaps(const void* a, size_t a_bytes, const void* b, size_t b_bytes) {
+  if (a == nullptr || b == nullptr || a_bytes == 0 || b_bytes == 0) return false;
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(a);
+  const uintptr_t b0 = reinterpret_cast<uintptr_t>(b);
+  return a0 < b0 + b_bytes && b0 < a0 + a_bytes;
 }
 
 int GridOf(int64_t items, int threads, int sm_count) {
@@ -365,6 +387,24 @@ extern "C" int64_t spai_pcg_device_noalloc(int64_t n, int64_t a_nnz, const doubl
       !CheckDeviceExtent(b, vec, device, "b", error, error_capacity) ||
       !CheckDeviceExtent(x, vec, device, "x", error, error_capacity)) {
     return -1;
+  }
+  // x is cleared before r = b is formed and written every iteration: it must alias no input
+  const struct {
+    const void* ptr;
+    size_t bytes;
+    const char* name;
+  } inputs[] = {{b, vec, "b"},
+                {a_offsets, offs, "a_offsets"},
+                {a_indices, sizeof(int32_t) * static_cast<size_t>(a_nnz), "a_indices"},
+                {a_values, sizeof(double) * static_cast<size_t>(a_nnz), "a_values"},
+                {m_offsets, offs, "m_offsets"},
+                {m_indices, sizeof(int32_t) * static_cast<size_t>(m_nnz), "m_indices"},
+                {m_values, sizeof(double) * static_cast<size_t>(m_nnz), "m_values"}};
+  for (const auto& in : inputs) {
+    if (Overlaps(x, vec, in.ptr, in.bytes)) {
+      SetError(error, error_capacity, "x overlaps %s: x must not alias any input", in.name);
+      return -1;
+    }
   }
 
   // SpMV launches use 128 threads per block, the vector updates 256

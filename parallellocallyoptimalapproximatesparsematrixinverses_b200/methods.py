@@ -12,7 +12,11 @@ as the reference.  Extra keyword arguments select the device-only forms:
 precision ("fp64" | "mixed"), topk_per_column (0 = the reference's global budget),
 device (CUDA ordinal, -1 = current) and summation ("device" | "reference": the
 reference's num_threads column batches and summation order, which reproduces
-its recorded results bit for bit in FP64).
+its recorded results bit for bit in FP64).  Left unset, summation follows the
+precision: an FP64 run with the reference's global budget (no top-k) uses the
+reference's order, so a call with only the reference's arguments returns the
+reference's bits; the extension forms (mixed precision, per-column top-k) use
+the device order.
 """
 from __future__ import annotations
 
@@ -150,10 +154,18 @@ def ext_params(precision="fp64", topk_per_column=0, device=-1, summation="device
     return _lib.SpaiExtParams(PRECISIONS[precision], int(topk_per_column), int(device), SUMMATIONS[summation])
 
 
+def default_summation(precision="fp64", topk_per_column=0) -> str:
+    """The summation order of a run that does not name one: the reference's
+    for its own form (FP64, global budget), the device order otherwise."""
+    return "reference" if precision == "fp64" and not topk_per_column else "device"
+
+
 def _call_method(family, name, A, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
                  inner_iterations=2, precision="fp64", topk_per_column=0, device=-1,
-                 summation="device") -> OutputResult:
+                 summation=None) -> OutputResult:
     """methods.pyx:147-179 plus the extension knobs."""
+    if summation is None:
+        summation = default_summation(precision, topk_per_column)
     lib = _lib.load()
     A_csc = as_csc(A)
     M0_csc = as_csc(M0, A_csc.shape) if M0 is not None else _empty_csc()
@@ -161,8 +173,8 @@ def _call_method(family, name, A, M0, Pr, max_iterations, tolerance, max_density
     params = method_params(A_csc, M0, Pr, max_iterations, tolerance, max_density, enable_dropping, num_threads,
                            inner_iterations)
     method_id = _lib.METHOD_IDS[(family, name)]
-    if precision == "fp64" and not topk_per_column and device == -1 and summation == "device":
-        # the reference's own entry points (methods_c_api.h:48-56)
+    if precision == "fp64" and not topk_per_column and device == -1 and summation == "reference":
+        # the reference's own entry points (methods_c_api.h:48-56), which run in its summation order
         entry = {0: lib.spai_global_cg, 1: lib.spai_global_mr, 2: lib.spai_global_lomr,
                  3: lib.inner_outer_mr, 4: lib.inner_outer_lomr}[method_id]
         result = entry(matrix_data(A_csc), matrix_data(M0_csc), matrix_data(Pr_csc), params)

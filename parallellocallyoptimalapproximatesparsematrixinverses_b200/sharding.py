@@ -185,11 +185,18 @@ def sharded_drop_cutoff(keys, offset_base: int, drop: int, group=None, device=No
     ranks: keys are this rank's ordered score bits (ordered_bits), its
     candidates holding global offsets offset_base, offset_base + 1, ...  Every
     rank returns the same pair; a candidate is dropped iff its (bits, offset)
-    <= the cutoff, as on one GPU."""
+    <= the cutoff, as on one GPU.  Raises ValueError on every rank unless
+    0 < drop <= the number of candidates over all ranks (the device select's
+    own check), so that no rank enters the radix passes alone."""
     import torch
     import torch.distributed as dist
     device = torch.device("cpu") if device is None else torch.device(device)
     hi = np.ascontiguousarray(keys, dtype=np.uint64)
+    count = torch.tensor([hi.size], dtype=torch.int64, device=device)
+    dist.all_reduce(count, group=group)
+    total = int(count.item())
+    if not 0 < int(drop) <= total:
+        raise ValueError(f"drop count {int(drop)} must lie in [1, {total}] (the candidates over all ranks)")
     lo = np.arange(offset_base, offset_base + hi.size, dtype=np.uint64)
     prefix_hi = np.uint64(0)
     prefix_lo = np.uint64(0)

@@ -17,7 +17,7 @@ FAMILIES = {"global_spai": global_spai, "inner_outer": inner_outer}
 def _run_both(family, name, A, M0, Pr, topk=0, **kw):
     method = getattr(FAMILIES[family], name)
     ext = {"topk_per_column": topk} if topk else {}
-    got = method(A, M0=M0, Pr=Pr, **kw, **ext)
+    got = method(A, M0=M0, Pr=Pr, summation="device", **kw, **ext)
     want = pyoracle.run(family, name, A, M0=M0, Pr=Pr, order=pyoracle.ORDER_DEVICE, topk_per_column=topk, **kw)
     return got, want
 

@@ -1,8 +1,10 @@
-"""The device library in the reference's summation order (summation=
-"reference": num_threads column batches, sums sequential through each batch)
-replays the reference's own recorded runs -- the per-iteration ||R||_F of
-scripts/results/results_sample, 17 significant digits -- bit for bit, and
-matches the oracle in the reference order on further cases."""
+"""The device library in the reference's summation order (num_threads column
+batches, sums sequential through each batch) replays the reference's own
+recorded runs -- the per-iteration ||R||_F of scripts/results/results_sample,
+17 significant digits -- bit for bit, and matches the oracle in the reference
+order on further cases.  A call with only the reference's arguments goes
+through the five methods_c_api.h entry points, which run in this order by
+default: the replays below use exactly that drop-in path."""
 import json
 from pathlib import Path
 
@@ -54,7 +56,8 @@ def test_device_replays_the_recorded_histories(require_gpu, entry, label, expect
               enable_dropping=entry["enable_dropping"], num_threads=entry["requested_threads"])
     if family == "inner_outer":
         kw["inner_iterations"] = inner
-    got = getattr(FAMILIES[family], name)(A, summation="reference", **kw).history["residual_norm"]
+    # no extension keyword: the reference's own C entry point (spai_global_cg, ...), default order
+    got = getattr(FAMILIES[family], name)(A, **kw).history["residual_norm"]
     want = np.array(expected[:rows])
     assert len(got) >= len(want), f"history shorter than the recording: {len(got)} < {len(want)}"
     assert np.array_equal(got[:rows].view(np.int64), want.view(np.int64)), (
@@ -62,11 +65,14 @@ def test_device_replays_the_recorded_histories(require_gpu, entry, label, expect
 
 
 @pytest.mark.parametrize("family,name", METHODS)
-@pytest.mark.parametrize("threads", [1, 7])
-def test_reference_order_matches_the_oracle(require_gpu, family, name, threads):
+@pytest.mark.parametrize("threads,summation", [(1, "reference"), (7, "reference"), (1, None), (5, None)])
+def test_reference_order_matches_the_oracle(require_gpu, family, name, threads, summation):
     A = problems.diffusion_2d(14, 1.0, 6)
     kw = dict(max_iterations=8, tolerance=1e-12, max_density=0.02, num_threads=threads)
-    got = getattr(FAMILIES[family], name)(A, M0=problems.diagonal_inverse(A), summation="reference", **kw)
+    if summation is not None:
+        kw["summation"] = summation  # spai_run_ex; without it the reference's own entry point runs
+    got = getattr(FAMILIES[family], name)(A, M0=problems.diagonal_inverse(A), **kw)
+    kw.pop("summation", None)
     want = pyoracle.run(family, name, A, M0=problems.diagonal_inverse(A), order=pyoracle.ORDER_REFERENCE,
                         omp_threads=2, **kw)
     assert_same_result(got, want, f"{family}.{name} threads={threads}")

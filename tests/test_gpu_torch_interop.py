@@ -30,7 +30,8 @@ def test_device_session_matches_host_entry_points(require_gpu, family, name, pre
     import torch
     A = problems.diffusion_2d(18, 1.0, 3)
     M0 = problems.diagonal_inverse(A)
-    kw = dict(max_iterations=6, tolerance=1e-12, max_density=0.05, precision=precision, topk_per_column=topk)
+    kw = dict(max_iterations=6, tolerance=1e-12, max_density=0.05, precision=precision, topk_per_column=topk,
+              summation="device")
     want = getattr(FAMILIES[family], name)(A, M0=M0, **kw)
     s = Session.from_torch(family, name, _torch_csc(torch, A), M0=_torch_csc(torch, M0), **kw)
     iterations, nnz = s.run()

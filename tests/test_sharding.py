@@ -158,6 +158,43 @@ def test_sharded_drop_cutoff_is_the_single_device_select(total, drop, world):
     assert sum(1 for k in keys if k <= want) == drop
 
 
+def _bad_drop_worker(rank, world, port, total, out):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    bounds = [total * r // world for r in range(world + 1)]
+    bits = sharding.ordered_bits(_scores(total, 9)[bounds[rank]:bounds[rank + 1]])
+    messages = []
+    for drop in (0, -3, total + 1):
+        try:
+            sharding.sharded_drop_cutoff(bits, bounds[rank], drop)
+            messages.append(None)
+        except ValueError as err:
+            messages.append(str(err))
+    # the group is still usable: a valid select afterwards agrees on every rank
+    messages.append(sharding.sharded_drop_cutoff(bits, bounds[rank], total))
+    out[rank] = messages
+    dist.destroy_process_group()
+
+
+def test_sharded_drop_cutoff_rejects_drop_counts_outside_the_candidates():
+    ctx = mp.get_context("spawn")
+    manager = ctx.Manager()
+    out = manager.dict()
+    port = _free_port()
+    total, world = 3_001, 2
+    procs = [ctx.Process(target=_bad_drop_worker, args=(r, world, port, total, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=180)
+        assert p.exitcode == 0
+    for r in range(world):
+        bad = out[r][:3]
+        assert all(m is not None and "[1, 3001]" in m for m in bad), bad
+    assert out[0][3] == out[1][3]
+
+
 def test_ordered_bits_preserve_the_order():
     v = np.array([-np.inf, -1e300, -2.0, -1e-300, -0.0, 0.0, 1e-300, 3.0, 1e300, np.inf])
     bits = sharding.ordered_bits(v)

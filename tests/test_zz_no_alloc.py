@@ -7,6 +7,12 @@ pass alone in a fresh process.  Both entry points compute the same bits, so
 the tolerance is zero.
 """
 import ctypes
+import json
+import os
+import subprocess
+import sys
+import textwrap
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -123,8 +129,85 @@ def test_noalloc_rejects_host_pointers_and_bad_csr(require_gpu):
     bad_idx[5] = a.shape[0] + 3
     assert call((a_dev[0], a_dev[1], bad_idx, a_dev[3]), b_dev.data_ptr()) == -1
     assert b"malformed CSR input (A)" in err.value
+    # x may not alias an input: x is cleared before r = b is formed
+    alias = lib.spai_pcg_device_noalloc(a.shape[0], a_dev[0], a_dev[1].data_ptr(), a_dev[2].data_ptr(),
+                                        a_dev[3].data_ptr(), m_dev[0], m_dev[1].data_ptr(), m_dev[2].data_ptr(),
+                                        m_dev[3].data_ptr(), b_dev.data_ptr(), b_dev.data_ptr(), 10, 1e-8, 0, None,
+                                        history.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(status),
+                                        err, len(err))
+    assert alias == -1
+    assert b"x overlaps b" in err.value
     # the valid call still works afterwards
     assert call(a_dev, b_dev.data_ptr()) > 1, err.value.decode()
+
+
+# A child process without torch: the runtime's own allocator holds the
+# buffers, so that cudaDeviceReset (which ends this process's context on the
+# device) leaves no other library state behind.  Only the no-alloc entry
+# point runs, before and after the reset.
+_RESET_CHILD = textwrap.dedent("""
+    import ctypes, json, sys
+    import numpy as np
+    from scipy import sparse
+    sys.path.insert(0, sys.argv[1])
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import _lib, problems
+    lib = _lib.load()
+    rt = ctypes.CDLL("libcudart.so.12")
+    def ok(rc, what):
+        if rc != 0:
+            raise SystemExit(f"{what}: cuda error {rc}")
+    ok(rt.cudaSetDevice(0), "cudaSetDevice")
+    a = sparse.csr_matrix(problems.diffusion_3d(24, 1.0, 2))
+    a.sort_indices()
+    d = sparse.diags(1.0 / np.sqrt(a.diagonal()))
+    m = sparse.csr_matrix(d @ (2.0 * sparse.identity(a.shape[0]) - d @ a @ d) @ d)
+    m.sum_duplicates()
+    m.sort_indices()
+    b, _ = problems.solution_rhs(a, seed=5)
+    n = a.shape[0]
+    def upload(arr):
+        arr = np.ascontiguousarray(arr)
+        ptr = ctypes.c_void_p()
+        ok(rt.cudaMalloc(ctypes.byref(ptr), ctypes.c_size_t(max(arr.nbytes, 8))), "cudaMalloc")
+        ok(rt.cudaMemcpy(ptr, arr.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(arr.nbytes), 1), "H2D")
+        return ptr
+    def solve():
+        bufs = [upload(x) for x in (a.data, a.indices.astype(np.int32), a.indptr.astype(np.int64), m.data,
+                                    m.indices.astype(np.int32), m.indptr.astype(np.int64), b, np.zeros(n))]
+        history = np.full(300, np.nan)
+        status = ctypes.c_int64(-7)
+        err = ctypes.create_string_buffer(512)
+        count = lib.spai_pcg_device_noalloc(n, a.nnz, bufs[0], bufs[1], bufs[2], m.nnz, bufs[3], bufs[4], bufs[5],
+                                            bufs[6], bufs[7], 300, 1e-9, 11, None,
+                                            history.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                                            ctypes.byref(status), err, len(err))
+        if count < 0:
+            raise SystemExit("noalloc: " + err.value.decode())
+        x = np.empty(n)
+        ok(rt.cudaMemcpy(x.ctypes.data_as(ctypes.c_void_p), bufs[7], ctypes.c_size_t(x.nbytes), 2), "D2H")
+        for ptr in bufs:
+            ok(rt.cudaFree(ptr), "cudaFree")
+        return history[:count], int(status.value), x
+    h1, s1, x1 = solve()
+    ok(rt.cudaDeviceReset(), "cudaDeviceReset")
+    ok(rt.cudaSetDevice(0), "cudaSetDevice")
+    h2, s2, x2 = solve()
+    print(json.dumps({"len": len(h1), "status": [s1, s2],
+                      "same_history": bool(np.array_equal(h1.view(np.int64), h2.view(np.int64))),
+                      "same_x": bool(np.array_equal(x1.view(np.int64), x2.view(np.int64)))}))
+""")
+
+
+@pytest.mark.gpu
+def test_noalloc_after_device_reset_gives_the_same_bits(require_gpu):
+    root = Path(__file__).resolve().parents[1]
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES=os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0])
+    proc = subprocess.run([sys.executable, "-c", _RESET_CHILD, str(root)], capture_output=True, text=True,
+                          timeout=300, env=env)
+    assert proc.returncode == 0, proc.stdout + proc.stderr
+    out = json.loads(proc.stdout.strip().splitlines()[-1])
+    assert out["len"] > 2 and out["status"][0] == out["status"][1] == 1, out
+    assert out["same_history"] and out["same_x"], out
 
 
 def test_noalloc_rejects_oversize_before_touching_the_device():
