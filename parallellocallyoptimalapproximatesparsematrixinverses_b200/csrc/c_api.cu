@@ -31,6 +31,8 @@ std::atomic<int64_t> g_fail_after{-1};
 }  // namespace
 
 void CountLaunch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// Kernel nodes executed by a graph launch.
+void CountLaunches(int64_t count) { g_launches.fetch_add(count, std::memory_order_relaxed); }
 
 bool AllocationFailureInjected() {
   if (g_fail_after.load(std::memory_order_relaxed) < 0) return false;

@@ -18,6 +18,7 @@
 #include "device.cuh"
 #include "ops.cuh"
 #include "profile.cuh"
+#include "tree.cuh"
 
 namespace spai {
 
@@ -26,9 +27,6 @@ namespace {
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 constexpr int64_t kScanTile = kScanThreads * kScanItems;
-
-constexpr int kTreeLanes = 256;
-constexpr int64_t kTreeChunk = 4096;
 
 constexpr double kDblEps = 2.220446049250313080847e-16;
 
@@ -109,26 +107,8 @@ struct TreeArgs {
   const double* src2[8];  // when set, level-one terms are src[i] * src2[i]
 };
 
-// The lanes' partial sums of one chunk -> the chunk's sum: a butterfly over
-// the kTreeLanes threads of the block (every thread returns the sum).
-__device__ __forceinline__ double ChunkButterfly(double s, double* shared) {
-  const int t = threadIdx.x;
-  shared[t] = s;
-  __syncthreads();
-#pragma unroll
-  for (int stride = kTreeLanes / 2; stride >= kWarp; stride >>= 1) {
-    const double other = shared[t ^ stride];
-    __syncthreads();
-    s = Add(s, other);
-    shared[t] = s;
-    __syncthreads();
-  }
-#pragma unroll
-  for (int stride = kWarp / 2; stride >= 1; stride >>= 1) {
-    s = Add(s, __shfl_xor_sync(0xffffffffu, s, stride));
-  }
-  return s;
-}
+// The lanes' partial sums of one chunk -> the chunk's sum (tree.cuh).
+__device__ __forceinline__ double ChunkButterfly(double s, double* shared) { return TreeButterfly(s, shared); }
 
 __global__ void TreeChunkKernel(TreeArgs args, int64_t n, double* __restrict__ out, int64_t out_stride) {
   __shared__ double shared[kTreeLanes];
