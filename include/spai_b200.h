@@ -59,6 +59,21 @@ struct Result {
 };
 #endif
 
+/* The reference's five entry points and free_mem (reference
+ * include/methods_c_api.h:48-58), repeated so that C callers can use this
+ * header alone; identical redeclarations of methods_c_api.h's. */
+struct Result spai_global_cg(struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                             struct MethodParams params);
+struct Result spai_global_mr(struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                             struct MethodParams params);
+struct Result spai_global_lomr(struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                               struct MethodParams params);
+struct Result inner_outer_mr(struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                             struct MethodParams params);
+struct Result inner_outer_lomr(struct MatrixData A, struct MatrixData M0, struct MatrixData Pr,
+                               struct MethodParams params);
+void free_mem(struct Result* result);
+
 /* Precision and selection knobs that the reference's MethodParams lacks. */
 typedef struct SpaiExtParams {
   int64_t precision;       /* 0: FP64 storage (bit-compatible with the reference's arithmetic order inside each
