@@ -459,27 +459,25 @@ def e2e(args, A, M0, b):
                    "backward_error.pcg(..., symmetric_part=True) -> spai_pcg"}
 
 
-def cpu_baseline(args, A, M0, b, threads=None):
-    """CPU oracle SPAI (the FP64 restatement, OpenMP over column batches) on a
-    bounded sample, plus the reference's own compiled PCG (oracle/_ref) to 1e-8."""
+def cpu_build(args, A, M0, threads):
+    """One full CPU SPAI build of the workload: the oracle port (FP64, the
+    reference's summation order over `threads` column batches, OpenMP on
+    `threads` host threads), all args.spai_iterations iterations, timed whole
+    as the reference times a method call (scripts/methods_thread_speedup.py:34-45)."""
+    from oracle import pyoracle
+    n = A.shape[0]
+    t0 = time.perf_counter()
+    r = pyoracle.run("global_spai", "mr", A, M0=M0, max_iterations=args.spai_iterations, tolerance=1e-12,
+                     max_density=float(args.topk) / n, num_threads=threads, omp_threads=threads,
+                     topk_per_column=args.topk, order=pyoracle.ORDER_REFERENCE)
+    return time.perf_counter() - t0, r
+
+
+def cpu_pcg(args, A, M, b, threads):
+    """PCG to args.pcg_tolerance with (M + M^T)/2 of the CPU-built M: the
+    reference's own compiled backward_error.pcg when present, else the oracle port."""
     from scipy import sparse
     from oracle import pyoracle
-    threads = threads or os.cpu_count() or 1
-    n = A.shape[0]
-    sample = 3
-    t_start = time.perf_counter()
-    r1 = pyoracle.run("global_spai", "mr", A, M0=M0, max_iterations=1, tolerance=1e-12,
-                      max_density=float(args.topk) / n, num_threads=threads, omp_threads=threads,
-                      topk_per_column=args.topk, order=pyoracle.ORDER_REFERENCE)
-    t1 = time.perf_counter()
-    r3 = pyoracle.run("global_spai", "mr", A, M0=M0, max_iterations=sample, tolerance=1e-12,
-                      max_density=float(args.topk) / n, num_threads=threads, omp_threads=threads,
-                      topk_per_column=args.topk, order=pyoracle.ORDER_REFERENCE)
-    t3 = time.perf_counter()
-    per_iteration = ((t3 - t1) - (t1 - t_start)) / (sample - 1)
-    its_per_s = 1.0 / per_iteration if per_iteration > 0 else None
-    # PCG: the reference's compiled backward_error.pcg when present, else the oracle port
-    M = r3.M
     msym = sparse.csr_matrix((M + M.T) * 0.5)
     msym.sort_indices()
     A_csr = sparse.csr_matrix(A)
@@ -490,54 +488,77 @@ def cpu_baseline(args, A, M0, b, threads=None):
         hist, status = ref.pcg(A_csr.data, A_csr.indices.astype(np.int64), A_csr.indptr.astype(np.int64),
                                msym.data, msym.indices.astype(np.int64), msym.indptr.astype(np.int64), b,
                                args.pcg_max_iterations, threads, args.pcg_tolerance)
-        pcg_kind = "reference (methods_cython/backward_error.pyx compiled from the reference source)"
+        kind = "reference (methods_cython/backward_error.pyx compiled from the reference source)"
     else:
         hist, status = pyoracle.pcg(A_csr, msym, b, args.pcg_max_iterations, args.pcg_tolerance)
-        pcg_kind = "port"
-    pcg_s = time.perf_counter() - t0
-    pcg_1_ms = None
-    if ref is not None:
-        # the same solve on one thread (the reference's default num_threads)
-        t0 = time.perf_counter()
-        ref.pcg(A_csr.data, A_csr.indices.astype(np.int64), A_csr.indptr.astype(np.int64), msym.data,
-                msym.indices.astype(np.int64), msym.indptr.astype(np.int64), b, args.pcg_max_iterations, 1,
-                args.pcg_tolerance)
-        pcg_1_ms = round((time.perf_counter() - t0) * 1e3, 3)
-    return {"value": round(its_per_s, 4) if its_per_s else None, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{sample} Global MR iterations minus 1 (setup excluded) on the same 64^3 operator, "
-                      f"FP64 CPU oracle, {threads} OpenMP threads over {threads} column batches",
-            "pcg_ms_to_tolerance": round(pcg_s * 1e3, 3), "pcg_ms_to_tolerance_1_thread": pcg_1_ms,
-            "pcg_iterations": len(hist) - 1, "pcg_status": int(status),
-            "pcg_kind": pcg_kind,
-            "pcg_note": f"preconditioner = (M+M^T)/2 of the CPU {sample}-iteration M"}
+        kind = "port"
+    return time.perf_counter() - t0, hist, int(status), kind
+
+
+def cpu_baseline(args, A, M0, b, threads=None):
+    """The CPU path on the host cores: one whole SPAI build (no extrapolation)
+    and PCG on its M, at all host threads, plus the same PCG on one thread."""
+    threads = threads or os.cpu_count() or 1
+    build_s, r = cpu_build(args, A, M0, threads)
+    pcg_s, hist, status, kind = cpu_pcg(args, A, r.M, b, threads)
+    pcg_1_s, _, _, _ = cpu_pcg(args, A, r.M, b, 1)
+    return {"value": round(r.iterations / build_s, 4), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one whole {r.iterations}-iteration Global MR build of the same operator (top-"
+                      f"{args.topk}), FP64 CPU oracle port, {threads} OpenMP threads over {threads} column batches, "
+                      f"timed whole; then PCG on its M",
+            "spai_seconds_per_build": round(build_s, 3),
+            "pcg_ms_to_tolerance": round(pcg_s * 1e3, 3), "pcg_ms_to_tolerance_1_thread": round(pcg_1_s * 1e3, 3),
+            "pcg_iterations": len(hist) - 1, "pcg_status": status, "pcg_kind": kind,
+            "pcg_note": "preconditioner = (M+M^T)/2 of the CPU-built M"}
+
+
+REFERENCE_MAX_STEPS = 3
+REFERENCE_MAX_WARMUP = 1
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU implementation of the path (the
-    oracle port for SPAI, the reference's compiled PCG) on the host cores."""
+    """--impl reference: the reference's CPU implementation of the path on the
+    host cores -- the oracle port for SPAI (the reference's own SPAI needs
+    Eigen, absent here), the reference's compiled PCG -- each step one whole
+    build plus PCG, at all host threads.  A step takes about 15 s at 64^3, so at
+    most REFERENCE_MAX_STEPS timed steps after REFERENCE_MAX_WARMUP warm-up
+    steps run; the line's `steps` and `warmup` are the counts that ran."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     A, M0, b = workload(args)
     threads = os.cpu_count() or 1
-    for _ in range(args.warmup):
-        pass  # the CPU path has no warm-up state; each step is a fresh bounded sample
-    rows = []
-    for _ in range(args.steps):
-        rows.append(cpu_baseline(args, A, M0, b, threads))
-    value = statistics.median(r["value"] for r in rows)
-    pcg_ms = statistics.median(r["pcg_ms_to_tolerance"] for r in rows)
+    steps = max(1, min(args.steps, REFERENCE_MAX_STEPS))
+    warmup = min(args.warmup, REFERENCE_MAX_WARMUP)
+    for _ in range(warmup):
+        cpu_build(args, A, M0, threads)
+    builds, pcgs, its = [], [], 0
+    pcg_info = None
+    for _ in range(steps):
+        build_s, r = cpu_build(args, A, M0, threads)
+        pcg_s, hist, status, kind = cpu_pcg(args, A, r.M, b, threads)
+        builds.append(build_s)
+        pcgs.append(pcg_s)
+        its += r.iterations
+        pcg_info = (len(hist) - 1, status, kind)
+    value = its / sum(builds)
     line = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": round(1e3 * args.spai_iterations / value + pcg_ms, 3),
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": warmup, "steps_requested": args.steps, "warmup_requested": args.warmup,
+        "ms_per_step": round(1e3 * (sum(builds) + sum(pcgs)) / steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded 64^3 log-normal diffusion operator; no public data set)",
         "config": config_dict(args, A), "impl": "reference",
-        "pcg_ms_to_tolerance": pcg_ms,
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": rows[0]["sample"], "pcg_kind": rows[0]["pcg_kind"]},
-        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "spai_seconds_per_build": round(sum(builds) / steps, 3),
+        "pcg_ms_to_tolerance": round(1e3 * sum(pcgs) / steps, 3),
+        "pcg_iterations": pcg_info[0], "pcg_status": pcg_info[1],
+        "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} whole {args.spai_iterations}-iteration Global MR builds (FP64 oracle "
+                                   f"port, the reference's summation order, {threads} OpenMP threads), each followed "
+                                   f"by PCG on its M",
+                         "pcg_kind": pcg_info[2]},
+        "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
 
