@@ -280,6 +280,13 @@ void spai_inject_allocation_failure(int64_t after);
 /* Number of kernels this library has launched since load (diagnostics). */
 int64_t spai_kernel_launches(void);
 
+/* Global MR with per-column top-k, a diagonal Pr and a stencil-like A runs
+ * its iterations as one CUDA graph of fused kernels (no host round trip per
+ * iteration).  enabled = 0 routes every run through the unfused kernels
+ * instead; both give the same bits (process-wide, default 1).  No
+ * counterpart in the reference. */
+void spai_set_fused_mr(int64_t enabled);
+
 /* Opt-in per-kernel-class accounting with CUDA events: enable (1) / disable (0),
  * reset, and read the totals of one class ("spgemm_numeric", "spgemm_symbolic",
  * "union", "transpose", "filter", "pcg_spmv"): elapsed ms, launches and the

@@ -17,7 +17,7 @@ CSRC = PACKAGE_DIR / "csrc"
 LIB_PATH = PACKAGE_DIR / "libspai_b200.so"
 BUILD_DIR = PACKAGE_DIR / "_build"
 
-SOURCES = ["ops.cu", "spgemm.cu", "update.cu", "solver.cu", "pcg.cu", "c_api.cu", "profile.cu", "noalloc.cu",
+SOURCES = ["ops.cu", "spgemm.cu", "update.cu", "solver.cu", "mr_fused.cu", "pcg.cu", "c_api.cu", "profile.cu", "noalloc.cu",
            "adjoint.cu", "mtx.cpp"]
 
 NVCC_FLAGS = [

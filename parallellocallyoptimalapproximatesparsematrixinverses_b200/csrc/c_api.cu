@@ -21,6 +21,7 @@
 #include "ops.cuh"
 #include "pcg.cuh"
 #include "profile.cuh"
+#include "mr_fused.cuh"
 #include "solver.cuh"
 
 namespace spai {
@@ -867,5 +868,7 @@ int64_t spai_profile_read(const char* name, double* ms, int64_t* launches, doubl
 }
 
 int64_t spai_kernel_launches(void) { return spai::g_launches.load(); }
+
+void spai_set_fused_mr(int64_t enabled) { spai::SetFusedMrEnabled(enabled != 0); }
 
 }  // extern "C"

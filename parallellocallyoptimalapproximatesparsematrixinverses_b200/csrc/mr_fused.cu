@@ -1,0 +1,1150 @@
+// The fused, graph-captured Global MR iteration (mr_fused.cuh).
+//
+// Slot layouts (all in HBM, sized once per solver):
+//   M    topk slots per column, rows ascending, count per column
+//   M^T  two sets (the drop kernel reads one and writes the other), cap_mt
+//        slots per row in arrival order, count per row
+//   Z    cap_z slots per column, rows ascending (Z = Pr R keeps R's pattern)
+//   Z^T  cap_zt slots per row in arrival order
+// The drop kernel consumes Z, Z^T and the current M^T set and clears their
+// counts as it reads them (each count belongs to one column's warp), so the
+// residual kernel refills Z^T and the next drop kernel fills the other M^T
+// set without a separate clearing pass.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <memory>
+#include <stdexcept>
+#include <vector>
+
+#include "colkit.cuh"
+#include "device.cuh"
+#include "mr_fused.cuh"
+#include "ops.cuh"
+#include "profile.cuh"
+#include "select.cuh"
+#include "tree.cuh"
+
+namespace spai {
+
+void CountLaunches(int64_t count);
+
+namespace {
+
+constexpr int kDropWarps = 8;       // warps per block of the drop kernel
+constexpr int kResidualWarps = 4;   // warps per block of the residual kernel
+constexpr int kWindowWords = 2048;  // row window of the residual kernel's bitmaps (65,536 rows)
+constexpr int kRowsCap = 1024;      // longest row list of one product column
+constexpr int kSideCap = 256;       // longest own / transposed side of a drop column
+constexpr int kMaxTopK = 32;
+
+// Overflow bits (FusedState::overflow).
+constexpr int kOverflowMt = 1;      // a row of M^T exceeded cap_mt
+constexpr int kOverflowZt = 2;      // a row of Z^T exceeded cap_zt
+constexpr int kOverflowSide = 4;    // a drop column exceeded kSideCap or kDropCap
+constexpr int kOverflowWindow = 8;  // a product column's rows spanned more than the window
+
+// Stop codes (FusedState::stop).
+constexpr int kRunning = 0;
+constexpr int kConverged = 1;
+constexpr int kBreakdown = 2;
+constexpr int kIterationLimit = 3;
+constexpr int kOverflowStop = 4;
+
+struct FusedRow {
+  int64_t iteration;
+  double residual_norm;
+  double density_m;
+  double density_direction;
+};
+
+// Device-resident loop state.
+struct FusedState {
+  double alpha;                 // step length of the next iteration
+  int64_t iteration;            // last history row appended
+  int64_t parity;               // M^T set the next drop kernel reads
+  unsigned long long nnz_m;     // entries of M written by this iteration's drop kernel
+  unsigned long long nnz_z;     // entries of Z written by this iteration's residual kernel
+  unsigned long long nnz_dir;   // entries of the Z this iteration's step used (its history row's direction)
+  unsigned long long last_nnz_m;  // the last iteration's counts (read by the host when profiling)
+  unsigned long long last_nnz_z;
+  int32_t overflow;
+  int32_t stop;
+  unsigned int arrive;          // blocks of the decide kernel that are done
+  int32_t pad;
+  int64_t bodies;               // loop-body executions
+};
+
+template <class T>
+struct FusedArgs {
+  int64_t n;
+  int topk;
+  int cap_z;
+  int cap_mt;
+  int cap_zt;
+  int ell;  // ELL slots of A (multiple of 4)
+  int m_hash_slots;
+  int z_hash_slots;
+  int64_t max_iterations;
+  double tolerance;
+  const int32_t* a_cols_ell;
+  const int32_t* a_rows_ell;
+  const T* a_rows_ell_val;
+  const T* pr;
+  int32_t* m_rows;
+  T* m_vals;
+  int32_t* m_cnt;
+  int32_t* mt_cols[2];
+  T* mt_vals[2];
+  int32_t* mt_cnt[2];
+  int32_t* z_rows;
+  T* z_vals;
+  int32_t* z_cnt;
+  int32_t* zt_cols;
+  T* zt_vals;
+  int32_t* zt_cnt;
+  double* sq;          // per-column sum of squares of R
+  double* tt;          // per-column ||Pr A Z(:, j)||^2
+  double* bt;          // per-column <Z(:, j), Pr A Z(:, j)>
+  double* chunk;       // 3 * chunks
+  FusedRow* history;   // max_iterations + 1 rows
+  FusedState* state;
+};
+
+// ---------------------------------------------------------------------------
+// Drop kernel: per column j, S = 0.5 (U(:, j) + U(j, :)^T) with U = M + alpha Z.
+
+struct DropSides {
+  int32_t* own_rows;  // U(:, j): rows of M(:, j) and Z(:, j), merged
+  void* own_vals;
+  int32_t* tr_rows;   // U(j, :)^T: columns of M(j, :) and Z(j, :), merged
+  void* tr_vals;
+};
+
+template <class T>
+__host__ __device__ constexpr size_t DropSidesBytes() {
+  return 2 * Round16Bytes(kSideCap * sizeof(int32_t)) + 2 * Round16Bytes(kSideCap * sizeof(T));
+}
+
+template <class T>
+__device__ DropSides SidesFor(unsigned char* base) {
+  DropSides d;
+  d.own_rows = reinterpret_cast<int32_t*>(base);
+  base += Round16Bytes(kSideCap * sizeof(int32_t));
+  d.own_vals = base;
+  base += Round16Bytes(kSideCap * sizeof(T));
+  d.tr_rows = reinterpret_cast<int32_t*>(base);
+  base += Round16Bytes(kSideCap * sizeof(int32_t));
+  d.tr_vals = base;
+  return d;
+}
+
+// pre[q] = number of the first q keys of x (sorted) found in y (sorted), q = 0..nx.
+__device__ __forceinline__ int MatchedPrefixShared(const int32_t* yk, int ny, const int32_t* xk, int nx, int* pre,
+                                                   int lane) {
+  int running = 0;
+  for (int base = 0; base < nx; base += kWarp) {
+    const int q = base + lane;
+    bool hit = false;
+    if (q < nx) {
+      const int32_t row = xk[q];
+      const int r = LowerBoundShared(yk, ny, row);
+      hit = r < ny && yk[r] == row;
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, hit);
+    if (q < nx) pre[q] = running + __popc(mask & LaneMaskBelow());
+    running += __popc(mask);
+  }
+  if (lane == 0) pre[nx] = running;
+  __syncwarp();
+  return running;
+}
+
+// Builds U(j, :)^T from M^T(:, j) (nmt entries) and Z^T(:, j) (nzt entries),
+// rows ascending, into d.tr_rows / d.tr_vals; returns its length.  The
+// entries arrive in any order: (column, source) keys are sorted in registers.
+template <class T, int R>
+__device__ int BuildTransposed(const FusedArgs<T>& a, int64_t parity, int64_t j, int nmt, int nzt, T alpha,
+                               DropSides& d, int lane) {
+  const int nt = nmt + nzt;
+  const int32_t* mt_cols = a.mt_cols[parity] + j * a.cap_mt;
+  const T* mt_vals = a.mt_vals[parity] + j * a.cap_mt;
+  const int32_t* zt_cols = a.zt_cols + j * a.cap_zt;
+  const T* zt_vals = a.zt_vals + j * a.cap_zt;
+  unsigned long long k[R];
+  uint32_t p[R];
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    const int e = t * kWarp + lane;
+    if (e < nmt) {
+      k[t] = static_cast<unsigned long long>(static_cast<uint32_t>(mt_cols[e])) << 1;
+    } else if (e < nt) {
+      k[t] = (static_cast<unsigned long long>(static_cast<uint32_t>(zt_cols[e - nmt])) << 1) | 1ull;
+    } else {
+      k[t] = ~0ull;
+    }
+    p[t] = static_cast<uint32_t>(e);
+  }
+  WarpBitonicSort<R>(k, p, lane);
+  T* tr_vals = static_cast<T*>(d.tr_vals);
+  int filled = 0;
+#pragma unroll
+  for (int t = 0; t < R; ++t) {
+    // the next element in the sorted order (t * 32 + lane + 1) and the previous one
+    unsigned long long next_k = __shfl_down_sync(0xffffffffu, k[t], 1);
+    uint32_t next_p = __shfl_down_sync(0xffffffffu, p[t], 1);
+    unsigned long long prev_k = __shfl_up_sync(0xffffffffu, k[t], 1);
+    const unsigned long long wrap_next_k = t + 1 < R ? __shfl_sync(0xffffffffu, k[t + 1 < R ? t + 1 : t], 0) : ~0ull;
+    const uint32_t wrap_next_p = t + 1 < R ? __shfl_sync(0xffffffffu, p[t + 1 < R ? t + 1 : t], 0) : 0u;
+    const unsigned long long wrap_prev_k = t > 0 ? __shfl_sync(0xffffffffu, k[t > 0 ? t - 1 : t], kWarp - 1) : ~0ull;
+    if (lane == kWarp - 1) {
+      next_k = wrap_next_k;
+      next_p = wrap_next_p;
+    }
+    if (lane == 0) prev_k = wrap_prev_k;
+    const bool valid = k[t] != ~0ull;
+    const uint32_t row = static_cast<uint32_t>(k[t] >> 1);
+    const bool from_z = (k[t] & 1ull) != 0;
+    // a row appears at most once from M^T and once from Z^T, the M entry first
+    const bool head = valid && (!from_z || prev_k == ~0ull || static_cast<uint32_t>(prev_k >> 1) != row ||
+                                (prev_k & 1ull) != 0);
+    T v = T(0);
+    if (head) {
+      if (!from_z) {
+        const T mv = mt_vals[p[t]];
+        const bool pair = next_k != ~0ull && static_cast<uint32_t>(next_k >> 1) == row && (next_k & 1ull) != 0;
+        // the union's arithmetic (UnionPadded): y + a x, y + 0, 0 + a x
+        v = pair ? Add(mv, Mul(alpha, zt_vals[next_p - nmt])) : Add(mv, T(0));
+      } else {
+        v = Add(T(0), Mul(alpha, zt_vals[p[t] - nmt]));
+      }
+    }
+    const unsigned mask = __ballot_sync(0xffffffffu, head);
+    if (head) {
+      const int at = filled + __popc(mask & LaneMaskBelow());
+      d.tr_rows[at] = static_cast<int32_t>(row);
+      tr_vals[at] = v;
+    }
+    filled += __popc(mask);
+  }
+  __syncwarp();
+  return filled;
+}
+
+template <class T>
+__global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char fused_drop_smem[];
+  const int lane = threadIdx.x & 31;
+  unsigned char* base = fused_drop_smem + (threadIdx.x >> 5) * (DropSlabBytes() + DropSidesBytes<T>());
+  DropSlab s = SlabFor(base);
+  DropSides d = SidesFor<T>(base + DropSlabBytes());
+  FusedState* state = a.state;
+  const int64_t parity = state->parity;
+  const T alpha = static_cast<T>(state->alpha);
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long written = 0;
+  int overflow = 0;
+  for (int64_t j = warp; j < a.n; j += warps) {
+    const int nm = a.m_cnt[j];
+    const int nz = a.z_cnt[j];
+    const int nmt_all = a.mt_cnt[parity][j];
+    const int nzt_all = a.zt_cnt[j];
+    __syncwarp();
+    if (lane == 0) {
+      // this column's transposed rows are consumed here: their sets refill from zero
+      a.mt_cnt[parity][j] = 0;
+      a.zt_cnt[j] = 0;
+    }
+    if (nmt_all > a.cap_mt || nzt_all > a.cap_zt || nm + nz > kSideCap || nmt_all + nzt_all > kSideCap) {
+      overflow |= kOverflowSide;
+      continue;
+    }
+    // own side U(:, j) = M(:, j) (+) alpha Z(:, j)
+    const int32_t* mr = a.m_rows + j * a.topk;
+    const T* mv = a.m_vals + j * a.topk;
+    const int32_t* zr = a.z_rows + j * a.cap_z;
+    const T* zv = a.z_vals + j * a.cap_z;
+    for (int i = lane; i < nm; i += kWarp) s.yk[i] = mr[i];
+    for (int i = lane; i < nz; i += kWarp) s.xk[i] = zr[i];
+    __syncwarp();
+    const int matched = MatchedPrefixShared(s.yk, nm, s.xk, nz, s.mx_prefix, lane);
+    const int no = nm + nz - matched;
+    T* own_vals = static_cast<T*>(d.own_vals);
+    for (int e = lane; e < nm; e += kWarp) {
+      const int32_t row = s.yk[e];
+      const int r = LowerBoundShared(s.xk, nz, row);
+      const T y = mv[e];
+      const T v = (r < nz && s.xk[r] == row) ? Add(y, Mul(alpha, zv[r])) : Add(y, T(0));
+      const int rank = e + r - s.mx_prefix[r];
+      d.own_rows[rank] = row;
+      own_vals[rank] = v;
+    }
+    for (int q = lane; q < nz; q += kWarp) {
+      const int32_t row = s.xk[q];
+      const int r = LowerBoundShared(s.yk, nm, row);
+      if (r < nm && s.yk[r] == row) continue;
+      const int rank = q - s.mx_prefix[q] + r;
+      d.own_rows[rank] = row;
+      own_vals[rank] = Add(T(0), Mul(alpha, zv[q]));
+    }
+    // transposed side U(j, :)^T
+    const int nt = nmt_all + nzt_all;
+    int ntr;
+    if (nt <= kWarp) {
+      ntr = BuildTransposed<T, 1>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
+    } else if (nt <= 2 * kWarp) {
+      ntr = BuildTransposed<T, 2>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
+    } else if (nt <= 4 * kWarp) {
+      ntr = BuildTransposed<T, 4>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
+    } else {
+      ntr = BuildTransposed<T, 8>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
+    }
+    __syncwarp();
+    // S(:, j) = 0.5 (own + transposed), merged in row order into the slab
+    const int matched2 = MatchedPrefixShared(d.own_rows, no, d.tr_rows, ntr, s.mx_prefix, lane);
+    const int count = no + ntr - matched2;
+    if (count > kDropCap) {
+      overflow |= kOverflowSide;
+      __syncwarp();
+      continue;
+    }
+    const T* tr_vals = static_cast<const T*>(d.tr_vals);
+    for (int e = lane; e < no; e += kWarp) {
+      const int32_t row = d.own_rows[e];
+      const int r = LowerBoundShared(d.tr_rows, ntr, row);
+      const T y = own_vals[e];
+      // the half sum of the symmetrisation (dropping.cpp:106-120)
+      const T v = (r < ntr && d.tr_rows[r] == row) ? Mul(T(0.5), Add(y, tr_vals[r])) : Mul(T(0.5), Add(y, T(0)));
+      const int rank = e + r - s.mx_prefix[r];
+      s.keys[rank] = row;
+      s.vals[rank] = static_cast<double>(v);
+    }
+    for (int q = lane; q < ntr; q += kWarp) {
+      const int32_t row = d.tr_rows[q];
+      const int r = LowerBoundShared(d.own_rows, no, row);
+      if (r < no && d.own_rows[r] == row) continue;
+      const int rank = q - s.mx_prefix[q] + r;
+      s.keys[rank] = row;
+      s.vals[rank] = static_cast<double>(Mul(T(0.5), Add(T(0), tr_vals[q])));
+    }
+    __syncwarp();
+    const int kept = DecideDrops(s, count, j, a.topk, lane);
+    // survivors: M(:, j) in place, and M^T into the other set
+    int32_t* out_rows = a.m_rows + j * a.topk;
+    T* out_vals = a.m_vals + j * a.topk;
+    const int64_t other = parity ^ 1;
+    int at = 0;
+    for (int b0 = 0; b0 < count; b0 += kWarp) {
+      const int i = b0 + lane;
+      const bool keep = i < count && s.keep[i] != 0;
+      const unsigned mask = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int o = at + __popc(mask & LaneMaskBelow());
+        const int32_t row = s.keys[i];
+        const T v = static_cast<T>(s.vals[i]);
+        out_rows[o] = row;
+        out_vals[o] = v;
+        const int slot = atomicAdd(&a.mt_cnt[other][row], 1);
+        if (slot < a.cap_mt) {
+          a.mt_cols[other][static_cast<int64_t>(row) * a.cap_mt + slot] = static_cast<int32_t>(j);
+          a.mt_vals[other][static_cast<int64_t>(row) * a.cap_mt + slot] = v;
+        } else {
+          overflow |= kOverflowMt;
+        }
+      }
+      at += __popc(mask);
+    }
+    if (lane == 0) a.m_cnt[j] = kept;
+    written += static_cast<unsigned long long>(kept);
+    __syncwarp();
+  }
+  overflow = __reduce_or_sync(0xffffffffu, overflow);
+  if (lane == 0) {
+    if (written != 0ull) atomicAdd(&state->nnz_m, written);
+    if (overflow != 0) atomicOr(&state->overflow, overflow);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Residual kernel: R = I - A M(:, j), Z = Pr R, ||R(:, j)||^2, then the MR
+// projection of A Z(:, j).  The arithmetic is ColumnProductKernel's
+// (spgemm.cu): rows in ascending order from the window bitmap, each row of A
+// (ELL copy) pulled in ascending k against a hash of the column, the
+// accumulator started at -0.0, sums sequential in row order on one lane.
+
+template <class T>
+__host__ __device__ size_t ResidualSlabBytes(int m_slots, int z_slots) {
+  return Round16(static_cast<size_t>(kWindowWords) * 4) + Round16(static_cast<size_t>(SummaryWords(kWindowWords)) * 4) +
+         Round16(static_cast<size_t>(kRowsCap) * 2) + Round16(static_cast<size_t>(m_slots) * 4) +
+         Round16(static_cast<size_t>(m_slots) * sizeof(T)) + Round16(static_cast<size_t>(z_slots) * 4) +
+         Round16(static_cast<size_t>(z_slots) * sizeof(T)) + Round16(static_cast<size_t>(kSideCap) * 4) +
+         2 * Round16(kWarp * sizeof(double));
+}
+
+// Sequential sum of `count` staged values onto s (one lane).
+__device__ __forceinline__ double SumStaged(double s, const double* src, int count) {
+  if (count == kWarp) {
+    const double2* src2 = reinterpret_cast<const double2*>(src);
+#pragma unroll
+    for (int l = 0; l < kWarp / 2; ++l) {
+      const double2 v = src2[l];
+      s = Add(s, v.x);
+      s = Add(s, v.y);
+    }
+  } else {
+    for (int l = 0; l < count; ++l) s = Add(s, src[l]);
+  }
+  return s;
+}
+
+template <class T, int kEll>
+__global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(FusedArgs<T> a) {
+  extern __shared__ __align__(16) unsigned char fused_res_smem[];
+  const int lane = threadIdx.x & 31;
+  constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
+  unsigned char* base = fused_res_smem + (threadIdx.x >> 5) * ResidualSlabBytes<T>(a.m_hash_slots, a.z_hash_slots);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(base);
+  base += Round16(static_cast<size_t>(kWindowWords) * 4);
+  uint32_t* summary = reinterpret_cast<uint32_t*>(base);
+  base += Round16(static_cast<size_t>(kSummary) * 4);
+  uint16_t* rows = reinterpret_cast<uint16_t*>(base);
+  base += Round16(static_cast<size_t>(kRowsCap) * 2);
+  int32_t* mkeys = reinterpret_cast<int32_t*>(base);
+  base += Round16(static_cast<size_t>(a.m_hash_slots) * 4);
+  T* mvals = reinterpret_cast<T*>(base);
+  base += Round16(static_cast<size_t>(a.m_hash_slots) * sizeof(T));
+  int32_t* zkeys = reinterpret_cast<int32_t*>(base);
+  base += Round16(static_cast<size_t>(a.z_hash_slots) * 4);
+  T* zvals = reinterpret_cast<T*>(base);
+  base += Round16(static_cast<size_t>(a.z_hash_slots) * sizeof(T));
+  int32_t* zlist = reinterpret_cast<int32_t*>(base);
+  base += Round16(static_cast<size_t>(kSideCap) * 4);
+  double* stage0 = reinterpret_cast<double*>(base);
+  double* stage1 = stage0 + kWarp;
+  const int mbits = Log2(a.m_hash_slots) - 1;  // buckets of two slots
+  const int zbits = Log2(a.z_hash_slots) - 1;
+  ClearWords(bm, kWindowWords, lane);
+  ClearWords(summary, kSummary, lane);
+  __syncwarp();
+  const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
+  const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
+  unsigned long long written = 0;
+  int overflow = 0;
+  for (int64_t j = warp; j < a.n; j += warps) {
+    // ---- R(:, j) = e_j - A M(:, j) ----------------------------------------
+    const int nm = a.m_cnt[j];
+    ClearTable(mkeys, a.m_hash_slots, lane);
+    __syncwarp();
+    int32_t k_mine = -1;
+    bool placed = true;
+    if (lane < nm) {
+      k_mine = a.m_rows[j * a.topk + lane];
+      placed = BucketInsert(mkeys, mvals, mbits, k_mine, a.m_vals[j * a.topk + lane]);
+    }
+    const bool m_displaced = !__all_sync(0xffffffffu, placed);
+    // the candidate rows: A(:, k) for k in M(:, j), and j itself
+    int32_t cand[kEll];
+    int32_t lo = static_cast<int32_t>(j);
+    int32_t hi = static_cast<int32_t>(j);
+#pragma unroll
+    for (int u = 0; u < kEll / 4; ++u) {
+      int4 r4 = make_int4(-1, -1, -1, -1);
+      if (k_mine >= 0) r4 = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(k_mine) * kEll)[u];
+      cand[4 * u] = r4.x;
+      cand[4 * u + 1] = r4.y;
+      cand[4 * u + 2] = r4.z;
+      cand[4 * u + 3] = r4.w;
+    }
+#pragma unroll
+    for (int u = 0; u < kEll; ++u) {
+      if (cand[u] >= 0) {
+        lo = min(lo, cand[u]);
+        hi = max(hi, cand[u]);
+      }
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    const int words = (hi - lo) / 32 + 1;
+    if (words > kWindowWords) {
+      overflow |= kOverflowWindow;
+      continue;
+    }
+    if (lane == 0) MarkRow(bm, summary, static_cast<int>(j) - lo);
+#pragma unroll
+    for (int u = 0; u < kEll; ++u) {
+      if (cand[u] >= 0) MarkRow(bm, summary, cand[u] - lo);
+    }
+    __syncwarp();
+    const int count = DrainRows(bm, summary, SummaryWords(words), rows, lane);
+    int32_t* zr_out = a.z_rows + j * a.cap_z;
+    T* zv_out = a.z_vals + j * a.cap_z;
+    ClearTable(zkeys, a.z_hash_slots, lane);
+    __syncwarp();
+    int kept = 0;
+    double sq = 0.0;
+    bool z_placed = true;
+    for (int r0 = 0; r0 < count; r0 += kWarp) {
+      const int r = r0 + lane;
+      bool keep = false;
+      int32_t i = 0;
+      T v = T(0);
+      if (r < count) {
+        i = lo + static_cast<int32_t>(rows[r]);
+        T acc = T(-0.0);
+        const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
+        const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
+#pragma unroll
+        for (int u = 0; u < kEll / 4; ++u) {
+          const int4 k4 = ks[u];
+          T v4[4];
+          LoadFour(vs + 4 * u, v4);
+          const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            T bv;
+            if (kk[e] >= 0 && BucketFind(mkeys, mvals, mbits, m_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
+          }
+        }
+        v = -acc;
+        if (static_cast<int64_t>(i) == j) v = Add(v, T(1));
+        const double sd = static_cast<double>(v);
+        stage0[lane] = Mul(sd, sd);
+        keep = !(v == T(0));  // Eigen prune(0.0)
+      }
+      const unsigned mask = __ballot_sync(0xffffffffu, keep);
+      if (keep) {
+        const int o = kept + __popc(mask & LaneMaskBelow());
+        const T z = Mul(a.pr[i], v);
+        zr_out[o] = i;
+        zv_out[o] = z;
+        zlist[o] = i;
+        z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
+        const int slot = atomicAdd(&a.zt_cnt[i], 1);
+        if (slot < a.cap_zt) {
+          a.zt_cols[static_cast<int64_t>(i) * a.cap_zt + slot] = static_cast<int32_t>(j);
+          a.zt_vals[static_cast<int64_t>(i) * a.cap_zt + slot] = z;
+        } else {
+          overflow |= kOverflowZt;
+        }
+      }
+      kept += __popc(mask);
+      __syncwarp();
+      if (lane == 0) sq = SumStaged(sq, stage0, min(kWarp, count - r0));
+      __syncwarp();
+    }
+    if (lane == 0) {
+      a.sq[j] = sq;
+      a.z_cnt[j] = kept;
+    }
+    written += static_cast<unsigned long long>(kept);
+    const bool z_displaced = !__all_sync(0xffffffffu, z_placed);
+    // ---- projection: tt = ||Pr A Z(:, j)||^2, bt = <Z(:, j), Pr A Z(:, j)> --
+    lo = INT32_MAX;
+    hi = -1;
+    for (int e = lane; e < kept; e += kWarp) {
+      const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zlist[e]) * kEll);
+#pragma unroll
+      for (int u = 0; u < kEll / 4; ++u) {
+        const int4 r4 = src[u];
+        const int32_t rr[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+          if (rr[t] >= 0) {
+            lo = min(lo, rr[t]);
+            hi = max(hi, rr[t]);
+          }
+        }
+      }
+    }
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    double tt = 0.0;
+    double bt = 0.0;
+    if (hi >= lo) {
+      const int words2 = (hi - lo) / 32 + 1;
+      if (words2 > kWindowWords) {
+        overflow |= kOverflowWindow;
+        continue;
+      }
+      for (int e = lane; e < kept; e += kWarp) {
+        const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zlist[e]) * kEll);
+#pragma unroll
+        for (int u = 0; u < kEll / 4; ++u) {
+          const int4 r4 = src[u];
+          if (r4.x >= 0) MarkRow(bm, summary, r4.x - lo);
+          if (r4.y >= 0) MarkRow(bm, summary, r4.y - lo);
+          if (r4.z >= 0) MarkRow(bm, summary, r4.z - lo);
+          if (r4.w >= 0) MarkRow(bm, summary, r4.w - lo);
+        }
+      }
+      __syncwarp();
+      const int count2 = DrainRows(bm, summary, SummaryWords(words2), rows, lane);
+      for (int r0 = 0; r0 < count2; r0 += kWarp) {
+        const int r = r0 + lane;
+        if (r < count2) {
+          const int32_t i = lo + static_cast<int32_t>(rows[r]);
+          T acc = T(-0.0);
+          const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
+          const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
+#pragma unroll
+          for (int u = 0; u < kEll / 4; ++u) {
+            const int4 k4 = ks[u];
+            T v4[4];
+            LoadFour(vs + 4 * u, v4);
+            const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              T bv;
+              if (kk[e] >= 0 && BucketFind(zkeys, zvals, zbits, z_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
+            }
+          }
+          const double td = static_cast<double>(Mul(a.pr[i], acc));
+          T zi;
+          stage0[lane] = Mul(td, td);
+          // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
+          stage1[lane] = BucketFind(zkeys, zvals, zbits, z_displaced, i, zi) ? Mul(static_cast<double>(zi), td) : 0.0;
+        }
+        __syncwarp();
+        const int span = min(kWarp, count2 - r0);
+        if (lane == 0) tt = SumStaged(tt, stage0, span);
+        if (lane == 1) bt = SumStaged(bt, stage1, span);
+        __syncwarp();
+      }
+    }
+    if (lane == 0) a.tt[j] = tt;
+    if (lane == 1) a.bt[j] = bt;
+    __syncwarp();
+  }
+  overflow = __reduce_or_sync(0xffffffffu, overflow);
+  if (lane == 0) {
+    if (written != 0ull) atomicAdd(&a.state->nnz_z, written);
+    if (overflow != 0) atomicOr(&a.state->overflow, overflow);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Decide kernel: the three tree sums; the last block appends the history row,
+// applies the stop rules (result_operations.cpp:53-67, minimal_residual.cpp:55-89),
+// forms the next step length and, inside the graph, sets the loop condition.
+template <class T>
+__global__ void __launch_bounds__(kTreeLanes) FusedDecideKernel(FusedArgs<T> a, cudaGraphConditionalHandle loop,
+                                                                bool in_graph) {
+  __shared__ double shared[kTreeLanes];
+  __shared__ int last;
+  const int t = threadIdx.x;
+  const int64_t base = static_cast<int64_t>(blockIdx.x) * kTreeChunk + t;
+  double s_sq = 0.0;
+  double s_bt = 0.0;
+  double s_tt = 0.0;
+#pragma unroll
+  for (int m = 0; m < kTreeTerms; ++m) {
+    const int64_t i = base + static_cast<int64_t>(kTreeLanes) * m;
+    if (i < a.n) {
+      s_sq = Add(s_sq, a.sq[i]);
+      s_bt = Add(s_bt, a.bt[i]);
+      s_tt = Add(s_tt, a.tt[i]);
+    }
+  }
+  double total_sq = TreeButterfly(s_sq, shared);
+  double total_bt = TreeButterfly(s_bt, shared);
+  double total_tt = TreeButterfly(s_tt, shared);
+  FusedState* state = a.state;
+  if (gridDim.x > 1) {
+    const int64_t chunks = gridDim.x;
+    if (t == 0) {
+      a.chunk[blockIdx.x] = total_sq;
+      a.chunk[chunks + blockIdx.x] = total_bt;
+      a.chunk[2 * chunks + blockIdx.x] = total_tt;
+      __threadfence();
+      last = atomicAdd(&state->arrive, 1u) == gridDim.x - 1 ? 1 : 0;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    total_sq = TreeLevel(a.chunk, chunks, shared);
+    total_bt = TreeLevel(a.chunk + chunks, chunks, shared);
+    total_tt = TreeLevel(a.chunk + 2 * chunks, chunks, shared);
+  }
+  if (t != 0) return;
+  state->arrive = 0u;
+  const int64_t it = state->iteration + 1;
+  const double entries = Mul(static_cast<double>(a.n), static_cast<double>(a.n));
+  FusedRow row;
+  row.iteration = it;
+  row.residual_norm = __dsqrt_rn(total_sq);
+  row.density_m = __ddiv_rn(static_cast<double>(state->nnz_m), entries);
+  // the row's direction is the Z the step M += alpha Z used, not the one just formed
+  // (the history row is appended before Z is recomputed, minimal_residual.cpp:78-88)
+  row.density_direction = __ddiv_rn(static_cast<double>(state->nnz_dir), entries);
+  a.history[it] = row;
+  state->iteration = it;
+  state->last_nnz_m = state->nnz_m;
+  state->last_nnz_z = state->nnz_z;
+  state->nnz_dir = state->nnz_z;
+  state->nnz_m = 0ull;
+  state->nnz_z = 0ull;
+  int stop = kRunning;
+  if (state->overflow != 0) {
+    stop = kOverflowStop;
+  } else if (row.residual_norm < a.tolerance) {
+    stop = kConverged;
+  } else if (it >= a.max_iterations) {
+    stop = kIterationLimit;
+  } else {
+    // the next iteration's step length (minimal_residual.cpp:55-60)
+    const double num = total_bt;
+    const double den = total_tt;
+    if (!isfinite(den) || !(fabs(den) > 0.0)) {
+      stop = kBreakdown;
+    } else {
+      const double alpha = __ddiv_rn(num, den);
+      if (!isfinite(alpha)) {
+        stop = kBreakdown;
+      } else {
+        state->alpha = alpha;
+      }
+    }
+  }
+  state->stop = stop;
+  state->parity ^= 1;
+  state->bodies += 1;
+  if (in_graph) {
+    // the body count bounds the loop whatever the recurrence does
+    const bool again = stop == kRunning && state->bodies < a.max_iterations + 1;
+    cudaGraphSetConditional(loop, again ? 1u : 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Conversions between compact CSC and the slots.
+
+// Column j of a compact CSC into `cap` slots (count per column); when t_cnt is
+// given, every entry (i, j) is also appended to row i of the transposed slots.
+template <class T>
+__global__ void ToSlotsKernel(CscView<T> x, int cap, int32_t* __restrict__ rows, T* __restrict__ vals,
+                              int32_t* __restrict__ cnt, int t_cap, int32_t* __restrict__ t_cols, T* __restrict__ t_vals,
+                              int32_t* __restrict__ t_cnt, FusedState* __restrict__ state) {
+  int overflow = 0;
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < x.cols;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = x.ptr[j];
+    const int64_t e = x.ptr[j + 1];
+    const int len = static_cast<int>(e - b);
+    if (len > cap) {
+      overflow |= kOverflowSide;
+      cnt[j] = 0;
+      continue;
+    }
+    for (int q = 0; q < len; ++q) {
+      const int32_t i = x.idx[b + q];
+      const T v = x.val[b + q];
+      rows[j * cap + q] = i;
+      vals[j * cap + q] = v;
+      if (t_cnt != nullptr) {
+        const int slot = atomicAdd(&t_cnt[i], 1);
+        if (slot < t_cap) {
+          t_cols[static_cast<int64_t>(i) * t_cap + slot] = static_cast<int32_t>(j);
+          t_vals[static_cast<int64_t>(i) * t_cap + slot] = v;
+        } else {
+          overflow |= kOverflowMt;
+        }
+      }
+    }
+    cnt[j] = len;
+  }
+  if (overflow != 0) atomicOr(&state->overflow, overflow);
+}
+
+__global__ void WidenCountsKernel(const int32_t* __restrict__ cnt, int64_t n, int64_t* __restrict__ out) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    out[j] = cnt[j];
+  }
+}
+
+template <class T>
+__global__ void FromSlotsKernel(int64_t n, int cap, const int32_t* __restrict__ rows, const T* __restrict__ vals,
+                                const int64_t* __restrict__ ptr, int32_t* __restrict__ idx_out, T* __restrict__ val_out) {
+  for (int64_t j = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; j < n;
+       j += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t o = ptr[j];
+    const int len = static_cast<int>(ptr[j + 1] - o);
+    for (int q = 0; q < len; ++q) {
+      idx_out[o + q] = rows[j * cap + q];
+      val_out[o + q] = vals[j * cap + q];
+    }
+  }
+}
+
+int CapZ(const FusedMrProblem& p) {
+  const int64_t bound = 1 + static_cast<int64_t>(p.topk) * p.a_longest;
+  return static_cast<int>(std::min<int64_t>(p.n, bound));
+}
+
+int NextPow2Int(int v) {
+  int p = 1;
+  while (p < v) p <<= 1;
+  return p;
+}
+
+std::atomic<bool> g_fused_mr_enabled{true};
+
+template <class T>
+class FusedMr final : public FusedMrBase {
+ public:
+  ~FusedMr() override {
+    if (exec_ != nullptr) cudaGraphExecDestroy(exec_);
+  }
+
+  FusedMrOutcome Run(Ctx& ctx, const FusedMrProblem& problem, void* m_csc, const void* z_csc, double alpha,
+                     std::vector<SingleIterationData>& history) override {
+    FusedMrOutcome outcome;
+    if (!FusedMrApplicable(problem)) return outcome;
+    auto& m = *static_cast<DevCsc<T>*>(m_csc);
+    const auto& z = *static_cast<const DevCsc<T>*>(z_csc);
+    const int64_t n = problem.n;
+    Reserve(ctx, problem);
+    Configure(problem);
+    const cudaStream_t st = ctx.stream;
+    // state: iteration 0 is in the history; M^T set 0 is filled below
+    FusedState init{};
+    init.alpha = alpha;
+    init.nnz_dir = static_cast<unsigned long long>(z.nnz);
+    *host_state_ = init;
+    SPAI_CUDA(cudaMemcpyAsync(state_.data(), host_state_, sizeof(FusedState), cudaMemcpyHostToDevice, st));
+    for (int s = 0; s < 2; ++s) SPAI_CUDA(cudaMemsetAsync(mt_cnt_[s].data(), 0, sizeof(int32_t) * n, st));
+    SPAI_CUDA(cudaMemsetAsync(zt_cnt_.data(), 0, sizeof(int32_t) * n, st));
+    const int grid = GridFor(n, 128);
+    ToSlotsKernel<T><<<grid, 128, 0, st>>>(View(m), args_.topk, args_.m_rows, args_.m_vals, args_.m_cnt, args_.cap_mt,
+                                           args_.mt_cols[0], args_.mt_vals[0], args_.mt_cnt[0], args_.state);
+    SPAI_LAUNCH_CHECK();
+    ToSlotsKernel<T><<<grid, 128, 0, st>>>(View(z), args_.cap_z, args_.z_rows, args_.z_vals, args_.z_cnt,
+                                           args_.cap_zt, args_.zt_cols, args_.zt_vals, args_.zt_cnt, args_.state);
+    SPAI_LAUNCH_CHECK();
+    FusedState out;
+    if (prof::Enabled()) {
+      out = RunStepwise(ctx, problem, m.nnz, z.nnz);
+    } else {
+      if (exec_ == nullptr) Capture();
+      {
+        prof::Scope scope(st, "fused_mr_loop", 0.0);
+        SPAI_CUDA(cudaGraphLaunch(exec_, st));
+      }
+      SPAI_CUDA(cudaMemcpyAsync(host_state_, state_.data(), sizeof(FusedState), cudaMemcpyDeviceToHost, st));
+      ctx.Sync();
+      out = *host_state_;
+      CountLaunches(3 * out.bodies);
+    }
+    outcome.ran = true;
+    outcome.graph_bodies = out.bodies;
+    if (out.stop == kOverflowStop || out.overflow != 0) {
+      outcome.overflow = true;
+      return outcome;
+    }
+    const int64_t rows = out.iteration;
+    std::vector<FusedRow> host_rows(static_cast<size_t>(rows + 1));
+    SPAI_CUDA(cudaMemcpyAsync(host_rows.data(), args_.history, sizeof(FusedRow) * (rows + 1), cudaMemcpyDeviceToHost,
+                              st));
+    // M back to compact CSC
+    DevCsc<T> result;
+    result.Shape(n, n, st);
+    ctx.counts.Reserve(static_cast<size_t>(n + 1), st);
+    WidenCountsKernel<<<GridFor(n, 256), 256, 0, st>>>(args_.m_cnt, n, ctx.counts.data());
+    SPAI_LAUNCH_CHECK();
+    const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), n, result.ptr.data());
+    result.ReserveNnz(nnz, st);
+    FromSlotsKernel<T><<<grid, 128, 0, st>>>(n, args_.topk, args_.m_rows, args_.m_vals, result.ptr.data(),
+                                             result.idx.data(), result.val.data());
+    SPAI_LAUNCH_CHECK();
+    m.Swap(result);
+    ctx.Sync();
+    for (int64_t r = 1; r <= rows; ++r) {
+      SingleIterationData row;
+      row.iteration = host_rows[r].iteration;
+      row.residual_norm = host_rows[r].residual_norm;
+      row.density_m = host_rows[r].density_m;
+      row.density_direction = host_rows[r].density_direction;
+      history.push_back(row);
+    }
+    outcome.iterations = rows;
+    outcome.converged = out.stop == kConverged;
+    return outcome;
+  }
+
+ private:
+  // The same three kernels launched one by one with the library's CUDA-event
+  // accounting around each (spai_profile_enable): the decide kernel's result
+  // is read back after every iteration, in place of the graph's condition.
+  FusedState RunStepwise(Ctx& ctx, const FusedMrProblem& p, int64_t m_nnz, int64_t z_nnz) {
+    const cudaStream_t st = ctx.stream;
+    const double e = static_cast<double>(sizeof(T) + sizeof(int32_t));
+    const double n = static_cast<double>(p.n);
+    const double a_bytes = static_cast<double>(p.a_nnz) * e + 8.0 * (n + 1.0);
+    double m_prev = static_cast<double>(m_nnz);
+    double z_prev = static_cast<double>(z_nnz);
+    FusedState out{};
+    for (int64_t body = 0; body <= p.max_iterations; ++body) {
+      {
+        prof::Scope scope(st, "fused_drop", 0.0);
+        FusedDropKernel<T><<<drop_grid_, kDropWarps * kWarp, drop_smem_, st>>>(args_);
+        SPAI_LAUNCH_CHECK();
+      }
+      {
+        prof::Scope scope(st, "fused_residual", 0.0);
+        res_kernel_<<<res_grid_, kResidualWarps * kWarp, res_smem_, st>>>(args_);
+        SPAI_LAUNCH_CHECK();
+      }
+      {
+        prof::Scope scope(st, "fused_decide", 24.0 * n);
+        FusedDecideKernel<T><<<decide_grid_, kTreeLanes, 0, st>>>(args_, 0, false);
+        SPAI_LAUNCH_CHECK();
+      }
+      SPAI_CUDA(cudaMemcpyAsync(host_state_, state_.data(), sizeof(FusedState), cudaMemcpyDeviceToHost, st));
+      ctx.Sync();
+      out = *host_state_;
+      // algorithmic bytes: the drop step reads M, Z and both transposes and writes M and M^T; the
+      // residual step reads M, A and Pr, writes Z, Z^T and the three column sums
+      const double m_new = static_cast<double>(out.last_nnz_m);
+      const double z_new = static_cast<double>(out.last_nnz_z);
+      prof::AddBytes("fused_drop", e * (2.0 * m_prev + 2.0 * z_prev + 2.0 * m_new) + 4.0 * 6.0 * n);
+      prof::AddBytes("fused_residual",
+                     e * m_new + a_bytes + sizeof(T) * n + 2.0 * e * z_new + 4.0 * 3.0 * n + 24.0 * n);
+      m_prev = m_new;
+      z_prev = z_new;
+      if (out.stop != kRunning) break;
+    }
+    return out;
+  }
+
+  void Reserve(Ctx& ctx, const FusedMrProblem& p) {
+    const cudaStream_t st = ctx.stream;
+    const int64_t n = p.n;
+    const int cap_z = CapZ(p);
+    const int cap_mt = static_cast<int>(std::min<int64_t>(n, 4 * static_cast<int64_t>(p.topk)));
+    const int cap_zt = static_cast<int>(std::min<int64_t>(n, 2 * static_cast<int64_t>(cap_z)));
+    const size_t un = static_cast<size_t>(n);
+    m_rows_.Reserve(un * p.topk, st);
+    m_vals_.Reserve(un * p.topk, st);
+    m_cnt_.Reserve(un, st);
+    for (int s = 0; s < 2; ++s) {
+      mt_cols_[s].Reserve(un * cap_mt, st);
+      mt_vals_[s].Reserve(un * cap_mt, st);
+      mt_cnt_[s].Reserve(un, st);
+    }
+    z_rows_.Reserve(un * cap_z, st);
+    z_vals_.Reserve(un * cap_z, st);
+    z_cnt_.Reserve(un, st);
+    zt_cols_.Reserve(un * cap_zt, st);
+    zt_vals_.Reserve(un * cap_zt, st);
+    zt_cnt_.Reserve(un, st);
+    sq_.Reserve(un, st);
+    tt_.Reserve(un, st);
+    bt_.Reserve(un, st);
+    chunk_.Reserve(static_cast<size_t>(3 * CeilDiv(n, kTreeChunk)), st);
+    history_.Reserve(static_cast<size_t>(p.max_iterations + 1), st);
+    state_.Reserve(1, st);
+    if (host_state_ == nullptr) {
+      SPAI_CUDA(cudaMallocHost(reinterpret_cast<void**>(&host_state_), sizeof(FusedState)));
+      host_state_holder_.reset(host_state_);
+    }
+    FusedArgs<T> a{};
+    a.n = n;
+    a.topk = p.topk;
+    a.cap_z = cap_z;
+    a.cap_mt = cap_mt;
+    a.cap_zt = cap_zt;
+    a.ell = p.ell_width;
+    a.m_hash_slots = NextPow2Int(std::max(4 * p.topk, kWarp));
+    a.z_hash_slots = NextPow2Int(std::max(2 * cap_z, kWarp));
+    a.max_iterations = p.max_iterations;
+    a.tolerance = p.tolerance;
+    a.a_cols_ell = p.a_cols_ell;
+    a.a_rows_ell = p.a_rows_ell;
+    a.a_rows_ell_val = static_cast<const T*>(p.a_rows_ell_val);
+    a.pr = static_cast<const T*>(p.pr);
+    a.m_rows = m_rows_.data();
+    a.m_vals = m_vals_.data();
+    a.m_cnt = m_cnt_.data();
+    for (int s = 0; s < 2; ++s) {
+      a.mt_cols[s] = mt_cols_[s].data();
+      a.mt_vals[s] = mt_vals_[s].data();
+      a.mt_cnt[s] = mt_cnt_[s].data();
+    }
+    a.z_rows = z_rows_.data();
+    a.z_vals = z_vals_.data();
+    a.z_cnt = z_cnt_.data();
+    a.zt_cols = zt_cols_.data();
+    a.zt_vals = zt_vals_.data();
+    a.zt_cnt = zt_cnt_.data();
+    a.sq = sq_.data();
+    a.tt = tt_.data();
+    a.bt = bt_.data();
+    a.chunk = chunk_.data();
+    a.history = history_.data();
+    a.state = state_.data();
+    // a captured graph holds the old pointers and sizes: capture again on any change
+    if (exec_ != nullptr && !SameArgs(a, args_)) {
+      cudaGraphExecDestroy(exec_);
+      exec_ = nullptr;
+    }
+    args_ = a;
+  }
+
+  static bool SameArgs(const FusedArgs<T>& x, const FusedArgs<T>& y) {
+    bool same = x.n == y.n && x.topk == y.topk && x.cap_z == y.cap_z && x.cap_mt == y.cap_mt &&
+                x.cap_zt == y.cap_zt && x.ell == y.ell && x.m_hash_slots == y.m_hash_slots &&
+                x.z_hash_slots == y.z_hash_slots && x.max_iterations == y.max_iterations &&
+                x.tolerance == y.tolerance && x.a_cols_ell == y.a_cols_ell && x.a_rows_ell == y.a_rows_ell &&
+                x.a_rows_ell_val == y.a_rows_ell_val && x.pr == y.pr && x.m_rows == y.m_rows &&
+                x.m_vals == y.m_vals && x.m_cnt == y.m_cnt && x.z_rows == y.z_rows && x.z_vals == y.z_vals &&
+                x.z_cnt == y.z_cnt && x.zt_cols == y.zt_cols && x.zt_vals == y.zt_vals && x.zt_cnt == y.zt_cnt &&
+                x.sq == y.sq && x.tt == y.tt && x.bt == y.bt && x.chunk == y.chunk && x.history == y.history &&
+                x.state == y.state;
+    for (int s = 0; s < 2; ++s) {
+      same = same && x.mt_cols[s] == y.mt_cols[s] && x.mt_vals[s] == y.mt_vals[s] && x.mt_cnt[s] == y.mt_cnt[s];
+    }
+    return same;
+  }
+
+  // Kernel choice, shared memory and grids (once per problem shape).
+  void Configure(const FusedMrProblem& p) {
+    switch (p.ell_width) {
+      case 4: res_kernel_ = FusedResidualKernel<T, 4>; break;
+      case 8: res_kernel_ = FusedResidualKernel<T, 8>; break;
+      case 12: res_kernel_ = FusedResidualKernel<T, 12>; break;
+      case 16: res_kernel_ = FusedResidualKernel<T, 16>; break;
+      default: throw std::invalid_argument("fused MR: unsupported ELL width");
+    }
+    drop_smem_ = static_cast<size_t>(kDropWarps) * (DropSlabBytes() + DropSidesBytes<T>());
+    res_smem_ = static_cast<size_t>(kResidualWarps) * ResidualSlabBytes<T>(args_.m_hash_slots, args_.z_hash_slots);
+    SPAI_CUDA(cudaFuncSetAttribute(FusedDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(drop_smem_)));
+    SPAI_CUDA(cudaFuncSetAttribute(res_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   static_cast<int>(res_smem_)));
+    int drop_blocks = 0;
+    int res_blocks = 0;
+    SPAI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&drop_blocks, FusedDropKernel<T>, kDropWarps * kWarp,
+                                                            drop_smem_));
+    SPAI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&res_blocks, res_kernel_, kResidualWarps * kWarp,
+                                                            res_smem_));
+    if (drop_blocks < 1 || res_blocks < 1) throw std::runtime_error("fused MR: kernels do not fit on an SM");
+    int device = 0;
+    SPAI_CUDA(cudaGetDevice(&device));
+    int sms = 0;
+    SPAI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    drop_grid_ = static_cast<unsigned>(std::min<int64_t>(CeilDiv(args_.n, kDropWarps), int64_t{sms} * drop_blocks));
+    res_grid_ =
+        static_cast<unsigned>(std::min<int64_t>(CeilDiv(args_.n, kResidualWarps), int64_t{sms} * res_blocks));
+    decide_grid_ = static_cast<unsigned>(CeilDiv(args_.n, kTreeChunk));
+  }
+
+  void Capture() {
+    const FusedArgs<T> a = args_;
+    cudaStream_t cs = nullptr;
+    cudaStream_t bs = nullptr;
+    cudaGraph_t graph = nullptr;
+    SPAI_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    try {
+      SPAI_CUDA(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking));
+      SPAI_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+      cudaStreamCaptureStatus status;
+      cudaGraph_t capture_graph = nullptr;
+      const cudaGraphNode_t* deps = nullptr;
+      size_t num_deps = 0;
+      SPAI_CUDA(cudaStreamGetCaptureInfo(cs, &status, nullptr, &capture_graph, &deps, &num_deps));
+      cudaGraphConditionalHandle loop;
+      SPAI_CUDA(cudaGraphConditionalHandleCreate(&loop, capture_graph, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams params = {};
+      params.type = cudaGraphNodeTypeConditional;
+      params.conditional.handle = loop;
+      params.conditional.type = cudaGraphCondTypeWhile;
+      params.conditional.size = 1;
+      cudaGraphNode_t loop_node;
+      SPAI_CUDA(cudaGraphAddNode(&loop_node, capture_graph, deps, num_deps, &params));
+      SPAI_CUDA(cudaStreamUpdateCaptureDependencies(cs, &loop_node, 1, cudaStreamSetCaptureDependencies));
+      cudaGraph_t body = params.conditional.phGraph_out[0];
+      SPAI_CUDA(cudaStreamBeginCaptureToGraph(bs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+      FusedDropKernel<T><<<drop_grid_, kDropWarps * kWarp, drop_smem_, bs>>>(a);
+      res_kernel_<<<res_grid_, kResidualWarps * kWarp, res_smem_, bs>>>(a);
+      FusedDecideKernel<T><<<decide_grid_, kTreeLanes, 0, bs>>>(a, loop, true);
+      SPAI_CUDA(cudaGetLastError());
+      cudaGraph_t body_out = nullptr;
+      SPAI_CUDA(cudaStreamEndCapture(bs, &body_out));
+      SPAI_CUDA(cudaStreamEndCapture(cs, &graph));
+      SPAI_CUDA(cudaGraphInstantiate(&exec_, graph, 0));
+    } catch (...) {
+      cudaStreamCaptureStatus st;
+      for (cudaStream_t stream : {bs, cs}) {
+        if (stream != nullptr && cudaStreamIsCapturing(stream, &st) == cudaSuccess &&
+            st != cudaStreamCaptureStatusNone) {
+          cudaGraph_t dropped = nullptr;
+          cudaStreamEndCapture(stream, &dropped);
+          if (dropped != nullptr && stream == cs) cudaGraphDestroy(dropped);
+        }
+      }
+      if (graph != nullptr) cudaGraphDestroy(graph);
+      if (bs != nullptr) cudaStreamDestroy(bs);
+      cudaStreamDestroy(cs);
+      cudaGetLastError();
+      exec_ = nullptr;
+      throw;
+    }
+    cudaGraphDestroy(graph);
+    cudaStreamDestroy(bs);
+    cudaStreamDestroy(cs);
+  }
+
+  struct PinnedFree {
+    void operator()(FusedState* p) const { cudaFreeHost(p); }
+  };
+
+  DevBuf<int32_t> m_rows_, m_cnt_, z_rows_, z_cnt_, zt_cols_, zt_cnt_;
+  DevBuf<T> m_vals_, z_vals_, zt_vals_;
+  DevBuf<int32_t> mt_cols_[2], mt_cnt_[2];
+  DevBuf<T> mt_vals_[2];
+  DevBuf<double> sq_, tt_, bt_, chunk_;
+  DevBuf<FusedRow> history_;
+  DevBuf<FusedState> state_;
+  FusedState* host_state_ = nullptr;
+  std::unique_ptr<FusedState, PinnedFree> host_state_holder_;
+  FusedArgs<T> args_{};
+  cudaGraphExec_t exec_ = nullptr;
+  void (*res_kernel_)(FusedArgs<T>) = nullptr;
+  size_t drop_smem_ = 0;
+  size_t res_smem_ = 0;
+  unsigned drop_grid_ = 1;
+  unsigned res_grid_ = 1;
+  unsigned decide_grid_ = 1;
+};
+
+}  // namespace
+
+bool FusedMrEnabled() { return g_fused_mr_enabled.load(std::memory_order_relaxed); }
+void SetFusedMrEnabled(bool enabled) { g_fused_mr_enabled.store(enabled, std::memory_order_relaxed); }
+
+bool FusedMrApplicable(const FusedMrProblem& p) {
+  if (p.n <= 0 || p.n > kTreeChunk * kTreeChunk) return false;
+  if (p.topk <= 0 || p.topk > kMaxTopK) return false;
+  if (p.ell_width != 4 && p.ell_width != 8 && p.ell_width != 12 && p.ell_width != 16) return false;
+  if (p.a_longest <= 0 || p.a_longest > p.ell_width) return false;
+  if (p.max_iterations < 1) return false;
+  const int cap_z = CapZ(p);
+  // the own side of a drop column and a product column's row lists must fit
+  if (p.topk + cap_z > kSideCap) return false;
+  if (static_cast<int64_t>(cap_z) * p.a_longest > kRowsCap) return false;
+  return true;
+}
+
+template <class T>
+std::unique_ptr<FusedMrBase> MakeFusedMr() {
+  return std::unique_ptr<FusedMrBase>(new FusedMr<T>());
+}
+
+template std::unique_ptr<FusedMrBase> MakeFusedMr<double>();
+template std::unique_ptr<FusedMrBase> MakeFusedMr<float>();
+
+}  // namespace spai

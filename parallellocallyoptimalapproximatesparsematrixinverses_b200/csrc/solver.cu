@@ -16,6 +16,7 @@
 
 #include "cod2x2.cuh"
 #include "device.cuh"
+#include "mr_fused.cuh"
 #include "ops.cuh"
 #include "solver.cuh"
 #include "spgemm.cuh"
@@ -334,6 +335,16 @@ class Solver final : public SolverBase {
   }
 
   void Run() override {
+    RunOnce();
+    if (fused_overflowed_) {
+      // a column outgrew the fused loop's slots: the same solve on the unfused kernels (same bits)
+      fused_allowed_ = false;
+      RunOnce();
+    }
+  }
+
+  void RunOnce() {
+    fused_overflowed_ = false;
     history_.clear();
     converged_ = false;
     iterations_ = 0;
@@ -707,6 +718,7 @@ class Solver final : public SolverBase {
                               ctx_.stream));
     ctx_.Sync();
     const int64_t longest = ctx_.host_counts[2];
+    a_longest_ = longest;
     if (longest > kMaxEllWidth) return;
     const int width = static_cast<int>(std::max<int64_t>(4, (longest + 3) / 4 * 4));
     const size_t slots = static_cast<size_t>(n_) * static_cast<size_t>(width);
@@ -1048,6 +1060,37 @@ class Solver final : public SolverBase {
     double num = 0.0;
     double den = 0.0;
     MrProjection(num, den);
+    if (FusedEligible()) {
+      // iterations 1.. as one CUDA graph of fused kernels (mr_fused.cu): same arithmetic, same bits
+      if (opt_.max_iterations < 1 || !FiniteNonZeroHost(den)) return;
+      const double alpha = num / den;
+      if (!std::isfinite(alpha)) return;
+      FusedMrProblem problem;
+      problem.n = n_;
+      problem.topk = static_cast<int>(opt_.topk);
+      problem.a_nnz = a64_.nnz;
+      problem.a_longest = a_longest_;
+      problem.ell_width = ell_width_;
+      problem.a_cols_ell = a_cols_ell_.data();
+      problem.a_rows_ell = a_rows_ell_.data();
+      problem.a_rows_ell_val = a_rows_ell_val_.data();
+      problem.pr = pr_vec_.data();
+      problem.max_iterations = opt_.max_iterations;
+      problem.tolerance = opt_.tolerance;
+      if (FusedMrApplicable(problem)) {
+        if (!fused_) fused_ = MakeFusedMr<T>();
+        const FusedMrOutcome outcome = fused_->Run(ctx_, problem, &m_, &z_, alpha, history_);
+        if (outcome.ran) {
+          if (outcome.overflow) {
+            fused_overflowed_ = true;
+            return;
+          }
+          iterations_ = outcome.iterations;
+          converged_ = outcome.converged;
+          return;
+        }
+      }
+    }
     for (int64_t i = 1; i <= opt_.max_iterations; ++i) {
       if (!FiniteNonZeroHost(den)) break;
       const double alpha = num / den;
@@ -1200,6 +1243,12 @@ class Solver final : public SolverBase {
     }
   }
 
+  // Global MR with per-column top-k, a diagonal Pr and ELL copies of A, in the device order.
+  bool FusedEligible() const {
+    return FusedMrEnabled() && fused_allowed_ && opt_.method == Method::kGlobalMr && opt_.dropping &&
+           opt_.topk > 0 && pr_diagonal_ && !ReferenceOrder() && ell_width_ > 0 && symmetric_;
+  }
+
   double* ColVec(int i) {
     ctx_.colvec[i].Reserve(static_cast<size_t>(n_), ctx_.stream);
     return ctx_.colvec[i].data();
@@ -1224,7 +1273,11 @@ class Solver final : public SolverBase {
   DevBuf<int32_t> a_rows_ell_;
   DevBuf<T> a_rows_ell_val_;
   int ell_width_ = 0;
+  int64_t a_longest_ = 0;  // longest column or row of A
   static constexpr int kMaxEllWidth = 16;
+  std::unique_ptr<FusedMrBase> fused_;
+  bool fused_allowed_ = true;
+  bool fused_overflowed_ = false;
   DevCsc<T> z_fused_;             // Pr*R written by the last residual product
   bool r_squares_ready_ = false;  // Partial(kResidualPartial) holds R's column squares
   bool z_fused_ready_ = false;

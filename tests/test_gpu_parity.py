@@ -165,3 +165,58 @@ def test_fp64_dense_column_global_hash_fallback(require_gpu, family, name):
     got, want = _run_both(family, name, A, M0, None, max_iterations=2, tolerance=1e-12, max_density=1.0,
                           enable_dropping=False)
     assert_same_result(got, want, f"{family}.{name} dense column")
+
+
+FUSED_CASES = {
+    # 3-D 7-point, top-8: windows of several planes
+    "diffusion_3d_16_top8": (lambda: problems.diffusion_3d(16, 1.0, 5), 8, 12),
+    # 2-D 5-point, top-10, the reference's CPU-runnable shape
+    "laplacian_64_top10": (lambda: problems.laplacian_2d(64), 10, 20),
+    # a larger 3-D problem with the bench's top-16, a few iterations
+    "diffusion_3d_40_top16": (lambda: problems.diffusion_3d(40, 1.0, 2), 16, 6),
+}
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("case", sorted(FUSED_CASES))
+def test_fused_graph_mr_matches_unfused_kernels(require_gpu, case, precision):
+    """Global MR with per-column top-k runs its iterations as one CUDA graph of
+    fused kernels (mr_fused.cu); switched off, the same run goes through the
+    unfused kernels.  Both must give the same bits: M and the whole history."""
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import _lib
+    maker, topk, iterations = FUSED_CASES[case]
+    A = maker()
+    n = A.shape[0]
+    kw = dict(M0=problems.diagonal_inverse(A), max_iterations=iterations, tolerance=1e-12,
+              max_density=topk / n, topk_per_column=topk, precision=precision, summation="device")
+    lib = _lib.load()
+    lib.spai_set_fused_mr(0)
+    try:
+        want = global_spai.mr(A, **kw)
+    finally:
+        lib.spai_set_fused_mr(1)
+    got = global_spai.mr(A, **kw)
+    assert_same_result(got, want, f"{case} {precision}")
+    if precision == "fp64":
+        oracle = pyoracle.run("global_spai", "mr", A, M0=kw["M0"], max_iterations=iterations, tolerance=1e-12,
+                              max_density=topk / n, topk_per_column=topk, order=pyoracle.ORDER_DEVICE)
+        assert_same_result(got, oracle, f"{case} against the oracle")
+
+
+def test_fused_graph_mr_profiled_steps_match(require_gpu):
+    """With the library's event accounting on, the fused kernels run one launch
+    at a time (no graph); the results are the same bits."""
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import _lib
+    A = problems.diffusion_3d(16, 1.0, 5)
+    n = A.shape[0]
+    kw = dict(M0=problems.diagonal_inverse(A), max_iterations=8, tolerance=1e-12, max_density=8 / n,
+              topk_per_column=8, precision="mixed")
+    lib = _lib.load()
+    want = global_spai.mr(A, **kw)
+    lib.spai_profile_reset()
+    lib.spai_profile_enable(1)
+    try:
+        got = global_spai.mr(A, **kw)
+    finally:
+        lib.spai_profile_enable(0)
+    assert_same_result(got, want, "profiled fused steps")
