@@ -277,6 +277,14 @@ void* spai_session_stream(SpaiSession* session);
  * path and releases what it held; the library stays usable. */
 void spai_inject_allocation_failure(int64_t after);
 
+/* The device's minimum-norm 2x2 least-squares solve (the per-column step of
+ * Inner-Outer LOMR, reference src/common/sparse_operations.cpp:58-73) on
+ * `count` systems: gram holds 4 doubles per system (row-major), rhs 2, out
+ * receives 2 (host arrays).  Exposes the device arithmetic to tests of the
+ * singular and non-finite branches.  Returns 0, or -1 with `error`. */
+int64_t spai_solve_2x2_device(int64_t count, const double* gram, const double* rhs, double* out, char* error,
+                              int64_t error_capacity);
+
 /* Number of kernels this library has launched since load (diagnostics). */
 int64_t spai_kernel_launches(void);
 

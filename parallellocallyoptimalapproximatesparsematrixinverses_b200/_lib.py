@@ -84,7 +84,7 @@ EXPORTED_SYMBOLS = (
     "spai_profile_read", "spai_pcg_device_noalloc", "spai_residual_adjoint", "spai_pcg_adjoint",
     "spai_mr_batched", "spai_mtx_read", "spai_mtx_write", "spai_free_int64_array", "spai_free_double_array",
     "spai_session_create_device", "spai_session_result_device", "spai_inject_allocation_failure",
-    "spai_set_fused_mr",
+    "spai_set_fused_mr", "spai_solve_2x2_device",
 )
 
 _lib = None
@@ -141,6 +141,8 @@ def _declare(lib) -> None:
     lib.spai_inject_allocation_failure.argtypes = [_i64]
     lib.spai_set_fused_mr.restype = None
     lib.spai_set_fused_mr.argtypes = [_i64]
+    lib.spai_solve_2x2_device.restype = _i64
+    lib.spai_solve_2x2_device.argtypes = [_i64, _pf64, _pf64, _pf64, ctypes.c_char_p, _i64]
     lib.spai_session_create_device.restype = ctypes.c_void_p
     lib.spai_session_create_device.argtypes = [_i64, _i64, _i64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                                _i64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, MethodParams,

@@ -14,6 +14,8 @@
 #include <thread>
 #include <vector>
 
+// cod2x2.cuh first: its arithmetic helpers must not see device.cuh's overloads
+#include "cod2x2.cuh"
 #include "../../include/methods_c_api.h"
 #include "../../include/spai_b200.h"
 #include "adjoint.cuh"
@@ -403,6 +405,49 @@ void free_mem(Result* result) {
 }
 
 void spai_inject_allocation_failure(int64_t after) { spai::g_fail_after.store(after, std::memory_order_relaxed); }
+
+namespace spai {
+namespace {
+// The device's 2x2 minimum-norm solve (the Inner-Outer LOMR step) on `count` systems.
+__global__ void Solve2x2Kernel(int64_t count, const double* __restrict__ gram, const double* __restrict__ rhs,
+                               double* __restrict__ out) {
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < count;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    double m[4] = {gram[4 * i], gram[4 * i + 1], gram[4 * i + 2], gram[4 * i + 3]};
+    double x[2] = {rhs[2 * i], rhs[2 * i + 1]};
+    double y[2];
+    SolveLeastSquares2x2(m, x, y);
+    out[2 * i] = y[0];
+    out[2 * i + 1] = y[1];
+  }
+}
+}  // namespace
+}  // namespace spai
+
+int64_t spai_solve_2x2_device(int64_t count, const double* gram, const double* rhs, double* out, char* error,
+                              int64_t error_capacity) {
+  try {
+    if (count <= 0 || gram == nullptr || rhs == nullptr || out == nullptr) {
+      throw std::invalid_argument("count must be positive and every array given");
+    }
+    spai::CtxGuard guard(spai::ResolveDevice(-1));
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevBuf<double> g, r, o;
+    g.Reserve(static_cast<size_t>(4 * count), ctx.stream);
+    r.Reserve(static_cast<size_t>(2 * count), ctx.stream);
+    o.Reserve(static_cast<size_t>(2 * count), ctx.stream);
+    SPAI_CUDA(cudaMemcpyAsync(g.data(), gram, sizeof(double) * 4 * count, cudaMemcpyHostToDevice, ctx.stream));
+    SPAI_CUDA(cudaMemcpyAsync(r.data(), rhs, sizeof(double) * 2 * count, cudaMemcpyHostToDevice, ctx.stream));
+    spai::Solve2x2Kernel<<<spai::GridFor(count, 128), 128, 0, ctx.stream>>>(count, g.data(), r.data(), o.data());
+    SPAI_LAUNCH_CHECK();
+    SPAI_CUDA(cudaMemcpyAsync(out, o.data(), sizeof(double) * 2 * count, cudaMemcpyDeviceToHost, ctx.stream));
+    ctx.Sync();
+    return 0;
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
 
 void spai_free_int64_array(int64_t* array) { delete[] array; }
 
