@@ -299,6 +299,7 @@ def run_ours(args):
     achieved = dom.get("gbs") or 0.0
     traffic = ncu_traffic(dominant) if dominant else None
 
+    mixed_error = mixed_vs_fp64(sessions, results) if rank == 0 else None
     line = None
     if rank == 0:
         rows = results["mixed"]
@@ -354,9 +355,6 @@ def run_ours(args):
             "clocks": clocks.summary(),
             "gpu_launches": launches,
         }
-    mixed_error = None
-    if rank == 0:
-        mixed_error = mixed_vs_fp64(sessions, results)
     for s in sessions.values():
         s.close()
 
