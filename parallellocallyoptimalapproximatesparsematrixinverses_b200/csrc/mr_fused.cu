@@ -36,7 +36,8 @@ namespace {
 
 constexpr int kDropWarps = 8;       // warps per block of the drop kernel
 constexpr int kResidualWarps = 4;   // warps per block of the residual kernel
-constexpr int kWindowWords = 2048;  // row window of the residual kernel's bitmaps (65,536 rows)
+constexpr int kWindowWords = 1024;  // bitmap words of the residual kernel: windows of 32,768 rows
+constexpr int kWindowRows = kWindowWords * 32;
 constexpr int kRowsCap = 1024;      // longest row list of one product column
 constexpr int kSideCap = 256;       // longest own / transposed side of a drop column
 constexpr int kMaxTopK = 32;
@@ -45,7 +46,6 @@ constexpr int kMaxTopK = 32;
 constexpr int kOverflowMt = 1;      // a row of M^T exceeded cap_mt
 constexpr int kOverflowZt = 2;      // a row of Z^T exceeded cap_zt
 constexpr int kOverflowSide = 4;    // a drop column exceeded kSideCap or kDropCap
-constexpr int kOverflowWindow = 8;  // a product column's rows spanned more than the window
 
 // Stop codes (FusedState::stop).
 constexpr int kRunning = 0;
@@ -468,18 +468,6 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
     }
     lo = __reduce_min_sync(0xffffffffu, lo);
     hi = __reduce_max_sync(0xffffffffu, hi);
-    const int words = (hi - lo) / 32 + 1;
-    if (words > kWindowWords) {
-      overflow |= kOverflowWindow;
-      continue;
-    }
-    if (lane == 0) MarkRow(bm, summary, static_cast<int>(j) - lo);
-#pragma unroll
-    for (int u = 0; u < kEll; ++u) {
-      if (cand[u] >= 0) MarkRow(bm, summary, cand[u] - lo);
-    }
-    __syncwarp();
-    const int count = DrainRows(bm, summary, SummaryWords(words), rows, lane);
     int32_t* zr_out = a.z_rows + j * a.cap_z;
     T* zv_out = a.z_vals + j * a.cap_z;
     ClearTable(zkeys, a.z_hash_slots, lane);
@@ -487,54 +475,66 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
     int kept = 0;
     double sq = 0.0;
     bool z_placed = true;
-    for (int r0 = 0; r0 < count; r0 += kWarp) {
-      const int r = r0 + lane;
-      bool keep = false;
-      int32_t i = 0;
-      T v = T(0);
-      if (r < count) {
-        i = lo + static_cast<int32_t>(rows[r]);
-        T acc = T(-0.0);
-        const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
-        const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
+    // the rows in ascending order, one window of kWindowRows rows at a time
+    for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
+      const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
+      const int words = (seg_hi - seg_lo) / 32 + 1;
+      if (lane == 0 && j >= seg_lo && j <= seg_hi) MarkRow(bm, summary, static_cast<int>(j - seg_lo));
 #pragma unroll
-        for (int u = 0; u < kEll / 4; ++u) {
-          const int4 k4 = ks[u];
-          T v4[4];
-          LoadFour(vs + 4 * u, v4);
-          const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+      for (int u = 0; u < kEll; ++u) {
+        if (cand[u] >= seg_lo && cand[u] <= seg_hi) MarkRow(bm, summary, cand[u] - seg_lo);
+      }
+      __syncwarp();
+      const int count = DrainRows(bm, summary, SummaryWords(words), rows, lane);
+      for (int r0 = 0; r0 < count; r0 += kWarp) {
+        const int r = r0 + lane;
+        bool keep = false;
+        int32_t i = 0;
+        T v = T(0);
+        if (r < count) {
+          i = seg_lo + static_cast<int32_t>(rows[r]);
+          T acc = T(-0.0);
+          const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
+          const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            T bv;
-            if (kk[e] >= 0 && BucketFind(mkeys, mvals, mbits, m_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
+          for (int u = 0; u < kEll / 4; ++u) {
+            const int4 k4 = ks[u];
+            T v4[4];
+            LoadFour(vs + 4 * u, v4);
+            const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+              T bv;
+              if (kk[e] >= 0 && BucketFind(mkeys, mvals, mbits, m_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
+            }
+          }
+          v = -acc;
+          if (static_cast<int64_t>(i) == j) v = Add(v, T(1));
+          const double sd = static_cast<double>(v);
+          stage0[lane] = Mul(sd, sd);
+          keep = !(v == T(0));  // Eigen prune(0.0)
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int o = kept + __popc(mask & LaneMaskBelow());
+          const T z = Mul(a.pr[i], v);
+          zr_out[o] = i;
+          zv_out[o] = z;
+          zlist[o] = i;
+          z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
+          const int slot = atomicAdd(&a.zt_cnt[i], 1);
+          if (slot < a.cap_zt) {
+            a.zt_cols[static_cast<int64_t>(i) * a.cap_zt + slot] = static_cast<int32_t>(j);
+            a.zt_vals[static_cast<int64_t>(i) * a.cap_zt + slot] = z;
+          } else {
+            overflow |= kOverflowZt;
           }
         }
-        v = -acc;
-        if (static_cast<int64_t>(i) == j) v = Add(v, T(1));
-        const double sd = static_cast<double>(v);
-        stage0[lane] = Mul(sd, sd);
-        keep = !(v == T(0));  // Eigen prune(0.0)
+        kept += __popc(mask);
+        __syncwarp();
+        if (lane == 0) sq = SumStaged(sq, stage0, min(kWarp, count - r0));
+        __syncwarp();
       }
-      const unsigned mask = __ballot_sync(0xffffffffu, keep);
-      if (keep) {
-        const int o = kept + __popc(mask & LaneMaskBelow());
-        const T z = Mul(a.pr[i], v);
-        zr_out[o] = i;
-        zv_out[o] = z;
-        zlist[o] = i;
-        z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
-        const int slot = atomicAdd(&a.zt_cnt[i], 1);
-        if (slot < a.cap_zt) {
-          a.zt_cols[static_cast<int64_t>(i) * a.cap_zt + slot] = static_cast<int32_t>(j);
-          a.zt_vals[static_cast<int64_t>(i) * a.cap_zt + slot] = z;
-        } else {
-          overflow |= kOverflowZt;
-        }
-      }
-      kept += __popc(mask);
-      __syncwarp();
-      if (lane == 0) sq = SumStaged(sq, stage0, min(kWarp, count - r0));
-      __syncwarp();
     }
     if (lane == 0) {
       a.sq[j] = sq;
@@ -564,21 +564,19 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
     hi = __reduce_max_sync(0xffffffffu, hi);
     double tt = 0.0;
     double bt = 0.0;
-    if (hi >= lo) {
-      const int words2 = (hi - lo) / 32 + 1;
-      if (words2 > kWindowWords) {
-        overflow |= kOverflowWindow;
-        continue;
-      }
+    for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
+      const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
+      const int words2 = (seg_hi - seg_lo) / 32 + 1;
       for (int e = lane; e < kept; e += kWarp) {
         const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zlist[e]) * kEll);
 #pragma unroll
         for (int u = 0; u < kEll / 4; ++u) {
           const int4 r4 = src[u];
-          if (r4.x >= 0) MarkRow(bm, summary, r4.x - lo);
-          if (r4.y >= 0) MarkRow(bm, summary, r4.y - lo);
-          if (r4.z >= 0) MarkRow(bm, summary, r4.z - lo);
-          if (r4.w >= 0) MarkRow(bm, summary, r4.w - lo);
+          const int32_t rr[4] = {r4.x, r4.y, r4.z, r4.w};
+#pragma unroll
+          for (int t = 0; t < 4; ++t) {
+            if (rr[t] >= seg_lo && rr[t] <= seg_hi) MarkRow(bm, summary, rr[t] - seg_lo);
+          }
         }
       }
       __syncwarp();
@@ -586,7 +584,7 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
       for (int r0 = 0; r0 < count2; r0 += kWarp) {
         const int r = r0 + lane;
         if (r < count2) {
-          const int32_t i = lo + static_cast<int32_t>(rows[r]);
+          const int32_t i = seg_lo + static_cast<int32_t>(rows[r]);
           T acc = T(-0.0);
           const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
           const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;

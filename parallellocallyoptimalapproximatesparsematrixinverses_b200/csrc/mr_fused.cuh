@@ -20,8 +20,8 @@
 // size is read back and no allocation happens inside the loop.  Every value
 // is formed with the same operations, in the same order, as the unfused
 // kernels (update.cu, spgemm.cu), so results are bit-identical.  A column
-// that does not fit its slots or windows flags an overflow: the loop stops
-// and the caller reruns the solve on the unfused path.
+// that does not fit its slots flags an overflow: the loop stops and the
+// caller reruns the solve on the unfused path.
 
 #include <cuda_runtime.h>
 
