@@ -909,6 +909,32 @@ int WarpsPerBlock(const void* kernel, size_t per_warp) {
   return warps;
 }
 
+// Block sizes of the column kernel, chosen by timing.  The first launch of a
+// (kernel, shared-memory slab) pair over at least kTuneMinColumns columns runs
+// the bin once with every block size whose slabs fit (1, 2, 4 or 8 warps),
+// timed with CUDA events on the launching stream; the fastest is kept for the
+// process.  The kernel writes the same outputs whatever its block size, so
+// the trial launches change no result.  Smaller launches use the block size
+// of highest occupancy until a tuned one exists.
+constexpr int64_t kTuneMinColumns = 8192;
+
+struct TunedWarps {
+  std::mutex mutex;
+  std::map<std::pair<const void*, size_t>, int> chosen;
+};
+
+TunedWarps& Tuned() {
+  static TunedWarps* table = new TunedWarps();  // kept for the process: launches may run during exit
+  return *table;
+}
+
+int LookUpTuned(const void* kernel, size_t per_warp) {
+  TunedWarps& t = Tuned();
+  std::lock_guard<std::mutex> lock(t.mutex);
+  const auto it = t.chosen.find(std::make_pair(kernel, per_warp));
+  return it == t.chosen.end() ? 0 : it->second;
+}
+
 // The column path: one launch per populated bitmap bin, over that bin's
 // column list (written by NeedKernel), with the bin's shared-memory layout.
 template <class T>
@@ -927,14 +953,51 @@ void LaunchColumnProducts(Ctx& ctx, const ColumnArgs<T>& args, const unsigned lo
       case 16: kernel = ColumnProductKernel<T, 16>; break;
       default: break;
     }
-    const int warps = WarpsPerBlock(reinterpret_cast<const void*>(kernel), per_warp);
-    const size_t smem = per_warp * static_cast<size_t>(warps);
-    SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     const int32_t* list = ctx.sg_bin_cols.data() + static_cast<int64_t>(bin) * args.b.cols;
-    kernel<<<GridFor(population * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(args, list, population,
-                                                                                           words_cap, rows_cap,
-                                                                                           hash_slots);
-    SPAI_LAUNCH_CHECK();
+    const void* key = reinterpret_cast<const void*>(kernel);
+    auto launch = [&](int warps) {
+      const size_t smem = per_warp * static_cast<size_t>(warps);
+      SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+      kernel<<<GridFor(population * kWarp, warps * kWarp), warps * kWarp, smem, ctx.stream>>>(
+          args, list, population, words_cap, rows_cap, hash_slots);
+      SPAI_LAUNCH_CHECK();
+    };
+    int warps = LookUpTuned(key, per_warp);
+    if (warps == 0 && population >= kTuneMinColumns) {
+      cudaEvent_t start = nullptr;
+      cudaEvent_t stop = nullptr;
+      SPAI_CUDA(cudaEventCreate(&start));
+      SPAI_CUDA(cudaEventCreate(&stop));
+      float best_ms = 0.0f;
+      for (int w = 1; w <= 8; w <<= 1) {
+        const size_t bytes = per_warp * static_cast<size_t>(w);
+        if (bytes > static_cast<size_t>(200 * 1024)) break;
+        SPAI_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(bytes)));
+        int blocks = 0;
+        SPAI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kernel, w * kWarp, bytes));
+        if (blocks < 1) break;
+        SPAI_CUDA(cudaEventRecord(start, ctx.stream));
+        launch(w);
+        SPAI_CUDA(cudaEventRecord(stop, ctx.stream));
+        SPAI_CUDA(cudaEventSynchronize(stop));
+        float ms = 0.0f;
+        SPAI_CUDA(cudaEventElapsedTime(&ms, start, stop));
+        if (warps == 0 || ms < best_ms) {
+          best_ms = ms;
+          warps = w;
+        }
+      }
+      cudaEventDestroy(start);
+      cudaEventDestroy(stop);
+      if (warps != 0) {
+        TunedWarps& t = Tuned();
+        std::lock_guard<std::mutex> lock(t.mutex);
+        t.chosen[std::make_pair(key, per_warp)] = warps;
+        continue;  // the trial launches already wrote this bin's outputs
+      }
+    }
+    if (warps == 0) warps = WarpsPerBlock(key, per_warp);
+    launch(warps);
   }
 }
 
