@@ -5,11 +5,11 @@
 //   M^T  two sets (the drop kernel reads one and writes the other), cap_mt
 //        slots per row in arrival order, count per row
 //   Z    cap_z slots per column, rows ascending (Z = Pr R keeps R's pattern)
-//   Z^T  cap_zt slots per row in arrival order
-// The drop kernel consumes Z, Z^T and the current M^T set and clears their
-// counts as it reads them (each count belongs to one column's warp), so the
-// residual kernel refills Z^T and the next drop kernel fills the other M^T
-// set without a separate clearing pass.
+// Z is never transposed: the drop kernel needs row j of Z only for column j,
+// and forms it from the rows of M it has (M^T) and row j of A, with the same
+// products in the same order as the residual kernel's column of R.  The
+// residual kernel clears the M^T set the drop kernel has just read, so the
+// next drop kernel fills it again from zero.
 
 #include <cuda_runtime.h>
 
@@ -39,13 +39,13 @@ constexpr int kResidualWarps = 4;   // warps per block of the residual kernel
 constexpr int kWindowWords = 1024;  // bitmap words of the residual kernel: windows of 32,768 rows
 constexpr int kWindowRows = kWindowWords * 32;
 constexpr int kRowsCap = 1024;      // longest row list of one product column
-constexpr int kSideCap = 256;       // longest own / transposed side of a drop column
 constexpr int kMaxTopK = 32;
+constexpr int kDropRowsCap = 512;  // candidate rows of one drop column; also bounds Z's slots per column
 
 // Overflow bits (FusedState::overflow).
 constexpr int kOverflowMt = 1;      // a row of M^T exceeded cap_mt
-constexpr int kOverflowZt = 2;      // a row of Z^T exceeded cap_zt
-constexpr int kOverflowSide = 4;    // a drop column exceeded kSideCap or kDropCap
+constexpr int kOverflowRow = 2;     // row j of R had more entries than its hash takes
+constexpr int kOverflowSide = 4;    // a drop column's merged rows exceeded kDropCap
 
 // Stop codes (FusedState::stop).
 constexpr int kRunning = 0;
@@ -84,10 +84,13 @@ struct FusedArgs {
   int topk;
   int cap_z;
   int cap_mt;
-  int cap_zt;
   int ell;  // ELL slots of A (multiple of 4)
-  int m_hash_slots;
-  int z_hash_slots;
+  int m_hash_slots;   // residual kernel: M(:, j)
+  int z_hash_slots;   // residual kernel: Z(:, j)
+  int d_mc_slots;     // drop kernel: M(:, j)
+  int d_zc_slots;     // drop kernel: Z(:, j)
+  int d_mt_slots;     // drop kernel: M(j, :)
+  int d_r_slots;      // drop kernel: R(j, :)
   int64_t max_iterations;
   double tolerance;
   const int32_t* a_cols_ell;
@@ -103,9 +106,6 @@ struct FusedArgs {
   int32_t* z_rows;
   T* z_vals;
   int32_t* z_cnt;
-  int32_t* zt_cols;
-  T* zt_vals;
-  int32_t* zt_cnt;
   double* sq;          // per-column sum of squares of R
   double* tt;          // per-column ||Pr A Z(:, j)||^2
   double* bt;          // per-column <Z(:, j), Pr A Z(:, j)>
@@ -116,133 +116,109 @@ struct FusedArgs {
 
 // ---------------------------------------------------------------------------
 // Drop kernel: per column j, S = 0.5 (U(:, j) + U(j, :)^T) with U = M + alpha Z.
+//
+// Four small hashes in shared memory hold M(:, j) and Z(:, j) (the column's
+// slots), M(j, :) (row j of M, from M^T) and R(j, :).  Row j of R is formed
+// here: for the entries k of row j of A in ascending order, every entry
+// M(k, i) of row k of M adds A(j, k) M(k, i) to R(j, i) -- for each i the
+// terms arrive in ascending k, exactly the sum the residual kernel forms for
+// R(j, i) in column i.  The candidate rows i of S(:, j) (the keys of the four
+// hashes, and j) are marked in a window bitmap and read back in ascending
+// order; each one's U(i, j), U(j, i) and S(i, j) come from hash lookups, with
+// the union's and the symmetrisation's arithmetic (UnionPadded,
+// SymmetrizeDropKernel).  Exact zeros of U are not pruned here: an entry that
+// is zero on both sides gives S(i, j) = 0, which the drop rule removes, and a
+// zero on one side gives the same half sum as an absent one, so the kept
+// entries and their order are the unfused kernels'.
 
-struct DropSides {
-  int32_t* own_rows;  // U(:, j): rows of M(:, j) and Z(:, j), merged
-  void* own_vals;
-  int32_t* tr_rows;   // U(j, :)^T: columns of M(j, :) and Z(j, :), merged
-  void* tr_vals;
-};
+// Returns the slot of key (inserted when absent: *fresh), or -1 when the table is full.
+__device__ __forceinline__ int FindOrInsert(int32_t* keys, int bits, int32_t key, bool* fresh) {
+  const uint32_t mask = (1u << bits) - 1u;
+  uint32_t h = (static_cast<uint32_t>(key) * 2654435761u) >> (32 - bits);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const int32_t old = atomicCAS(&keys[h], kEmpty, key);
+    if (old == kEmpty) {
+      *fresh = true;
+      return static_cast<int>(h);
+    }
+    if (old == key) {
+      *fresh = false;
+      return static_cast<int>(h);
+    }
+    h = (h + 1u) & mask;
+  }
+  *fresh = false;
+  return -1;
+}
 
-template <class T>
-__host__ __device__ constexpr size_t DropSidesBytes() {
-  return 2 * Round16Bytes(kSideCap * sizeof(int32_t)) + 2 * Round16Bytes(kSideCap * sizeof(T));
+__device__ __forceinline__ int FindSlot(const int32_t* keys, int bits, int32_t key) {
+  const uint32_t mask = (1u << bits) - 1u;
+  uint32_t h = (static_cast<uint32_t>(key) * 2654435761u) >> (32 - bits);
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    const int32_t k = keys[h];
+    if (k == key) return static_cast<int>(h);
+    if (k == kEmpty) return -1;
+    h = (h + 1u) & mask;
+  }
+  return -1;
 }
 
 template <class T>
-__device__ DropSides SidesFor(unsigned char* base) {
-  DropSides d;
-  d.own_rows = reinterpret_cast<int32_t*>(base);
-  base += Round16Bytes(kSideCap * sizeof(int32_t));
-  d.own_vals = base;
-  base += Round16Bytes(kSideCap * sizeof(T));
-  d.tr_rows = reinterpret_cast<int32_t*>(base);
-  base += Round16Bytes(kSideCap * sizeof(int32_t));
-  d.tr_vals = base;
-  return d;
-}
-
-// pre[q] = number of the first q keys of x (sorted) found in y (sorted), q = 0..nx.
-__device__ __forceinline__ int MatchedPrefixShared(const int32_t* yk, int ny, const int32_t* xk, int nx, int* pre,
-                                                   int lane) {
-  int running = 0;
-  for (int base = 0; base < nx; base += kWarp) {
-    const int q = base + lane;
-    bool hit = false;
-    if (q < nx) {
-      const int32_t row = xk[q];
-      const int r = LowerBoundShared(yk, ny, row);
-      hit = r < ny && yk[r] == row;
-    }
-    const unsigned mask = __ballot_sync(0xffffffffu, hit);
-    if (q < nx) pre[q] = running + __popc(mask & LaneMaskBelow());
-    running += __popc(mask);
-  }
-  if (lane == 0) pre[nx] = running;
-  __syncwarp();
-  return running;
-}
-
-// Builds U(j, :)^T from M^T(:, j) (nmt entries) and Z^T(:, j) (nzt entries),
-// rows ascending, into d.tr_rows / d.tr_vals; returns its length.  The
-// entries arrive in any order: (column, source) keys are sorted in registers.
-template <class T, int R>
-__device__ int BuildTransposed(const FusedArgs<T>& a, int64_t parity, int64_t j, int nmt, int nzt, T alpha,
-                               DropSides& d, int lane) {
-  const int nt = nmt + nzt;
-  const int32_t* mt_cols = a.mt_cols[parity] + j * a.cap_mt;
-  const T* mt_vals = a.mt_vals[parity] + j * a.cap_mt;
-  const int32_t* zt_cols = a.zt_cols + j * a.cap_zt;
-  const T* zt_vals = a.zt_vals + j * a.cap_zt;
-  unsigned long long k[R];
-  uint32_t p[R];
-#pragma unroll
-  for (int t = 0; t < R; ++t) {
-    const int e = t * kWarp + lane;
-    if (e < nmt) {
-      k[t] = static_cast<unsigned long long>(static_cast<uint32_t>(mt_cols[e])) << 1;
-    } else if (e < nt) {
-      k[t] = (static_cast<unsigned long long>(static_cast<uint32_t>(zt_cols[e - nmt])) << 1) | 1ull;
-    } else {
-      k[t] = ~0ull;
-    }
-    p[t] = static_cast<uint32_t>(e);
-  }
-  WarpBitonicSort<R>(k, p, lane);
-  T* tr_vals = static_cast<T*>(d.tr_vals);
-  int filled = 0;
-#pragma unroll
-  for (int t = 0; t < R; ++t) {
-    // the next element in the sorted order (t * 32 + lane + 1) and the previous one
-    unsigned long long next_k = __shfl_down_sync(0xffffffffu, k[t], 1);
-    uint32_t next_p = __shfl_down_sync(0xffffffffu, p[t], 1);
-    unsigned long long prev_k = __shfl_up_sync(0xffffffffu, k[t], 1);
-    const unsigned long long wrap_next_k = t + 1 < R ? __shfl_sync(0xffffffffu, k[t + 1 < R ? t + 1 : t], 0) : ~0ull;
-    const uint32_t wrap_next_p = t + 1 < R ? __shfl_sync(0xffffffffu, p[t + 1 < R ? t + 1 : t], 0) : 0u;
-    const unsigned long long wrap_prev_k = t > 0 ? __shfl_sync(0xffffffffu, k[t > 0 ? t - 1 : t], kWarp - 1) : ~0ull;
-    if (lane == kWarp - 1) {
-      next_k = wrap_next_k;
-      next_p = wrap_next_p;
-    }
-    if (lane == 0) prev_k = wrap_prev_k;
-    const bool valid = k[t] != ~0ull;
-    const uint32_t row = static_cast<uint32_t>(k[t] >> 1);
-    const bool from_z = (k[t] & 1ull) != 0;
-    // a row appears at most once from M^T and once from Z^T, the M entry first
-    const bool head = valid && (!from_z || prev_k == ~0ull || static_cast<uint32_t>(prev_k >> 1) != row ||
-                                (prev_k & 1ull) != 0);
-    T v = T(0);
-    if (head) {
-      if (!from_z) {
-        const T mv = mt_vals[p[t]];
-        const bool pair = next_k != ~0ull && static_cast<uint32_t>(next_k >> 1) == row && (next_k & 1ull) != 0;
-        // the union's arithmetic (UnionPadded): y + a x, y + 0, 0 + a x
-        v = pair ? Add(mv, Mul(alpha, zt_vals[next_p - nmt])) : Add(mv, T(0));
-      } else {
-        v = Add(T(0), Mul(alpha, zt_vals[p[t] - nmt]));
-      }
-    }
-    const unsigned mask = __ballot_sync(0xffffffffu, head);
-    if (head) {
-      const int at = filled + __popc(mask & LaneMaskBelow());
-      d.tr_rows[at] = static_cast<int32_t>(row);
-      tr_vals[at] = v;
-    }
-    filled += __popc(mask);
-  }
-  __syncwarp();
-  return filled;
+__host__ __device__ size_t DropWarpBytes(int mc, int zc, int mt, int r) {
+  constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
+  return Round16(static_cast<size_t>(kWindowWords) * 4) + Round16(static_cast<size_t>(kSummary) * 4) +
+         Round16(static_cast<size_t>(kDropRowsCap) * 2) +
+         Round16(static_cast<size_t>(mc + zc + mt + r) * 4) + Round16(static_cast<size_t>(mc + zc + mt + r) * sizeof(T)) +
+         Round16(kDropCap * sizeof(double)) + Round16(kDropCap * sizeof(int32_t)) + Round16(kDropCap) +
+         Round16(4 * kWarp * sizeof(int32_t));
 }
 
 template <class T>
 __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<T> a) {
   extern __shared__ __align__(16) unsigned char fused_drop_smem[];
+  constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
   const int lane = threadIdx.x & 31;
-  unsigned char* base = fused_drop_smem + (threadIdx.x >> 5) * (DropSlabBytes() + DropSidesBytes<T>());
-  DropSlab s = SlabFor(base);
-  DropSides d = SidesFor<T>(base + DropSlabBytes());
+  const int table = a.d_mc_slots + a.d_zc_slots + a.d_mt_slots + a.d_r_slots;
+  unsigned char* base =
+      fused_drop_smem + (threadIdx.x >> 5) * DropWarpBytes<T>(a.d_mc_slots, a.d_zc_slots, a.d_mt_slots, a.d_r_slots);
+  uint32_t* bm = reinterpret_cast<uint32_t*>(base);
+  base += Round16(static_cast<size_t>(kWindowWords) * 4);
+  uint32_t* summary = reinterpret_cast<uint32_t*>(base);
+  base += Round16(static_cast<size_t>(kSummary) * 4);
+  uint16_t* rows = reinterpret_cast<uint16_t*>(base);
+  base += Round16(static_cast<size_t>(kDropRowsCap) * 2);
+  int32_t* keys = reinterpret_cast<int32_t*>(base);  // the four tables, one after another
+  base += Round16(static_cast<size_t>(table) * 4);
+  T* vals = reinterpret_cast<T*>(base);
+  base += Round16(static_cast<size_t>(table) * sizeof(T));
+  DropSlab s;
+  s.vals = reinterpret_cast<double*>(base);
+  base += Round16(kDropCap * sizeof(double));
+  s.keys = reinterpret_cast<int32_t*>(base);
+  base += Round16(kDropCap * sizeof(int32_t));
+  s.keep = base;
+  base += Round16(kDropCap);
+  s.xk = reinterpret_cast<int32_t*>(base);  // staging of the top-k selection
+  s.yk = s.xk;
+  s.mx_prefix = nullptr;
+  int32_t* k_mc = keys;
+  int32_t* k_zc = k_mc + a.d_mc_slots;
+  int32_t* k_mt = k_zc + a.d_zc_slots;
+  int32_t* k_r = k_mt + a.d_mt_slots;
+  T* v_mc = vals;
+  T* v_zc = v_mc + a.d_mc_slots;
+  T* v_mt = v_zc + a.d_zc_slots;
+  T* v_r = v_mt + a.d_mt_slots;
+  const int b_mc = Log2(a.d_mc_slots);
+  const int b_zc = Log2(a.d_zc_slots);
+  const int b_mt = Log2(a.d_mt_slots);
+  const int b_r = Log2(a.d_r_slots);
+  const int r_limit = a.d_r_slots / 2;  // distinct keys of R(j, :) the table takes
+  ClearWords(bm, kWindowWords, lane);
+  ClearWords(summary, kSummary, lane);
   FusedState* state = a.state;
   const int64_t parity = state->parity;
+  const int64_t other = parity ^ 1;
   const T alpha = static_cast<T>(state->alpha);
   const int64_t warp = (static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x) >> 5;
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
@@ -251,92 +227,178 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
   for (int64_t j = warp; j < a.n; j += warps) {
     const int nm = a.m_cnt[j];
     const int nz = a.z_cnt[j];
-    const int nmt_all = a.mt_cnt[parity][j];
-    const int nzt_all = a.zt_cnt[j];
-    __syncwarp();
-    if (lane == 0) {
-      // this column's transposed rows are consumed here: their sets refill from zero
-      a.mt_cnt[parity][j] = 0;
-      a.zt_cnt[j] = 0;
-    }
-    if (nmt_all > a.cap_mt || nzt_all > a.cap_zt || nm + nz > kSideCap || nmt_all + nzt_all > kSideCap) {
-      overflow |= kOverflowSide;
+    const int nmt = a.mt_cnt[parity][j];
+    if (nmt > a.cap_mt) {
+      overflow |= kOverflowMt;
       continue;
     }
-    // own side U(:, j) = M(:, j) (+) alpha Z(:, j)
+    ClearTable(keys, table, lane);
+    __syncwarp();
+    // M(:, j), Z(:, j), M(j, :)
     const int32_t* mr = a.m_rows + j * a.topk;
     const T* mv = a.m_vals + j * a.topk;
     const int32_t* zr = a.z_rows + j * a.cap_z;
     const T* zv = a.z_vals + j * a.cap_z;
-    for (int i = lane; i < nm; i += kWarp) s.yk[i] = mr[i];
-    for (int i = lane; i < nz; i += kWarp) s.xk[i] = zr[i];
-    __syncwarp();
-    const int matched = MatchedPrefixShared(s.yk, nm, s.xk, nz, s.mx_prefix, lane);
-    const int no = nm + nz - matched;
-    T* own_vals = static_cast<T*>(d.own_vals);
+    const int32_t* mtc = a.mt_cols[parity] + j * a.cap_mt;
+    const T* mtv = a.mt_vals[parity] + j * a.cap_mt;
+    int32_t lo = static_cast<int32_t>(j);
+    int32_t hi = static_cast<int32_t>(j);
+    bool fresh;
     for (int e = lane; e < nm; e += kWarp) {
-      const int32_t row = s.yk[e];
-      const int r = LowerBoundShared(s.xk, nz, row);
-      const T y = mv[e];
-      const T v = (r < nz && s.xk[r] == row) ? Add(y, Mul(alpha, zv[r])) : Add(y, T(0));
-      const int rank = e + r - s.mx_prefix[r];
-      d.own_rows[rank] = row;
-      own_vals[rank] = v;
+      const int at = FindOrInsert(k_mc, b_mc, mr[e], &fresh);
+      v_mc[at] = mv[e];
+      lo = min(lo, mr[e]);
+      hi = max(hi, mr[e]);
     }
-    for (int q = lane; q < nz; q += kWarp) {
-      const int32_t row = s.xk[q];
-      const int r = LowerBoundShared(s.yk, nm, row);
-      if (r < nm && s.yk[r] == row) continue;
-      const int rank = q - s.mx_prefix[q] + r;
-      d.own_rows[rank] = row;
-      own_vals[rank] = Add(T(0), Mul(alpha, zv[q]));
+    for (int e = lane; e < nz; e += kWarp) {
+      const int at = FindOrInsert(k_zc, b_zc, zr[e], &fresh);
+      v_zc[at] = zv[e];
+      lo = min(lo, zr[e]);
+      hi = max(hi, zr[e]);
     }
-    // transposed side U(j, :)^T
-    const int nt = nmt_all + nzt_all;
-    int ntr;
-    if (nt <= kWarp) {
-      ntr = BuildTransposed<T, 1>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
-    } else if (nt <= 2 * kWarp) {
-      ntr = BuildTransposed<T, 2>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
-    } else if (nt <= 4 * kWarp) {
-      ntr = BuildTransposed<T, 4>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
-    } else {
-      ntr = BuildTransposed<T, 8>(a, parity, j, nmt_all, nzt_all, alpha, d, lane);
+    for (int e = lane; e < nmt; e += kWarp) {
+      const int at = FindOrInsert(k_mt, b_mt, mtc[e], &fresh);
+      v_mt[at] = mtv[e];
+      lo = min(lo, mtc[e]);
+      hi = max(hi, mtc[e]);
     }
-    __syncwarp();
-    // S(:, j) = 0.5 (own + transposed), merged in row order into the slab
-    const int matched2 = MatchedPrefixShared(d.own_rows, no, d.tr_rows, ntr, s.mx_prefix, lane);
-    const int count = no + ntr - matched2;
-    if (count > kDropCap) {
-      overflow |= kOverflowSide;
+    // R(j, :) = e_j^T - A(j, :) M: terms in ascending k for every column i
+    int r_keys = 0;
+    bool r_full = false;
+    for (int u = 0; u < a.ell; ++u) {
+      const int32_t k = a.a_rows_ell[j * a.ell + u];
+      if (k < 0) continue;  // warp-uniform
+      const T a_jk = a.a_rows_ell_val[j * a.ell + u];
+      const int nk = a.mt_cnt[parity][k];
+      if (nk > a.cap_mt) {
+        r_full = true;
+        break;
+      }
+      const int32_t* kc = a.mt_cols[parity] + static_cast<int64_t>(k) * a.cap_mt;
+      const T* kv = a.mt_vals[parity] + static_cast<int64_t>(k) * a.cap_mt;
+      for (int e0 = 0; e0 < nk; e0 += kWarp) {
+        const int e = e0 + lane;
+        bool is_new = false;
+        bool lost = false;
+        if (e < nk) {
+          const int32_t i = kc[e];
+          const T prod = Mul(a_jk, kv[e]);
+          const int at = FindOrInsert(k_r, b_r, i, &is_new);
+          if (at < 0) {
+            lost = true;
+          } else {
+            // a column i appears once in row k of M: no two lanes share a slot here
+            v_r[at] = is_new ? prod : Add(v_r[at], prod);
+            lo = min(lo, i);
+            hi = max(hi, i);
+          }
+        }
+        r_keys += __popc(__ballot_sync(0xffffffffu, is_new));
+        if (__any_sync(0xffffffffu, lost)) r_full = true;
+      }
       __syncwarp();
+      if (r_full || r_keys > r_limit) break;
+    }
+    if (r_full || r_keys > r_limit) {
+      overflow |= kOverflowRow;
       continue;
     }
-    const T* tr_vals = static_cast<const T*>(d.tr_vals);
-    for (int e = lane; e < no; e += kWarp) {
-      const int32_t row = d.own_rows[e];
-      const int r = LowerBoundShared(d.tr_rows, ntr, row);
-      const T y = own_vals[e];
-      // the half sum of the symmetrisation (dropping.cpp:106-120)
-      const T v = (r < ntr && d.tr_rows[r] == row) ? Mul(T(0.5), Add(y, tr_vals[r])) : Mul(T(0.5), Add(y, T(0)));
-      const int rank = e + r - s.mx_prefix[r];
-      s.keys[rank] = row;
-      s.vals[rank] = static_cast<double>(v);
+    lo = __reduce_min_sync(0xffffffffu, lo);
+    hi = __reduce_max_sync(0xffffffffu, hi);
+    // S(:, j) in row order, one window of kWindowRows rows at a time
+    int count = 0;
+    bool too_long = false;
+    for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
+      const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
+      const int words = (seg_hi - seg_lo) / 32 + 1;
+      if (lane == 0 && j >= seg_lo && j <= seg_hi) MarkRow(bm, summary, static_cast<int>(j - seg_lo));
+      for (int t = lane; t < table; t += kWarp) {
+        const int32_t key = keys[t];
+        if (key != kEmpty && key >= seg_lo && key <= seg_hi) MarkRow(bm, summary, key - seg_lo);
+      }
+      __syncwarp();
+      const int found = DrainRows(bm, summary, SummaryWords(words), rows, lane);
+      if (count + found > kDropCap || found > kDropRowsCap) {
+        too_long = true;
+        break;
+      }
+      for (int r0 = 0; r0 < found; r0 += kWarp) {
+        const int r = r0 + lane;
+        bool emit = false;
+        int32_t i = 0;
+        T v = T(0);
+        if (r < found) {
+          i = seg_lo + static_cast<int32_t>(rows[r]);
+          // U(i, j) = M(i, j) (+) alpha Z(i, j)
+          const int pm = FindSlot(k_mc, b_mc, i);
+          const int pz = FindSlot(k_zc, b_zc, i);
+          const bool own = pm >= 0 || pz >= 0;
+          T u_own = T(0);
+          if (pm >= 0 && pz >= 0) {
+            u_own = Add(v_mc[pm], Mul(alpha, v_zc[pz]));
+          } else if (pm >= 0) {
+            u_own = Add(v_mc[pm], T(0));
+          } else if (pz >= 0) {
+            u_own = Add(T(0), Mul(alpha, v_zc[pz]));
+          }
+          // U(j, i) = M(j, i) (+) alpha Z(j, i), Z(j, i) = pr_j R(j, i) unless R(j, i) is an exact zero
+          const int pmt = FindSlot(k_mt, b_mt, i);
+          const int pr = FindSlot(k_r, b_r, i);
+          bool z_row = false;
+          T z_ji = T(0);
+          if (pr >= 0 || static_cast<int64_t>(i) == j) {
+            T rv = pr >= 0 ? -v_r[pr] : T(0);
+            if (static_cast<int64_t>(i) == j) rv = Add(rv, T(1));
+            if (!(rv == T(0))) {
+              z_row = true;
+              z_ji = Mul(a.pr[j], rv);
+            }
+          }
+          const bool trans = pmt >= 0 || z_row;
+          T u_tr = T(0);
+          if (pmt >= 0 && z_row) {
+            u_tr = Add(v_mt[pmt], Mul(alpha, z_ji));
+          } else if (pmt >= 0) {
+            u_tr = Add(v_mt[pmt], T(0));
+          } else if (z_row) {
+            u_tr = Add(T(0), Mul(alpha, z_ji));
+          }
+          // the half sum of the symmetrisation (dropping.cpp:106-120)
+          if (own && trans) {
+            v = Mul(T(0.5), Add(u_own, u_tr));
+          } else if (own) {
+            v = Mul(T(0.5), Add(u_own, T(0)));
+          } else if (trans) {
+            v = Mul(T(0.5), Add(T(0), u_tr));
+          }
+          emit = own || trans;
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, emit);
+        if (emit) {
+          const int o = count + __popc(mask & LaneMaskBelow());
+          s.keys[o] = i;
+          s.vals[o] = static_cast<double>(v);
+        }
+        count += __popc(mask);
+      }
+      __syncwarp();
     }
-    for (int q = lane; q < ntr; q += kWarp) {
-      const int32_t row = d.tr_rows[q];
-      const int r = LowerBoundShared(d.own_rows, no, row);
-      if (r < no && d.own_rows[r] == row) continue;
-      const int rank = q - s.mx_prefix[q] + r;
-      s.keys[rank] = row;
-      s.vals[rank] = static_cast<double>(Mul(T(0.5), Add(T(0), tr_vals[q])));
+    if (too_long) {
+      // leave the bitmap clear for the next column before skipping this one
+      for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
+        const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
+        ClearWords(bm, (seg_hi - seg_lo) / 32 + 1, lane);
+        ClearWords(summary, SummaryWords((seg_hi - seg_lo) / 32 + 1), lane);
+      }
+      __syncwarp();
+      overflow |= kOverflowSide;
+      continue;
     }
     __syncwarp();
     const int kept = DecideDrops(s, count, j, a.topk, lane);
     // survivors: M(:, j) in place, and M^T into the other set
     int32_t* out_rows = a.m_rows + j * a.topk;
     T* out_vals = a.m_vals + j * a.topk;
-    const int64_t other = parity ^ 1;
     int at = 0;
     for (int b0 = 0; b0 < count; b0 += kWarp) {
       const int i = b0 + lane;
@@ -381,7 +443,7 @@ __host__ __device__ size_t ResidualSlabBytes(int m_slots, int z_slots) {
   return Round16(static_cast<size_t>(kWindowWords) * 4) + Round16(static_cast<size_t>(SummaryWords(kWindowWords)) * 4) +
          Round16(static_cast<size_t>(kRowsCap) * 2) + Round16(static_cast<size_t>(m_slots) * 4) +
          Round16(static_cast<size_t>(m_slots) * sizeof(T)) + Round16(static_cast<size_t>(z_slots) * 4) +
-         Round16(static_cast<size_t>(z_slots) * sizeof(T)) + Round16(static_cast<size_t>(kSideCap) * 4) +
+         Round16(static_cast<size_t>(z_slots) * sizeof(T)) + Round16(static_cast<size_t>(kDropRowsCap) * 4) +
          2 * Round16(kWarp * sizeof(double));
 }
 
@@ -422,7 +484,7 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
   T* zvals = reinterpret_cast<T*>(base);
   base += Round16(static_cast<size_t>(a.z_hash_slots) * sizeof(T));
   int32_t* zlist = reinterpret_cast<int32_t*>(base);
-  base += Round16(static_cast<size_t>(kSideCap) * 4);
+  base += Round16(static_cast<size_t>(kDropRowsCap) * 4);
   double* stage0 = reinterpret_cast<double*>(base);
   double* stage1 = stage0 + kWarp;
   const int mbits = Log2(a.m_hash_slots) - 1;  // buckets of two slots
@@ -434,8 +496,10 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
   const int64_t warps = (static_cast<int64_t>(gridDim.x) * blockDim.x) >> 5;
   unsigned long long written = 0;
   int overflow = 0;
+  const int64_t read_set = a.state->parity;  // the M^T set the drop kernel has just read
   for (int64_t j = warp; j < a.n; j += warps) {
     // ---- R(:, j) = e_j - A M(:, j) ----------------------------------------
+    if (lane == 0) a.mt_cnt[read_set][j] = 0;  // that set refills from zero in the next drop kernel
     const int nm = a.m_cnt[j];
     ClearTable(mkeys, a.m_hash_slots, lane);
     __syncwarp();
@@ -522,13 +586,6 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
           zv_out[o] = z;
           zlist[o] = i;
           z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
-          const int slot = atomicAdd(&a.zt_cnt[i], 1);
-          if (slot < a.cap_zt) {
-            a.zt_cols[static_cast<int64_t>(i) * a.cap_zt + slot] = static_cast<int32_t>(j);
-            a.zt_vals[static_cast<int64_t>(i) * a.cap_zt + slot] = z;
-          } else {
-            overflow |= kOverflowZt;
-          }
         }
         kept += __popc(mask);
         __syncwarp();
@@ -789,6 +846,15 @@ int NextPow2Int(int v) {
   return p;
 }
 
+int CapMt(const FusedMrProblem& p) { return static_cast<int>(std::min<int64_t>(p.n, 4 * static_cast<int64_t>(p.topk))); }
+
+// Slots of the drop kernel's hash of R(j, :): twice the row's bound (every entry of row j of A times a row of M)
+// up to 256; a longer row flags an overflow.
+int DropRowSlots(const FusedMrProblem& p) {
+  const int64_t bound = static_cast<int64_t>(p.a_longest) * CapMt(p) + 1;
+  return NextPow2Int(static_cast<int>(std::min<int64_t>(std::max<int64_t>(2 * bound, kWarp), 256)));
+}
+
 std::atomic<bool> g_fused_mr_enabled{true};
 
 template <class T>
@@ -815,13 +881,12 @@ class FusedMr final : public FusedMrBase {
     *host_state_ = init;
     SPAI_CUDA(cudaMemcpyAsync(state_.data(), host_state_, sizeof(FusedState), cudaMemcpyHostToDevice, st));
     for (int s = 0; s < 2; ++s) SPAI_CUDA(cudaMemsetAsync(mt_cnt_[s].data(), 0, sizeof(int32_t) * n, st));
-    SPAI_CUDA(cudaMemsetAsync(zt_cnt_.data(), 0, sizeof(int32_t) * n, st));
     const int grid = GridFor(n, 128);
     ToSlotsKernel<T><<<grid, 128, 0, st>>>(View(m), args_.topk, args_.m_rows, args_.m_vals, args_.m_cnt, args_.cap_mt,
                                            args_.mt_cols[0], args_.mt_vals[0], args_.mt_cnt[0], args_.state);
     SPAI_LAUNCH_CHECK();
-    ToSlotsKernel<T><<<grid, 128, 0, st>>>(View(z), args_.cap_z, args_.z_rows, args_.z_vals, args_.z_cnt,
-                                           args_.cap_zt, args_.zt_cols, args_.zt_vals, args_.zt_cnt, args_.state);
+    ToSlotsKernel<T><<<grid, 128, 0, st>>>(View(z), args_.cap_z, args_.z_rows, args_.z_vals, args_.z_cnt, 0,
+                                           nullptr, nullptr, nullptr, args_.state);
     SPAI_LAUNCH_CHECK();
     FusedState out;
     if (prof::Enabled()) {
@@ -922,8 +987,7 @@ class FusedMr final : public FusedMrBase {
     const cudaStream_t st = ctx.stream;
     const int64_t n = p.n;
     const int cap_z = CapZ(p);
-    const int cap_mt = static_cast<int>(std::min<int64_t>(n, 4 * static_cast<int64_t>(p.topk)));
-    const int cap_zt = static_cast<int>(std::min<int64_t>(n, 2 * static_cast<int64_t>(cap_z)));
+    const int cap_mt = CapMt(p);
     const size_t un = static_cast<size_t>(n);
     m_rows_.Reserve(un * p.topk, st);
     m_vals_.Reserve(un * p.topk, st);
@@ -936,9 +1000,6 @@ class FusedMr final : public FusedMrBase {
     z_rows_.Reserve(un * cap_z, st);
     z_vals_.Reserve(un * cap_z, st);
     z_cnt_.Reserve(un, st);
-    zt_cols_.Reserve(un * cap_zt, st);
-    zt_vals_.Reserve(un * cap_zt, st);
-    zt_cnt_.Reserve(un, st);
     sq_.Reserve(un, st);
     tt_.Reserve(un, st);
     bt_.Reserve(un, st);
@@ -954,10 +1015,13 @@ class FusedMr final : public FusedMrBase {
     a.topk = p.topk;
     a.cap_z = cap_z;
     a.cap_mt = cap_mt;
-    a.cap_zt = cap_zt;
     a.ell = p.ell_width;
     a.m_hash_slots = NextPow2Int(std::max(4 * p.topk, kWarp));
     a.z_hash_slots = NextPow2Int(std::max(2 * cap_z, kWarp));
+    a.d_mc_slots = NextPow2Int(std::max(2 * p.topk, kWarp));
+    a.d_zc_slots = NextPow2Int(std::max(2 * cap_z, kWarp));
+    a.d_mt_slots = NextPow2Int(std::max(2 * cap_mt, kWarp));
+    a.d_r_slots = DropRowSlots(p);
     a.max_iterations = p.max_iterations;
     a.tolerance = p.tolerance;
     a.a_cols_ell = p.a_cols_ell;
@@ -975,9 +1039,6 @@ class FusedMr final : public FusedMrBase {
     a.z_rows = z_rows_.data();
     a.z_vals = z_vals_.data();
     a.z_cnt = z_cnt_.data();
-    a.zt_cols = zt_cols_.data();
-    a.zt_vals = zt_vals_.data();
-    a.zt_cnt = zt_cnt_.data();
     a.sq = sq_.data();
     a.tt = tt_.data();
     a.bt = bt_.data();
@@ -994,12 +1055,13 @@ class FusedMr final : public FusedMrBase {
 
   static bool SameArgs(const FusedArgs<T>& x, const FusedArgs<T>& y) {
     bool same = x.n == y.n && x.topk == y.topk && x.cap_z == y.cap_z && x.cap_mt == y.cap_mt &&
-                x.cap_zt == y.cap_zt && x.ell == y.ell && x.m_hash_slots == y.m_hash_slots &&
+                x.ell == y.ell && x.m_hash_slots == y.m_hash_slots && x.d_r_slots == y.d_r_slots &&
+                x.d_mc_slots == y.d_mc_slots && x.d_zc_slots == y.d_zc_slots && x.d_mt_slots == y.d_mt_slots &&
                 x.z_hash_slots == y.z_hash_slots && x.max_iterations == y.max_iterations &&
                 x.tolerance == y.tolerance && x.a_cols_ell == y.a_cols_ell && x.a_rows_ell == y.a_rows_ell &&
                 x.a_rows_ell_val == y.a_rows_ell_val && x.pr == y.pr && x.m_rows == y.m_rows &&
                 x.m_vals == y.m_vals && x.m_cnt == y.m_cnt && x.z_rows == y.z_rows && x.z_vals == y.z_vals &&
-                x.z_cnt == y.z_cnt && x.zt_cols == y.zt_cols && x.zt_vals == y.zt_vals && x.zt_cnt == y.zt_cnt &&
+                x.z_cnt == y.z_cnt &&
                 x.sq == y.sq && x.tt == y.tt && x.bt == y.bt && x.chunk == y.chunk && x.history == y.history &&
                 x.state == y.state;
     for (int s = 0; s < 2; ++s) {
@@ -1017,7 +1079,8 @@ class FusedMr final : public FusedMrBase {
       case 16: res_kernel_ = FusedResidualKernel<T, 16>; break;
       default: throw std::invalid_argument("fused MR: unsupported ELL width");
     }
-    drop_smem_ = static_cast<size_t>(kDropWarps) * (DropSlabBytes() + DropSidesBytes<T>());
+    drop_smem_ = static_cast<size_t>(kDropWarps) *
+                 DropWarpBytes<T>(args_.d_mc_slots, args_.d_zc_slots, args_.d_mt_slots, args_.d_r_slots);
     res_smem_ = static_cast<size_t>(kResidualWarps) * ResidualSlabBytes<T>(args_.m_hash_slots, args_.z_hash_slots);
     SPAI_CUDA(cudaFuncSetAttribute(FusedDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(drop_smem_)));
@@ -1100,8 +1163,8 @@ class FusedMr final : public FusedMrBase {
     void operator()(FusedState* p) const { cudaFreeHost(p); }
   };
 
-  DevBuf<int32_t> m_rows_, m_cnt_, z_rows_, z_cnt_, zt_cols_, zt_cnt_;
-  DevBuf<T> m_vals_, z_vals_, zt_vals_;
+  DevBuf<int32_t> m_rows_, m_cnt_, z_rows_, z_cnt_;
+  DevBuf<T> m_vals_, z_vals_;
   DevBuf<int32_t> mt_cols_[2], mt_cnt_[2];
   DevBuf<T> mt_vals_[2];
   DevBuf<double> sq_, tt_, bt_, chunk_;
@@ -1131,8 +1194,9 @@ bool FusedMrApplicable(const FusedMrProblem& p) {
   if (p.a_longest <= 0 || p.a_longest > p.ell_width) return false;
   if (p.max_iterations < 1) return false;
   const int cap_z = CapZ(p);
-  // the own side of a drop column and a product column's row lists must fit
-  if (p.topk + cap_z > kSideCap) return false;
+  // a drop column's candidate rows and a product column's row lists must fit
+  const int64_t drop_candidates = p.topk + cap_z + CapMt(p) + DropRowSlots(p) / 2 + 1;
+  if (drop_candidates > kDropRowsCap) return false;
   if (static_cast<int64_t>(cap_z) * p.a_longest > kRowsCap) return false;
   return true;
 }

@@ -6,17 +6,18 @@
 //
 // One iteration is three kernels:
 //   drop      M := top-k(threshold(0.5 (U + U^T))) with U = M + alpha Z formed
-//             on the fly from M, Z and their transposes (no union, no
-//             transpose pass over HBM); writes M in place and scatters M^T;
-//   residual  R = I - A M, Z = Pr R (written, and scattered as Z^T), the
-//             column squares of R, and the MR projection of A Z from the Z
-//             column still in shared memory (no second pass over Z);
+//             on the fly: column j from M's and Z's slots, row j from M^T and
+//             row j of A (row j of Z is recomputed, never transposed); writes
+//             M in place and scatters M^T;
+//   residual  R = I - A M, Z = Pr R written, the column squares of R, and the
+//             MR projection of A Z from the Z column still in shared memory
+//             (no second pass over Z);
 //   decide    the three fixed-tree reductions (||R||^2, <Z, Pr A Z>,
 //             ||Pr A Z||^2), the history row, the stop tests and the next
 //             step length, all on the device; it sets the condition of the
 //             CUDA graph's WHILE node that repeats the three kernels.
 // Matrices live in fixed-capacity column slots (M: topk per column; Z: the
-// bound 1 + topk * (longest column of A); transposes: per-row slots), so no
+// bound 1 + topk * (longest column of A); M^T: per-row slots), so no
 // size is read back and no allocation happens inside the loop.  Every value
 // is formed with the same operations, in the same order, as the unfused
 // kernels (update.cu, spgemm.cu), so results are bit-identical.  A column
