@@ -34,7 +34,9 @@ void CountLaunches(int64_t count);
 
 namespace {
 
-constexpr int kDropWarps = 8;       // warps per block of the drop kernel
+constexpr int kDropWarps = 4;       // warps per block of the drop kernel
+constexpr int kDropWindowWords = 512;  // bitmap words of the drop kernel: windows of 16,384 rows
+constexpr int kDropWindowRows = kDropWindowWords * 32;
 constexpr int kResidualWarps = 4;   // warps per block of the residual kernel
 constexpr int kWindowWords = 1024;  // bitmap words of the residual kernel: windows of 32,768 rows
 constexpr int kWindowRows = kWindowWords * 32;
@@ -87,8 +89,6 @@ struct FusedArgs {
   int ell;  // ELL slots of A (multiple of 4)
   int m_hash_slots;   // residual kernel: M(:, j)
   int z_hash_slots;   // residual kernel: Z(:, j)
-  int d_mc_slots;     // drop kernel: M(:, j)
-  int d_zc_slots;     // drop kernel: Z(:, j)
   int d_mt_slots;     // drop kernel: M(j, :)
   int d_r_slots;      // drop kernel: R(j, :)
   int64_t max_iterations;
@@ -117,14 +117,16 @@ struct FusedArgs {
 // ---------------------------------------------------------------------------
 // Drop kernel: per column j, S = 0.5 (U(:, j) + U(j, :)^T) with U = M + alpha Z.
 //
-// Four small hashes in shared memory hold M(:, j) and Z(:, j) (the column's
-// slots), M(j, :) (row j of M, from M^T) and R(j, :).  Row j of R is formed
+// M(:, j) and Z(:, j) are read from the column's sorted slots (binary
+// searches); two small hashes in shared memory hold M(j, :) (row j of M, from
+// M^T) and R(j, :).  Row j of R is formed
 // here: for the entries k of row j of A in ascending order, every entry
 // M(k, i) of row k of M adds A(j, k) M(k, i) to R(j, i) -- for each i the
 // terms arrive in ascending k, exactly the sum the residual kernel forms for
-// R(j, i) in column i.  The candidate rows i of S(:, j) (the keys of the four
-// hashes, and j) are marked in a window bitmap and read back in ascending
-// order; each one's U(i, j), U(j, i) and S(i, j) come from hash lookups, with
+// R(j, i) in column i.  The candidate rows i of S(:, j) (the rows of M(:, j)
+// and Z(:, j), the keys of the two hashes, and j) are marked in a window
+// bitmap and read back in ascending order; each one's U(i, j), U(j, i) and
+// S(i, j) come from those lookups, with
 // the union's and the symmetrisation's arithmetic (UnionPadded,
 // SymmetrizeDropKernel).  Exact zeros of U are not pruned here: an entry that
 // is zero on both sides gives S(i, j) = 0, which the drop rule removes, and a
@@ -163,12 +165,27 @@ __device__ __forceinline__ int FindSlot(const int32_t* keys, int bits, int32_t k
   return -1;
 }
 
+// First position in the sorted keys[0, n) (global memory) whose key is >= key.
+__device__ __forceinline__ int LowerBoundGlobal(const int32_t* keys, int n, int32_t key) {
+  int lo = 0;
+  int hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (keys[mid] < key) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
 template <class T>
-__host__ __device__ size_t DropWarpBytes(int mc, int zc, int mt, int r) {
-  constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
-  return Round16(static_cast<size_t>(kWindowWords) * 4) + Round16(static_cast<size_t>(kSummary) * 4) +
+__host__ __device__ size_t DropWarpBytes(int mt, int r) {
+  constexpr int kSummary = (kDropWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
+  return Round16(static_cast<size_t>(kDropWindowWords) * 4) + Round16(static_cast<size_t>(kSummary) * 4) +
          Round16(static_cast<size_t>(kDropRowsCap) * 2) +
-         Round16(static_cast<size_t>(mc + zc + mt + r) * 4) + Round16(static_cast<size_t>(mc + zc + mt + r) * sizeof(T)) +
+         Round16(static_cast<size_t>(mt + r) * 4) + Round16(static_cast<size_t>(mt + r) * sizeof(T)) +
          Round16(kDropCap * sizeof(double)) + Round16(kDropCap * sizeof(int32_t)) + Round16(kDropCap) +
          Round16(4 * kWarp * sizeof(int32_t));
 }
@@ -176,18 +193,17 @@ __host__ __device__ size_t DropWarpBytes(int mc, int zc, int mt, int r) {
 template <class T>
 __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<T> a) {
   extern __shared__ __align__(16) unsigned char fused_drop_smem[];
-  constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
+  constexpr int kSummary = (kDropWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
   const int lane = threadIdx.x & 31;
-  const int table = a.d_mc_slots + a.d_zc_slots + a.d_mt_slots + a.d_r_slots;
-  unsigned char* base =
-      fused_drop_smem + (threadIdx.x >> 5) * DropWarpBytes<T>(a.d_mc_slots, a.d_zc_slots, a.d_mt_slots, a.d_r_slots);
+  const int table = a.d_mt_slots + a.d_r_slots;
+  unsigned char* base = fused_drop_smem + (threadIdx.x >> 5) * DropWarpBytes<T>(a.d_mt_slots, a.d_r_slots);
   uint32_t* bm = reinterpret_cast<uint32_t*>(base);
-  base += Round16(static_cast<size_t>(kWindowWords) * 4);
+  base += Round16(static_cast<size_t>(kDropWindowWords) * 4);
   uint32_t* summary = reinterpret_cast<uint32_t*>(base);
   base += Round16(static_cast<size_t>(kSummary) * 4);
   uint16_t* rows = reinterpret_cast<uint16_t*>(base);
   base += Round16(static_cast<size_t>(kDropRowsCap) * 2);
-  int32_t* keys = reinterpret_cast<int32_t*>(base);  // the four tables, one after another
+  int32_t* keys = reinterpret_cast<int32_t*>(base);  // the two tables, one after another
   base += Round16(static_cast<size_t>(table) * 4);
   T* vals = reinterpret_cast<T*>(base);
   base += Round16(static_cast<size_t>(table) * sizeof(T));
@@ -201,20 +217,14 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
   s.xk = reinterpret_cast<int32_t*>(base);  // staging of the top-k selection
   s.yk = s.xk;
   s.mx_prefix = nullptr;
-  int32_t* k_mc = keys;
-  int32_t* k_zc = k_mc + a.d_mc_slots;
-  int32_t* k_mt = k_zc + a.d_zc_slots;
+  int32_t* k_mt = keys;
   int32_t* k_r = k_mt + a.d_mt_slots;
-  T* v_mc = vals;
-  T* v_zc = v_mc + a.d_mc_slots;
-  T* v_mt = v_zc + a.d_zc_slots;
+  T* v_mt = vals;
   T* v_r = v_mt + a.d_mt_slots;
-  const int b_mc = Log2(a.d_mc_slots);
-  const int b_zc = Log2(a.d_zc_slots);
   const int b_mt = Log2(a.d_mt_slots);
   const int b_r = Log2(a.d_r_slots);
   const int r_limit = a.d_r_slots / 2;  // distinct keys of R(j, :) the table takes
-  ClearWords(bm, kWindowWords, lane);
+  ClearWords(bm, kDropWindowWords, lane);
   ClearWords(summary, kSummary, lane);
   FusedState* state = a.state;
   const int64_t parity = state->parity;
@@ -244,17 +254,14 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
     int32_t lo = static_cast<int32_t>(j);
     int32_t hi = static_cast<int32_t>(j);
     bool fresh;
-    for (int e = lane; e < nm; e += kWarp) {
-      const int at = FindOrInsert(k_mc, b_mc, mr[e], &fresh);
-      v_mc[at] = mv[e];
-      lo = min(lo, mr[e]);
-      hi = max(hi, mr[e]);
+    // M(:, j) and Z(:, j) are sorted: their ends bound the window, and lookups are binary searches
+    if (nm > 0) {
+      lo = min(lo, mr[0]);
+      hi = max(hi, mr[nm - 1]);
     }
-    for (int e = lane; e < nz; e += kWarp) {
-      const int at = FindOrInsert(k_zc, b_zc, zr[e], &fresh);
-      v_zc[at] = zv[e];
-      lo = min(lo, zr[e]);
-      hi = max(hi, zr[e]);
+    if (nz > 0) {
+      lo = min(lo, zr[0]);
+      hi = max(hi, zr[nz - 1]);
     }
     for (int e = lane; e < nmt; e += kWarp) {
       const int at = FindOrInsert(k_mt, b_mt, mtc[e], &fresh);
@@ -305,13 +312,19 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
     }
     lo = __reduce_min_sync(0xffffffffu, lo);
     hi = __reduce_max_sync(0xffffffffu, hi);
-    // S(:, j) in row order, one window of kWindowRows rows at a time
+    // S(:, j) in row order, one window of kDropWindowRows rows at a time
     int count = 0;
     bool too_long = false;
-    for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
-      const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
+    for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kDropWindowRows) {
+      const int32_t seg_hi = hi - seg_lo < kDropWindowRows ? hi : seg_lo + (kDropWindowRows - 1);
       const int words = (seg_hi - seg_lo) / 32 + 1;
       if (lane == 0 && j >= seg_lo && j <= seg_hi) MarkRow(bm, summary, static_cast<int>(j - seg_lo));
+      for (int e = lane; e < nm; e += kWarp) {
+        if (mr[e] >= seg_lo && mr[e] <= seg_hi) MarkRow(bm, summary, mr[e] - seg_lo);
+      }
+      for (int e = lane; e < nz; e += kWarp) {
+        if (zr[e] >= seg_lo && zr[e] <= seg_hi) MarkRow(bm, summary, zr[e] - seg_lo);
+      }
       for (int t = lane; t < table; t += kWarp) {
         const int32_t key = keys[t];
         if (key != kEmpty && key >= seg_lo && key <= seg_hi) MarkRow(bm, summary, key - seg_lo);
@@ -330,16 +343,18 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
         if (r < found) {
           i = seg_lo + static_cast<int32_t>(rows[r]);
           // U(i, j) = M(i, j) (+) alpha Z(i, j)
-          const int pm = FindSlot(k_mc, b_mc, i);
-          const int pz = FindSlot(k_zc, b_zc, i);
+          int pm = LowerBoundGlobal(mr, nm, i);
+          int pz = LowerBoundGlobal(zr, nz, i);
+          pm = pm < nm && mr[pm] == i ? pm : -1;
+          pz = pz < nz && zr[pz] == i ? pz : -1;
           const bool own = pm >= 0 || pz >= 0;
           T u_own = T(0);
           if (pm >= 0 && pz >= 0) {
-            u_own = Add(v_mc[pm], Mul(alpha, v_zc[pz]));
+            u_own = Add(mv[pm], Mul(alpha, zv[pz]));
           } else if (pm >= 0) {
-            u_own = Add(v_mc[pm], T(0));
+            u_own = Add(mv[pm], T(0));
           } else if (pz >= 0) {
-            u_own = Add(T(0), Mul(alpha, v_zc[pz]));
+            u_own = Add(T(0), Mul(alpha, zv[pz]));
           }
           // U(j, i) = M(j, i) (+) alpha Z(j, i), Z(j, i) = pr_j R(j, i) unless R(j, i) is an exact zero
           const int pmt = FindSlot(k_mt, b_mt, i);
@@ -385,8 +400,8 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
     }
     if (too_long) {
       // leave the bitmap clear for the next column before skipping this one
-      for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
-        const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
+      for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kDropWindowRows) {
+        const int32_t seg_hi = hi - seg_lo < kDropWindowRows ? hi : seg_lo + (kDropWindowRows - 1);
         ClearWords(bm, (seg_hi - seg_lo) / 32 + 1, lane);
         ClearWords(summary, SummaryWords((seg_hi - seg_lo) / 32 + 1), lane);
       }
@@ -1018,8 +1033,6 @@ class FusedMr final : public FusedMrBase {
     a.ell = p.ell_width;
     a.m_hash_slots = NextPow2Int(std::max(4 * p.topk, kWarp));
     a.z_hash_slots = NextPow2Int(std::max(2 * cap_z, kWarp));
-    a.d_mc_slots = NextPow2Int(std::max(2 * p.topk, kWarp));
-    a.d_zc_slots = NextPow2Int(std::max(2 * cap_z, kWarp));
     a.d_mt_slots = NextPow2Int(std::max(2 * cap_mt, kWarp));
     a.d_r_slots = DropRowSlots(p);
     a.max_iterations = p.max_iterations;
@@ -1056,7 +1069,7 @@ class FusedMr final : public FusedMrBase {
   static bool SameArgs(const FusedArgs<T>& x, const FusedArgs<T>& y) {
     bool same = x.n == y.n && x.topk == y.topk && x.cap_z == y.cap_z && x.cap_mt == y.cap_mt &&
                 x.ell == y.ell && x.m_hash_slots == y.m_hash_slots && x.d_r_slots == y.d_r_slots &&
-                x.d_mc_slots == y.d_mc_slots && x.d_zc_slots == y.d_zc_slots && x.d_mt_slots == y.d_mt_slots &&
+                x.d_mt_slots == y.d_mt_slots &&
                 x.z_hash_slots == y.z_hash_slots && x.max_iterations == y.max_iterations &&
                 x.tolerance == y.tolerance && x.a_cols_ell == y.a_cols_ell && x.a_rows_ell == y.a_rows_ell &&
                 x.a_rows_ell_val == y.a_rows_ell_val && x.pr == y.pr && x.m_rows == y.m_rows &&
@@ -1080,7 +1093,7 @@ class FusedMr final : public FusedMrBase {
       default: throw std::invalid_argument("fused MR: unsupported ELL width");
     }
     drop_smem_ = static_cast<size_t>(kDropWarps) *
-                 DropWarpBytes<T>(args_.d_mc_slots, args_.d_zc_slots, args_.d_mt_slots, args_.d_r_slots);
+                 DropWarpBytes<T>(args_.d_mt_slots, args_.d_r_slots);
     res_smem_ = static_cast<size_t>(kResidualWarps) * ResidualSlabBytes<T>(args_.m_hash_slots, args_.z_hash_slots);
     SPAI_CUDA(cudaFuncSetAttribute(FusedDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(drop_smem_)));
