@@ -165,27 +165,17 @@ __device__ __forceinline__ int FindSlot(const int32_t* keys, int bits, int32_t k
   return -1;
 }
 
-// First position in the sorted keys[0, n) (global memory) whose key is >= key.
-__device__ __forceinline__ int LowerBoundGlobal(const int32_t* keys, int n, int32_t key) {
-  int lo = 0;
-  int hi = n;
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (keys[mid] < key) {
-      lo = mid + 1;
-    } else {
-      hi = mid;
-    }
-  }
-  return lo;
-}
+// Entries of one row of M^T a lane holds while row j of R is formed (cap_mt <= 4 * kMaxTopK).
+constexpr int kMtPerLane = 4;
+static_assert(4 * kMaxTopK <= kMtPerLane * kWarp, "a row of M^T must fit the lanes' registers");
 
 template <class T>
-__host__ __device__ size_t DropWarpBytes(int mt, int r) {
+__host__ __device__ size_t DropWarpBytes(int own, int mt, int r) {
   constexpr int kSummary = (kDropWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
   return Round16(static_cast<size_t>(kDropWindowWords) * 4) + Round16(static_cast<size_t>(kSummary) * 4) +
          Round16(static_cast<size_t>(kDropRowsCap) * 2) +
          Round16(static_cast<size_t>(mt + r) * 4) + Round16(static_cast<size_t>(mt + r) * sizeof(T)) +
+         Round16(static_cast<size_t>(own) * 4) + Round16(static_cast<size_t>(own) * sizeof(T)) +
          Round16(kDropCap * sizeof(double)) + Round16(kDropCap * sizeof(int32_t)) + Round16(kDropCap) +
          Round16(4 * kWarp * sizeof(int32_t));
 }
@@ -196,7 +186,8 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
   constexpr int kSummary = (kDropWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
   const int lane = threadIdx.x & 31;
   const int table = a.d_mt_slots + a.d_r_slots;
-  unsigned char* base = fused_drop_smem + (threadIdx.x >> 5) * DropWarpBytes<T>(a.d_mt_slots, a.d_r_slots);
+  const int own = a.topk + a.cap_z;  // M(:, j) and Z(:, j), staged
+  unsigned char* base = fused_drop_smem + (threadIdx.x >> 5) * DropWarpBytes<T>(own, a.d_mt_slots, a.d_r_slots);
   uint32_t* bm = reinterpret_cast<uint32_t*>(base);
   base += Round16(static_cast<size_t>(kDropWindowWords) * 4);
   uint32_t* summary = reinterpret_cast<uint32_t*>(base);
@@ -207,6 +198,12 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
   base += Round16(static_cast<size_t>(table) * 4);
   T* vals = reinterpret_cast<T*>(base);
   base += Round16(static_cast<size_t>(table) * sizeof(T));
+  int32_t* mr = reinterpret_cast<int32_t*>(base);  // M(:, j) then Z(:, j): rows
+  int32_t* zr = mr + a.topk;
+  base += Round16(static_cast<size_t>(own) * 4);
+  T* mv = reinterpret_cast<T*>(base);  // and values
+  T* zv = mv + a.topk;
+  base += Round16(static_cast<size_t>(own) * sizeof(T));
   DropSlab s;
   s.vals = reinterpret_cast<double*>(base);
   base += Round16(kDropCap * sizeof(double));
@@ -243,12 +240,16 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
       continue;
     }
     ClearTable(keys, table, lane);
+    // M(:, j) and Z(:, j) into shared memory (sorted by row), then M(j, :) into its hash
+    for (int e = lane; e < nm; e += kWarp) {
+      mr[e] = a.m_rows[j * a.topk + e];
+      mv[e] = a.m_vals[j * a.topk + e];
+    }
+    for (int e = lane; e < nz; e += kWarp) {
+      zr[e] = a.z_rows[j * a.cap_z + e];
+      zv[e] = a.z_vals[j * a.cap_z + e];
+    }
     __syncwarp();
-    // M(:, j), Z(:, j), M(j, :)
-    const int32_t* mr = a.m_rows + j * a.topk;
-    const T* mv = a.m_vals + j * a.topk;
-    const int32_t* zr = a.z_rows + j * a.cap_z;
-    const T* zv = a.z_vals + j * a.cap_z;
     const int32_t* mtc = a.mt_cols[parity] + j * a.cap_mt;
     const T* mtv = a.mt_vals[parity] + j * a.cap_mt;
     int32_t lo = static_cast<int32_t>(j);
@@ -269,44 +270,81 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
       lo = min(lo, mtc[e]);
       hi = max(hi, mtc[e]);
     }
-    // R(j, :) = e_j^T - A(j, :) M: terms in ascending k for every column i
-    int r_keys = 0;
-    bool r_full = false;
-    for (int u = 0; u < a.ell; ++u) {
-      const int32_t k = a.a_rows_ell[j * a.ell + u];
-      if (k < 0) continue;  // warp-uniform
-      const T a_jk = a.a_rows_ell_val[j * a.ell + u];
-      const int nk = a.mt_cnt[parity][k];
-      if (nk > a.cap_mt) {
-        r_full = true;
-        break;
+    // R(j, :) = e_j^T - A(j, :) M: terms in ascending k for every column i.  Lane u holds
+    // entry u of row j of A and the length of row k_u of M^T; the rows of M^T are loaded
+    // one step ahead of the step that adds them, so their loads overlap.
+    int32_t k_lane = -1;
+    T a_lane = T(0);
+    int nk_lane = 0;
+    if (lane < a.ell) {
+      k_lane = a.a_rows_ell[j * a.ell + lane];
+      if (k_lane >= 0) {
+        a_lane = a.a_rows_ell_val[j * a.ell + lane];
+        nk_lane = a.mt_cnt[parity][k_lane];
       }
+    }
+    int r_keys = 0;
+    bool r_full = __any_sync(0xffffffffu, nk_lane > a.cap_mt);
+    int32_t cur_i[kMtPerLane];
+    T cur_v[kMtPerLane];
+    int32_t next_i[kMtPerLane];
+    T next_v[kMtPerLane];
+    auto load_row = [&](int u, int32_t (&ii)[kMtPerLane], T (&vv)[kMtPerLane]) {
+      const int32_t k = __shfl_sync(0xffffffffu, k_lane, u);
+      const int nk = r_full ? 0 : __shfl_sync(0xffffffffu, nk_lane, u);
       const int32_t* kc = a.mt_cols[parity] + static_cast<int64_t>(k) * a.cap_mt;
       const T* kv = a.mt_vals[parity] + static_cast<int64_t>(k) * a.cap_mt;
-      for (int e0 = 0; e0 < nk; e0 += kWarp) {
-        const int e = e0 + lane;
-        bool is_new = false;
-        bool lost = false;
-        if (e < nk) {
-          const int32_t i = kc[e];
-          const T prod = Mul(a_jk, kv[e]);
-          const int at = FindOrInsert(k_r, b_r, i, &is_new);
-          if (at < 0) {
-            lost = true;
-          } else {
-            // a column i appears once in row k of M: no two lanes share a slot here
-            v_r[at] = is_new ? prod : Add(v_r[at], prod);
-            lo = min(lo, i);
-            hi = max(hi, i);
+#pragma unroll
+      for (int q = 0; q < kMtPerLane; ++q) {
+        const int e = q * kWarp + lane;
+        ii[q] = -1;
+        vv[q] = T(0);
+        if (k >= 0 && e < nk) {
+          ii[q] = kc[e];
+          vv[q] = kv[e];
+        }
+      }
+    };
+    load_row(0, cur_i, cur_v);
+    for (int u = 0; u < a.ell && !r_full; ++u) {
+      const int32_t k = __shfl_sync(0xffffffffu, k_lane, u);
+      const int nk = __shfl_sync(0xffffffffu, nk_lane, u);
+      const T a_jk = __shfl_sync(0xffffffffu, a_lane, u);
+      if (u + 1 < a.ell) load_row(u + 1, next_i, next_v);
+      if (k >= 0) {  // warp-uniform
+#pragma unroll
+        for (int q = 0; q < kMtPerLane; ++q) {
+          if (q * kWarp < nk) {  // warp-uniform
+            const int e = q * kWarp + lane;
+            bool is_new = false;
+            bool lost = false;
+            if (e < nk) {
+              const int32_t i = cur_i[q];
+              const T prod = Mul(a_jk, cur_v[q]);
+              const int at = FindOrInsert(k_r, b_r, i, &is_new);
+              if (at < 0) {
+                lost = true;
+              } else {
+                // a column i appears once in row k of M: no two lanes share a slot here
+                v_r[at] = is_new ? prod : Add(v_r[at], prod);
+                lo = min(lo, i);
+                hi = max(hi, i);
+              }
+            }
+            r_keys += __popc(__ballot_sync(0xffffffffu, is_new));
+            if (__any_sync(0xffffffffu, lost)) r_full = true;
           }
         }
-        r_keys += __popc(__ballot_sync(0xffffffffu, is_new));
-        if (__any_sync(0xffffffffu, lost)) r_full = true;
+        __syncwarp();
+        if (r_keys > r_limit) r_full = true;
       }
-      __syncwarp();
-      if (r_full || r_keys > r_limit) break;
+#pragma unroll
+      for (int q = 0; q < kMtPerLane; ++q) {
+        cur_i[q] = next_i[q];
+        cur_v[q] = next_v[q];
+      }
     }
-    if (r_full || r_keys > r_limit) {
+    if (r_full) {
       overflow |= kOverflowRow;
       continue;
     }
@@ -343,8 +381,8 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
         if (r < found) {
           i = seg_lo + static_cast<int32_t>(rows[r]);
           // U(i, j) = M(i, j) (+) alpha Z(i, j)
-          int pm = LowerBoundGlobal(mr, nm, i);
-          int pz = LowerBoundGlobal(zr, nz, i);
+          int pm = LowerBoundShared(mr, nm, i);
+          int pz = LowerBoundShared(zr, nz, i);
           pm = pm < nm && mr[pm] == i ? pm : -1;
           pz = pz < nz && zr[pz] == i ? pz : -1;
           const bool own = pm >= 0 || pz >= 0;
@@ -634,8 +672,7 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
     }
     lo = __reduce_min_sync(0xffffffffu, lo);
     hi = __reduce_max_sync(0xffffffffu, hi);
-    double tt = 0.0;
-    double bt = 0.0;
+    double proj = 0.0;  // tt on lane 0, bt on lane 1
     for (int32_t seg_lo = lo; seg_lo <= hi; seg_lo += kWindowRows) {
       const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
       const int words2 = (seg_hi - seg_lo) / 32 + 1;
@@ -679,14 +716,14 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
           stage1[lane] = BucketFind(zkeys, zvals, zbits, z_displaced, i, zi) ? Mul(static_cast<double>(zi), td) : 0.0;
         }
         __syncwarp();
+        // lane 0 extends tt and lane 1 bt, side by side in one instruction stream
         const int span = min(kWarp, count2 - r0);
-        if (lane == 0) tt = SumStaged(tt, stage0, span);
-        if (lane == 1) bt = SumStaged(bt, stage1, span);
+        if (lane < 2) proj = SumStaged(proj, lane == 0 ? stage0 : stage1, span);
         __syncwarp();
       }
     }
-    if (lane == 0) a.tt[j] = tt;
-    if (lane == 1) a.bt[j] = bt;
+    if (lane == 0) a.tt[j] = proj;
+    if (lane == 1) a.bt[j] = proj;
     __syncwarp();
   }
   overflow = __reduce_or_sync(0xffffffffu, overflow);
@@ -1093,7 +1130,7 @@ class FusedMr final : public FusedMrBase {
       default: throw std::invalid_argument("fused MR: unsupported ELL width");
     }
     drop_smem_ = static_cast<size_t>(kDropWarps) *
-                 DropWarpBytes<T>(args_.d_mt_slots, args_.d_r_slots);
+                 DropWarpBytes<T>(args_.topk + args_.cap_z, args_.d_mt_slots, args_.d_r_slots);
     res_smem_ = static_cast<size_t>(kResidualWarps) * ResidualSlabBytes<T>(args_.m_hash_slots, args_.z_hash_slots);
     SPAI_CUDA(cudaFuncSetAttribute(FusedDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(drop_smem_)));
