@@ -490,6 +490,10 @@ void RunFilter(Ctx& ctx, DevCsc<T>& x, const Pred& pred) {
   DevCsc<T> out;
   out.Shape(x.rows, cols, ctx.stream);
   const int64_t nnz = ScanCounts(ctx, ctx.counts.data(), cols, out.ptr.data());
+  // algorithmic bytes: x read, the survivors written
+  const double entry = static_cast<double>(sizeof(int32_t) + sizeof(T));
+  prof::AddBytes("filter", entry * static_cast<double>(x.nnz + (nnz == x.nnz ? 0 : nnz)) +
+                               16.0 * static_cast<double>(cols + 1));
   if (nnz == x.nnz) {
     return;  // nothing removed: keep x as it is
   }
@@ -1383,9 +1387,15 @@ void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T
   const int64_t cap = UnionWarpCap();
   const bool half_sum = mode == UnionMode::kHalfSum;
   prof::Scope scope(ctx.stream, "union", 0.0);
+  // algorithmic bytes: both operands read, the union written
+  auto account = [&](const DevCsc<T>& u) {
+    const double entry = static_cast<double>(sizeof(int32_t) + sizeof(T));
+    prof::AddBytes("union", entry * static_cast<double>(y.nnz + x.nnz + u.nnz) + 24.0 * static_cast<double>(cols + 1));
+  };
   {
     DevCsc<T> single;
     if (UnionPadded(ctx, y, scale_y, ys, x, xs, half_sum, !half_sum, single)) {
+      account(single);
       out.Swap(single);
       return;
     }
@@ -1409,6 +1419,7 @@ void Union(Ctx& ctx, const DevCsc<T>& y, bool scale_y, double ys, const DevCsc<T
     ctx.Sync();
     if (ctx.host_flags[0] != 0) DropZeros(ctx, result);
   }
+  account(result);
   out.Swap(result);
 }
 
@@ -1560,6 +1571,9 @@ void Transpose(Ctx& ctx, const DevCsc<T>& x, DevCsc<T>& t) {
     SPAI_LAUNCH_CHECK();
     SortSegments<T>(ctx, result.ptr.data(), x.rows, result.idx.data(), result.val.data(), longest_row);
   }
+  // algorithmic bytes: x read, its transpose written
+  prof::AddBytes("transpose", static_cast<double>(sizeof(int32_t) + sizeof(T)) * 2.0 * static_cast<double>(x.nnz) +
+                                  8.0 * static_cast<double>(x.cols + 1 + x.rows + 1));
   t.Swap(result);
 }
 

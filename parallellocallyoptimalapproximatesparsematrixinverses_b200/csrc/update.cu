@@ -440,6 +440,12 @@ bool SymmetrizeAndDrop(Ctx& ctx, DevCsc<T>& m, bool symmetric, int64_t topk) {
   out.ReserveNnz(nnz, ctx.stream);
   CompactPadded(ctx, m.ptr.data(), symmetric ? mt.ptr.data() : nullptr, cols, out.ptr.data(), tmp_idx, tmp_val,
                 out.idx.data(), out.val.data());
+  // algorithmic bytes: M and M^T read (and M^T formed: M read, M^T written), the result written
+  const double entry = static_cast<double>(sizeof(int32_t) + sizeof(T));
+  const double ptrs = 8.0 * static_cast<double>(cols + 1);
+  const double mt_nnz = symmetric ? static_cast<double>(mt.nnz) : 0.0;
+  prof::AddBytes("drop_update", entry * (static_cast<double>(m.nnz) + 3.0 * mt_nnz + static_cast<double>(nnz)) +
+                                    ptrs * (symmetric ? 4.0 : 2.0));
   m.Swap(out);
   return true;
 }

@@ -43,3 +43,27 @@ def test_parallel_threads_rejects_like_the_reference():
         parallel_threads)
     with pytest.raises(ValueError):
         parallel_threads(0, 1)
+
+
+DRIVERS = ROOT / "oracle" / "_ref" / "drivers" / "scripts"
+DRIVER_PROBE = r"""
+import common, methods_convergence
+import scripts.utils.backward_error as be
+import parallellocallyoptimalapproximatesparsematrixinverses_b200 as pkg
+assert common.methods.global_spai is pkg.global_spai and common.methods.inner_outer is pkg.inner_outer
+assert be.pcg is pkg.pcg and be.matvec is pkg.matvec
+assert len(common.SAMPLE_DATASETS) == 10
+print("ok")
+"""
+
+
+def test_compiled_reference_drivers_bind_to_this_library():
+    """The reference's drivers, compiled unchanged by oracle/build_drivers.sh,
+    import and reach this library through the shims (no GPU call is made)."""
+    if not list(DRIVERS.glob("methods_convergence*.so")):
+        pytest.skip("oracle/_ref/drivers is built by build() where the reference tree is present")
+    stubs = ROOT / "tests" / "driver_stubs"
+    env = dict(os.environ, PYTHONPATH=os.pathsep.join([str(stubs), str(COMPAT), str(DRIVERS), str(ROOT)]))
+    out = subprocess.run([sys.executable, "-c", DRIVER_PROBE], env=env, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.strip() == "ok"
