@@ -496,8 +496,7 @@ __host__ __device__ size_t ResidualSlabBytes(int m_slots, int z_slots) {
   return Round16(static_cast<size_t>(kWindowWords) * 4) + Round16(static_cast<size_t>(SummaryWords(kWindowWords)) * 4) +
          Round16(static_cast<size_t>(kRowsCap) * 2) + Round16(static_cast<size_t>(m_slots) * 4) +
          Round16(static_cast<size_t>(m_slots) * sizeof(T)) + Round16(static_cast<size_t>(z_slots) * 4) +
-         Round16(static_cast<size_t>(z_slots) * sizeof(T)) + Round16(static_cast<size_t>(kDropRowsCap) * 4) +
-         2 * Round16(kWarp * sizeof(double));
+         Round16(static_cast<size_t>(z_slots) * sizeof(T)) + 2 * Round16(kWarp * sizeof(double));
 }
 
 // Sequential sum of `count` staged values onto s (one lane).
@@ -536,8 +535,6 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
   base += Round16(static_cast<size_t>(a.z_hash_slots) * 4);
   T* zvals = reinterpret_cast<T*>(base);
   base += Round16(static_cast<size_t>(a.z_hash_slots) * sizeof(T));
-  int32_t* zlist = reinterpret_cast<int32_t*>(base);
-  base += Round16(static_cast<size_t>(kDropRowsCap) * 4);
   double* stage0 = reinterpret_cast<double*>(base);
   double* stage1 = stage0 + kWarp;
   const int mbits = Log2(a.m_hash_slots) - 1;  // buckets of two slots
@@ -637,7 +634,6 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
           const T z = Mul(a.pr[i], v);
           zr_out[o] = i;
           zv_out[o] = z;
-          zlist[o] = i;
           z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
         }
         kept += __popc(mask);
@@ -656,7 +652,7 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
     lo = INT32_MAX;
     hi = -1;
     for (int e = lane; e < kept; e += kWarp) {
-      const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zlist[e]) * kEll);
+      const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zr_out[e]) * kEll);
 #pragma unroll
       for (int u = 0; u < kEll / 4; ++u) {
         const int4 r4 = src[u];
@@ -677,7 +673,7 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
       const int32_t seg_hi = hi - seg_lo < kWindowRows ? hi : seg_lo + (kWindowRows - 1);
       const int words2 = (seg_hi - seg_lo) / 32 + 1;
       for (int e = lane; e < kept; e += kWarp) {
-        const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zlist[e]) * kEll);
+        const int4* src = reinterpret_cast<const int4*>(a.a_cols_ell + static_cast<int64_t>(zr_out[e]) * kEll);
 #pragma unroll
         for (int u = 0; u < kEll / 4; ++u) {
           const int4 r4 = src[u];
