@@ -201,6 +201,31 @@ int64_t spai_pcg_adjoint(int64_t n, const double* a_values, const int64_t* a_ind
                          const double* grad_x, PcgParams params, double* grad_b, double* grad_a, double* history,
                          int64_t* status, char* error, int64_t error_capacity);
 
+/* ---- The same, on arrays already in device memory ----
+ * Device forms of spai_pcg, spai_pcg_adjoint and spai_residual_adjoint for
+ * callers whose data live on the GPU (torch CUDA tensors): every array
+ * argument is device (or managed) memory of the call's device, with the
+ * layouts, checks, arithmetic and results of the host forms (so the bits are
+ * the same); the offsets and indices are validated on the device.  history,
+ * status and loss stay host pointers.  Outputs must not alias inputs.  The
+ * calls run on the library's own stream and return after it has finished:
+ * the caller finishes the work that produces the inputs first (e.g. synchronises
+ * its stream).  Each names its nnz explicitly: a_nnz = a_offsets[n]. */
+int64_t spai_pcg_device(int64_t n, int64_t a_nnz, const double* a_values, const int64_t* a_indices,
+                        const int64_t* a_offsets, int64_t m_nnz, const double* m_values, const int64_t* m_indices,
+                        const int64_t* m_offsets, const double* b, PcgParams params, double* history, int64_t* status,
+                        double* x, char* error, int64_t error_capacity);
+int64_t spai_pcg_adjoint_device(int64_t n, int64_t a_nnz, const double* a_values, const int64_t* a_indices,
+                                const int64_t* a_offsets, int64_t m_nnz, const double* m_values,
+                                const int64_t* m_indices, const int64_t* m_offsets, const double* x,
+                                const double* grad_x, PcgParams params, double* grad_b, double* grad_a,
+                                double* history, int64_t* status, char* error, int64_t error_capacity);
+int64_t spai_residual_adjoint_device(int64_t n, int64_t a_nnz, const int64_t* a_col_offsets,
+                                     const int64_t* a_row_indices, const double* a_values, int64_t m_nnz,
+                                     const int64_t* m_col_offsets, const int64_t* m_row_indices,
+                                     const double* m_values, int64_t device, double* loss, double* grad_m,
+                                     double* grad_a, char* error, int64_t error_capacity);
+
 /* ---- Matrix Market files, read and written natively (host) ---- */
 
 /* Reads a Matrix Market matrix file (coordinate or array; real, integer or

@@ -82,6 +82,7 @@ EXPORTED_SYMBOLS = (
     "spai_session_result", "spai_session_set_rhs", "spai_session_pcg", "spai_session_destroy",
     "spai_kernel_launches", "spai_session_stream", "spai_profile_enable", "spai_profile_reset",
     "spai_profile_read", "spai_pcg_device_noalloc", "spai_residual_adjoint", "spai_pcg_adjoint",
+    "spai_pcg_device", "spai_pcg_adjoint_device", "spai_residual_adjoint_device",
     "spai_mr_batched", "spai_mtx_read", "spai_mtx_write", "spai_free_int64_array", "spai_free_double_array",
     "spai_session_create_device", "spai_session_result_device", "spai_inject_allocation_failure",
     "spai_set_fused_mr", "spai_solve_2x2_device",
@@ -163,6 +164,16 @@ def _declare(lib) -> None:
                                     ctypes.POINTER(SpaiExtParams), ctypes.POINTER(Result), ctypes.c_char_p, _i64]
     lib.spai_residual_adjoint.restype = _i64
     lib.spai_residual_adjoint.argtypes = [MatrixData, MatrixData, _i64, _pf64, _pf64, _pf64, ctypes.c_char_p, _i64]
+    _vp = ctypes.c_void_p
+    lib.spai_pcg_device.restype = _i64
+    lib.spai_pcg_device.argtypes = [_i64, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, PcgParams, _pf64,
+                                    ctypes.POINTER(_i64), _vp, ctypes.c_char_p, _i64]
+    lib.spai_pcg_adjoint_device.restype = _i64
+    lib.spai_pcg_adjoint_device.argtypes = [_i64, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _vp, _vp, PcgParams, _vp,
+                                            _vp, _pf64, ctypes.POINTER(_i64), ctypes.c_char_p, _i64]
+    lib.spai_residual_adjoint_device.restype = _i64
+    lib.spai_residual_adjoint_device.argtypes = [_i64, _i64, _vp, _vp, _vp, _i64, _vp, _vp, _vp, _i64, _pf64, _vp,
+                                                 _vp, ctypes.c_char_p, _i64]
     lib.spai_pcg_adjoint.restype = _i64
     lib.spai_pcg_adjoint.argtypes = [_i64, _pf64, _pi64, _pi64, _pf64, _pi64, _pi64, _pf64, _pf64, PcgParams, _pf64,
                                      _pf64, _pf64, _pi64, ctypes.c_char_p, _i64]

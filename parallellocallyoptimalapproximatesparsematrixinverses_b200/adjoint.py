@@ -14,9 +14,13 @@ compute:
   implicit-function adjoint, exact for the solution map A^-1 b).
 
 `residual_objective` and `pcg_solve` wrap both for torch autograd over the
-stored values of fixed sparsity patterns.  Tensors may live on any device:
-values cross the C ABI through host memory, and gradients come back on the
-device and in the dtype (float64) of the inputs.
+stored values of fixed sparsity patterns.  CUDA tensors stay on their device:
+their pointers go to the device forms of the entry points
+(`spai_residual_adjoint_device`, `spai_pcg_device`,
+`spai_pcg_adjoint_device`), which give the same bits as the host forms, and
+only the patterns (when given as numpy arrays), the loss and the solve's
+history cross to or from the host.  CPU tensors go through the host forms.
+Gradients come back on the device and in the dtype (float64) of the inputs.
 """
 from __future__ import annotations
 
@@ -123,6 +127,45 @@ def _host(t):
     return t.detach().to("cpu", torch.float64).numpy()
 
 
+def _on_device(values, device):
+    """A contiguous float64 / int64 copy-or-view of `values` on `device`."""
+    if isinstance(values, torch.Tensor):
+        t = values.detach()
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(values))
+    dtype = torch.float64 if t.is_floating_point() else torch.int64
+    return t.to(device=device, dtype=dtype).contiguous()
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else None
+
+
+def _ready(device):
+    # the library runs on its own stream: the inputs' producers must be done
+    torch.cuda.current_stream(device).synchronize()
+
+
+def _residual_adjoint_device(n, a_pattern, a_values, m_pattern, m_values, want_m, want_a):
+    dev = a_values.device
+    if m_values.device != dev:
+        raise ValueError("A's and M's values must live on the same device")
+    a_ptr, a_idx = _on_device(a_pattern[0], dev), _on_device(a_pattern[1], dev)
+    m_ptr, m_idx = _on_device(m_pattern[0], dev), _on_device(m_pattern[1], dev)
+    av, mv = _on_device(a_values, dev), _on_device(m_values, dev)
+    grad_m = torch.empty(mv.numel(), dtype=torch.float64, device=dev) if want_m else None
+    grad_a = torch.empty(av.numel(), dtype=torch.float64, device=dev) if want_a else None
+    loss = ctypes.c_double(0.0)
+    err = _lib.error_buffer()
+    _ready(dev)
+    rc = _lib.load().spai_residual_adjoint_device(n, av.numel(), _ptr(a_ptr), _ptr(a_idx), _ptr(av), mv.numel(),
+                                                  _ptr(m_ptr), _ptr(m_idx), _ptr(mv), dev.index, ctypes.byref(loss),
+                                                  _ptr(grad_m), _ptr(grad_a), err, len(err))
+    if rc != 0:
+        raise RuntimeError(err.value.decode("utf-8", "replace"))
+    return float(loss.value), grad_m, grad_a
+
+
 class ResidualObjective(torch.autograd.Function):
     """f = ||I - A M||_F^2 over the stored values of A and M (fixed canonical
     CSC patterns, given as (indptr, indices) numpy arrays)."""
@@ -130,6 +173,10 @@ class ResidualObjective(torch.autograd.Function):
     @staticmethod
     def forward(ctx, a_values, m_values, a_pattern, m_pattern, n, device):
         want_m, want_a = ctx.needs_input_grad[1], ctx.needs_input_grad[0]
+        if a_values.is_cuda:
+            loss, ctx.grad_m, ctx.grad_a = _residual_adjoint_device(n, a_pattern, a_values, m_pattern, m_values,
+                                                                    want_m, want_a)
+            return torch.tensor(loss, dtype=torch.float64, device=a_values.device)
         loss, gm, ga = _residual_adjoint_arrays(n, a_pattern[0], a_pattern[1], _host(a_values), m_pattern[0],
                                                 m_pattern[1], _host(m_values), want_m, want_a, device)
         ctx.grad_m = None if gm is None else torch.from_numpy(gm).to(m_values.device)
@@ -161,6 +208,8 @@ class PcgSolve(torch.autograd.Function):
     def forward(ctx, a_values, b, a_pattern, m_csr, options):
         a_indices, a_offsets = a_pattern
         m_values, m_indices, m_offsets = m_csr
+        if a_values.is_cuda:
+            return PcgSolve._forward_device(ctx, a_values, b, a_pattern, m_csr, options)
         av = _host(a_values)
         history, status, x = pcg(av, a_indices, a_offsets, m_values, m_indices, m_offsets, _host(b),
                                  options["max_iterations"], 1, options["tolerance"],
@@ -172,7 +221,61 @@ class PcgSolve(torch.autograd.Function):
         return torch.from_numpy(x).to(b.device)
 
     @staticmethod
+    def _params(options, device):
+        return _lib.PcgParams(int(options["max_iterations"]), float(options["tolerance"]),
+                              int(options.get("refresh_period", 0)), M_PRECISIONS[options.get("m_precision", "fp64")],
+                              int(device), 1 if options.get("symmetric_part", False) else 0)
+
+    @staticmethod
+    def _forward_device(ctx, a_values, b, a_pattern, m_csr, options):
+        dev = a_values.device
+        if b.device != dev:
+            raise ValueError("A's values and b must live on the same device")
+        av, bv = _on_device(a_values, dev), _on_device(b, dev)
+        ai, ao = _on_device(a_pattern[0], dev), _on_device(a_pattern[1], dev)
+        mv, mi, mo = (_on_device(v, dev) for v in m_csr)
+        n = bv.numel()
+        if ao.numel() != n + 1 or mo.numel() != n + 1:
+            raise ValueError("b and the CSR offsets must describe the same n")
+        x = torch.empty(n, dtype=torch.float64, device=dev)
+        history = np.zeros(int(options["max_iterations"]), np.float64)
+        status = ctypes.c_int64(0)
+        err = _lib.error_buffer()
+        _ready(dev)
+        count = _lib.load().spai_pcg_device(n, av.numel(), _ptr(av), _ptr(ai), _ptr(ao), mv.numel(), _ptr(mv),
+                                            _ptr(mi), _ptr(mo), _ptr(bv), PcgSolve._params(options, dev.index),
+                                            history.ctypes.data_as(_PF64), ctypes.byref(status), _ptr(x), err,
+                                            len(err))
+        if count < 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        ctx.device_state = (av, ai, ao, mv, mi, mo, x, options)
+        ctx.history, ctx.status = history[:count].copy(), int(status.value)
+        return x
+
+    @staticmethod
+    def _backward_device(ctx, grad_x):
+        av, ai, ao, mv, mi, mo, x, options = ctx.device_state
+        dev = x.device
+        gx = _on_device(grad_x, dev)
+        n = x.numel()
+        grad_b = torch.empty(n, dtype=torch.float64, device=dev)
+        grad_a = torch.empty(av.numel(), dtype=torch.float64, device=dev)
+        history = np.zeros(int(options["max_iterations"]), np.float64)
+        status = ctypes.c_int64(0)
+        err = _lib.error_buffer()
+        _ready(dev)
+        count = _lib.load().spai_pcg_adjoint_device(n, av.numel(), _ptr(av), _ptr(ai), _ptr(ao), mv.numel(),
+                                                    _ptr(mv), _ptr(mi), _ptr(mo), _ptr(x), _ptr(gx),
+                                                    PcgSolve._params(options, dev.index), _ptr(grad_b), _ptr(grad_a),
+                                                    history.ctypes.data_as(_PF64), ctypes.byref(status), err, len(err))
+        if count < 0:
+            raise RuntimeError(err.value.decode("utf-8", "replace"))
+        return grad_a, grad_b, None, None, None
+
+    @staticmethod
     def backward(ctx, grad_x):
+        if getattr(ctx, "device_state", None) is not None:
+            return PcgSolve._backward_device(ctx, grad_x)
         av, (a_indices, a_offsets), (m_values, m_indices, m_offsets), options, x = ctx.state
         grad_b, grad_a, _, _ = pcg_adjoint(av, a_indices, a_offsets, m_values, m_indices, m_offsets, x,
                                            _host(grad_x), options["max_iterations"], options["tolerance"],

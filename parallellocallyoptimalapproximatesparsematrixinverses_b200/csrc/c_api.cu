@@ -325,6 +325,95 @@ void PcgOnDevice(Ctx& ctx, int64_t n, const DevCsc<double>& a, const double* m_v
   }
 }
 
+
+// CSR offsets in device memory: *bad |= 1 unless they start at 0, never
+// decrease and end at nnz.
+__global__ void CheckOffsetsKernel(const int64_t* __restrict__ offsets, int64_t n, int64_t nnz,
+                                   int32_t* __restrict__ bad) {
+  bool wrong = false;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+    const int64_t b = offsets[i];
+    const int64_t e = offsets[i + 1];
+    wrong |= e < b || (i == 0 && b != 0) || (i == n - 1 && e != nnz);
+  }
+  if (__any_sync(0xffffffffu, wrong) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+}
+
+// Throws unless ptr is device (or managed) memory of `device`.
+void CheckDevicePointer(const void* ptr, int64_t count, const char* name, int device) {
+  if (count <= 0) return;
+  if (ptr == nullptr) throw std::invalid_argument(std::string(name) + " must not be null");
+  cudaPointerAttributes attr{};
+  if (cudaPointerGetAttributes(&attr, ptr) != cudaSuccess) {
+    cudaGetLastError();
+    throw std::invalid_argument(std::string(name) + " is not a pointer CUDA knows");
+  }
+  if (attr.type != cudaMemoryTypeDevice && attr.type != cudaMemoryTypeManaged) {
+    throw std::invalid_argument(std::string(name) + " must point to device memory");
+  }
+  if (attr.type == cudaMemoryTypeDevice && attr.device != device) {
+    throw std::invalid_argument(std::string(name) + " lives on another device than the call's");
+  }
+}
+
+// Throws when the byte ranges [a, a + a_bytes) and [b, b + b_bytes) overlap.
+void CheckDisjoint(const void* a, size_t a_bytes, const void* b, size_t b_bytes, const char* what) {
+  const uintptr_t a0 = reinterpret_cast<uintptr_t>(a);
+  const uintptr_t b0 = reinterpret_cast<uintptr_t>(b);
+  if (a == nullptr || b == nullptr || a_bytes == 0 || b_bytes == 0) return;
+  if (a0 < b0 + b_bytes && b0 < a0 + a_bytes) throw std::invalid_argument(what);
+}
+
+// Device CSR (int64 offsets and indices, FP64 values) -> device row-compressed
+// DevCsc<T>: offsets and index range checked on the device, values converted
+// to T.  The device form of UploadCsr.
+template <class T>
+void UploadCsrDevice(Ctx& ctx, int64_t n, int64_t nnz, const double* values, const int64_t* indices,
+                     const int64_t* offsets, DevCsc<T>& out) {
+  out.Shape(n, n, ctx.stream);
+  out.ReserveNnz(nnz, ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), offsets, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, ctx.stream));
+  int32_t* bad = ctx.flags.data() + 3;
+  SPAI_CUDA(cudaMemsetAsync(bad, 0, 2 * sizeof(int32_t), ctx.stream));
+  CheckOffsetsKernel<<<GridFor(n, 256), 256, 0, ctx.stream>>>(offsets, n, nnz, bad + 1);
+  SPAI_LAUNCH_CHECK();
+  if (nnz > 0) {
+    NarrowCheckedKernel<<<GridFor(nnz, 256), 256, 0, ctx.stream>>>(indices, out.idx.data(), nnz, n, bad);
+    SPAI_LAUNCH_CHECK();
+    if constexpr (sizeof(T) == sizeof(double)) {
+      SPAI_CUDA(cudaMemcpyAsync(out.val.data(), values, sizeof(double) * nnz, cudaMemcpyDeviceToDevice, ctx.stream));
+    } else {
+      ConvertValues<double, T>(ctx, values, out.val.data(), nnz);
+    }
+  }
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 3, bad, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.Sync();
+  if (ctx.host_flags[4] != 0) throw std::invalid_argument("CSR offsets must start at 0, not decrease and end at nnz");
+  if (ctx.host_flags[3] != 0) throw std::invalid_argument("CSR column index out of range");
+}
+
+// PcgOnDevice with M as device CSR arrays.
+void PcgOnDeviceArrays(Ctx& ctx, int64_t n, const DevCsc<double>& a, int64_t m_nnz, const double* m_values,
+                       const int64_t* m_indices, const int64_t* m_offsets, const PcgParams& params, const double* rhs,
+                       double* x, PcgResult& result) {
+  PcgOptions opt;
+  opt.max_iterations = params.max_iterations;
+  opt.tolerance = params.tolerance;
+  opt.refresh_period = params.refresh_period;
+  if (params.m_precision == 1) {
+    DevCsc<float> m;
+    UploadCsrDevice(ctx, n, m_nnz, m_values, m_indices, m_offsets, m);
+    if (params.symmetric_part) SymmetricPart(ctx, m);
+    RunPcg(ctx, a, m, rhs, x, opt, result);
+  } else {
+    DevCsc<double> m;
+    UploadCsrDevice(ctx, n, m_nnz, m_values, m_indices, m_offsets, m);
+    if (params.symmetric_part) SymmetricPart(ctx, m);
+    RunPcg(ctx, a, m, rhs, x, opt, result);
+  }
+}
+
 // The adjoint entry points index their gradients by stored entry, so they
 // take canonical CSC only: offsets from 0 to nnz, rows strictly increasing
 // inside every column (what methods.pyx:82-86 hands the reference).
@@ -654,6 +743,124 @@ int64_t spai_residual_adjoint(MatrixData A, MatrixData M, int64_t device, double
     if (grad_a != nullptr) {
       SPAI_CUDA(cudaMemcpyAsync(grad_a, ga.data(), sizeof(double) * a.nnz, cudaMemcpyDeviceToHost, ctx.stream));
     }
+    ctx.Sync();
+    return 0;
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_pcg_device(int64_t n, int64_t a_nnz, const double* a_values, const int64_t* a_indices,
+                        const int64_t* a_offsets, int64_t m_nnz, const double* m_values, const int64_t* m_indices,
+                        const int64_t* m_offsets, const double* b, PcgParams params, double* history, int64_t* status,
+                        double* x, char* error, int64_t error_capacity) {
+  try {
+    spai::CheckPcgParams(n, params);
+    if (a_nnz < 0 || m_nnz < 0) throw std::invalid_argument("nnz must be non-negative");
+    const int device = spai::ResolveDevice(params.device);
+    spai::DeviceScope scope(device);
+    spai::CheckDevicePointer(a_offsets, n + 1, "A offsets", device);
+    spai::CheckDevicePointer(a_indices, a_nnz, "A indices", device);
+    spai::CheckDevicePointer(a_values, a_nnz, "A values", device);
+    spai::CheckDevicePointer(m_offsets, n + 1, "M offsets", device);
+    spai::CheckDevicePointer(m_indices, m_nnz, "M indices", device);
+    spai::CheckDevicePointer(m_values, m_nnz, "M values", device);
+    spai::CheckDevicePointer(b, n, "b", device);
+    spai::CheckDevicePointer(x, n, "x", device);
+    spai::CheckDisjoint(x, sizeof(double) * n, b, sizeof(double) * n, "x overlaps b: x must not alias any input");
+    spai::CtxGuard guard(device);
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevCsc<double> a;
+    spai::UploadCsrDevice(ctx, n, a_nnz, a_values, a_indices, a_offsets, a);
+    spai::PcgResult result;
+    spai::PcgOnDeviceArrays(ctx, n, a, m_nnz, m_values, m_indices, m_offsets, params, b, x, result);
+    ctx.Sync();
+    return spai::FinishPcg(result, params.max_iterations, history, status);
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_pcg_adjoint_device(int64_t n, int64_t a_nnz, const double* a_values, const int64_t* a_indices,
+                                const int64_t* a_offsets, int64_t m_nnz, const double* m_values,
+                                const int64_t* m_indices, const int64_t* m_offsets, const double* x,
+                                const double* grad_x, PcgParams params, double* grad_b, double* grad_a,
+                                double* history, int64_t* status, char* error, int64_t error_capacity) {
+  try {
+    spai::CheckPcgParams(n, params);
+    if (a_nnz < 0 || m_nnz < 0) throw std::invalid_argument("nnz must be non-negative");
+    if (grad_x == nullptr) throw std::invalid_argument("grad_x must not be null");
+    if (grad_a != nullptr && x == nullptr) throw std::invalid_argument("x must not be null when grad_a is requested");
+    const int device = spai::ResolveDevice(params.device);
+    spai::DeviceScope scope(device);
+    spai::CheckDevicePointer(a_offsets, n + 1, "A offsets", device);
+    spai::CheckDevicePointer(a_indices, a_nnz, "A indices", device);
+    spai::CheckDevicePointer(a_values, a_nnz, "A values", device);
+    spai::CheckDevicePointer(m_offsets, n + 1, "M offsets", device);
+    spai::CheckDevicePointer(m_indices, m_nnz, "M indices", device);
+    spai::CheckDevicePointer(m_values, m_nnz, "M values", device);
+    spai::CheckDevicePointer(grad_x, n, "grad_x", device);
+    if (x != nullptr) spai::CheckDevicePointer(x, n, "x", device);
+    if (grad_b != nullptr) {
+      spai::CheckDevicePointer(grad_b, n, "grad_b", device);
+      spai::CheckDisjoint(grad_b, sizeof(double) * n, grad_x, sizeof(double) * n,
+                          "grad_b overlaps grad_x: outputs must not alias any input");
+      spai::CheckDisjoint(grad_b, sizeof(double) * n, x, sizeof(double) * n,
+                          "grad_b overlaps x: outputs must not alias any input");
+    }
+    if (grad_a != nullptr) spai::CheckDevicePointer(grad_a, a_nnz, "grad_a", device);
+    spai::CtxGuard guard(device);
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevCsc<double> a;
+    spai::UploadCsrDevice(ctx, n, a_nnz, a_values, a_indices, a_offsets, a);
+    // A symmetric: A^T lambda = grad_x is the forward's own solve; lambda lands in grad_b when it is asked for
+    spai::DevBuf<double> own;
+    double* lambda = grad_b;
+    if (lambda == nullptr) {
+      own.Reserve(static_cast<size_t>(n), ctx.stream);
+      lambda = own.data();
+    }
+    spai::PcgResult result;
+    spai::PcgOnDeviceArrays(ctx, n, a, m_nnz, m_values, m_indices, m_offsets, params, grad_x, lambda, result);
+    if (grad_a != nullptr && a.nnz > 0) spai::NegativeOuterOnRows(ctx, a, lambda, x, grad_a);
+    ctx.Sync();
+    return spai::FinishPcg(result, params.max_iterations, history, status);
+  } catch (const std::exception& ex) {
+    spai::CopyError(ex.what(), error, error_capacity);
+    return -1;
+  }
+}
+
+int64_t spai_residual_adjoint_device(int64_t n, int64_t a_nnz, const int64_t* a_col_offsets,
+                                     const int64_t* a_row_indices, const double* a_values, int64_t m_nnz,
+                                     const int64_t* m_col_offsets, const int64_t* m_row_indices,
+                                     const double* m_values, int64_t device, double* loss, double* grad_m,
+                                     double* grad_a, char* error, int64_t error_capacity) {
+  try {
+    if (n <= 0 || a_nnz < 0 || m_nnz < 0) throw std::invalid_argument("n must be positive and nnz non-negative");
+    if (n > static_cast<int64_t>(INT32_MAX)) {
+      throw std::invalid_argument("Sparse matrix dimensions exceed the 32-bit row index range of the device layout");
+    }
+    if (loss == nullptr) throw std::invalid_argument("loss must not be null");
+    const int dev = spai::ResolveDevice(device);
+    spai::DeviceScope scope(dev);
+    spai::CheckDevicePointer(a_col_offsets, n + 1, "A col_offsets", dev);
+    spai::CheckDevicePointer(a_row_indices, a_nnz, "A row_indices", dev);
+    spai::CheckDevicePointer(a_values, a_nnz, "A values", dev);
+    spai::CheckDevicePointer(m_col_offsets, n + 1, "M col_offsets", dev);
+    spai::CheckDevicePointer(m_row_indices, m_nnz, "M row_indices", dev);
+    spai::CheckDevicePointer(m_values, m_nnz, "M values", dev);
+    if (grad_m != nullptr) spai::CheckDevicePointer(grad_m, m_nnz, "grad_m", dev);
+    if (grad_a != nullptr) spai::CheckDevicePointer(grad_a, a_nnz, "grad_a", dev);
+    spai::CtxGuard guard(dev);
+    spai::Ctx& ctx = guard.ctx;
+    spai::DevCsc<double> ad;
+    spai::DevCsc<double> md;
+    spai::UploadCheckedDeviceCsc(ctx, spai::DeviceCscInput{n, a_nnz, a_col_offsets, a_row_indices, a_values}, ad, "A");
+    spai::UploadCheckedDeviceCsc(ctx, spai::DeviceCscInput{n, m_nnz, m_col_offsets, m_row_indices, m_values}, md, "M");
+    spai::ResidualAdjoint(ctx, ad, md, loss, grad_m, grad_a);
     ctx.Sync();
     return 0;
   } catch (const std::exception& ex) {

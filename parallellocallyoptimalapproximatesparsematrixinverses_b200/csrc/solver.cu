@@ -241,6 +241,32 @@ __global__ void NarrowIndexKernel(const int64_t* __restrict__ src, int32_t* __re
 
 }  // namespace
 
+// A canonical CSC in device memory -> out (int32 rows), checked on the device.
+void UploadCheckedDeviceCsc(Ctx& ctx, const DeviceCscInput& in, DevCsc<double>& out, const char* name) {
+  out.Shape(in.n, in.n, ctx.stream);
+  out.ReserveNnz(in.nnz, ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), in.col_offsets, sizeof(int64_t) * (in.n + 1), cudaMemcpyDeviceToDevice,
+                            ctx.stream));
+  if (in.nnz > 0) {
+    SPAI_CUDA(cudaMemcpyAsync(out.val.data(), in.values, sizeof(double) * in.nnz, cudaMemcpyDeviceToDevice,
+                              ctx.stream));
+  }
+  int32_t* bad = ctx.flags.data() + 5;
+  SPAI_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx.stream));
+  CheckNarrowCscKernel<<<GridFor(in.n, 128), 128, 0, ctx.stream>>>(in.n, in.nnz, in.col_offsets, in.row_indices,
+                                                                   out.idx.data(), bad);
+  SPAI_LAUNCH_CHECK();
+  SPAI_CUDA(cudaMemcpyAsync(ctx.host_flags + 5, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.Sync();
+  if (ctx.host_flags[5] & 1) {
+    throw std::invalid_argument(std::string(name) + ": column offsets must run from 0 to nnz without decreasing");
+  }
+  if (ctx.host_flags[5] & 2) {
+    throw std::invalid_argument(std::string(name) +
+                                ": row indices must lie in [0, n) and increase strictly in every column");
+  }
+}
+
 template <class T>
 void UploadCsc(Ctx& ctx, const HostCsc& h, DevCsc<T>& d, DevBuf<int64_t>& stage_idx, DevBuf<double>& stage_val) {
   d.Shape(h.rows, h.cols, ctx.stream);
@@ -680,30 +706,8 @@ class Solver final : public SolverBase {
     SPAI_LAUNCH_CHECK();
   }
 
-  // A canonical CSC in device memory -> out (int32 rows), checked on the device.
   void CopyCheckedFromDevice(const DeviceCscInput& in, DevCsc<double>& out, const char* name) {
-    out.Shape(in.n, in.n, ctx_.stream);
-    out.ReserveNnz(in.nnz, ctx_.stream);
-    SPAI_CUDA(cudaMemcpyAsync(out.ptr.data(), in.col_offsets, sizeof(int64_t) * (in.n + 1), cudaMemcpyDeviceToDevice,
-                              ctx_.stream));
-    if (in.nnz > 0) {
-      SPAI_CUDA(cudaMemcpyAsync(out.val.data(), in.values, sizeof(double) * in.nnz, cudaMemcpyDeviceToDevice,
-                                ctx_.stream));
-    }
-    int32_t* bad = ctx_.flags.data() + 5;
-    SPAI_CUDA(cudaMemsetAsync(bad, 0, sizeof(int32_t), ctx_.stream));
-    CheckNarrowCscKernel<<<GridFor(in.n, 128), 128, 0, ctx_.stream>>>(in.n, in.nnz, in.col_offsets, in.row_indices,
-                                                                      out.idx.data(), bad);
-    SPAI_LAUNCH_CHECK();
-    SPAI_CUDA(cudaMemcpyAsync(ctx_.host_flags + 5, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, ctx_.stream));
-    ctx_.Sync();
-    if (ctx_.host_flags[5] & 1) {
-      throw std::invalid_argument(std::string(name) + ": column offsets must run from 0 to nnz without decreasing");
-    }
-    if (ctx_.host_flags[5] & 2) {
-      throw std::invalid_argument(std::string(name) +
-                                  ": row indices must lie in [0, n) and increase strictly in every column");
-    }
+    UploadCheckedDeviceCsc(ctx_, in, out, name);
   }
 
   // ELL copies of A when no row or column of A holds more than kMaxEllWidth entries.

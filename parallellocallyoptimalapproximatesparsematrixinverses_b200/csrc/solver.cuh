@@ -137,6 +137,8 @@ void UploadCsc(Ctx& ctx, const HostCsc& h, DevCsc<T>& d, DevBuf<int64_t>& stage_
 // Validation shared by the C entry points (reference methods_c_api.cpp:16-40,
 // methods_common.cpp:12-48); throws std::invalid_argument with the reference's messages.
 HostCsc CheckedMatrix(const MatrixData& data);
+// A canonical CSC in device memory -> out (int32 rows), checked on the device; throws with `name`.
+void UploadCheckedDeviceCsc(Ctx& ctx, const DeviceCscInput& in, DevCsc<double>& out, const char* name);
 void ValidateProblem(const HostCsc& a, const HostCsc* m0, const HostCsc* pr, const MethodParams& p);
 
 }  // namespace spai

@@ -128,3 +128,80 @@ def test_residual_objective_autograd(require_gpu):
             fm = adjoint.residual_objective(a - h * da, m - h * dm, a_pattern, m_pattern).item()
         got = ((a.grad @ da + m.grad @ dm) / 3.0).item()
         assert got == pytest.approx((fp - fm) / (2 * h), rel=1e-6)
+
+
+def test_autograd_on_cuda_tensors_stays_on_the_device_and_matches_the_host_path(require_gpu):
+    """CUDA tensors go through the device entry points (no host copies of the
+    values): the same bits as the host path, gradients on the device."""
+    import torch
+    dev = torch.device("cuda:0")
+    A = adjoint_oracle.canonical_csc(problems.diffusion_2d(14, 1.0, 6))
+    M = _m_from_mr(A, 6)
+    a_pattern, m_pattern = (A.indptr, A.indices), (M.indptr, M.indices)
+    grads = {}
+    for where in ("cpu", dev):
+        a = torch.from_numpy(A.data.copy()).to(where).requires_grad_(True)
+        m = torch.from_numpy(M.data.copy()).to(where).requires_grad_(True)
+        f = adjoint.residual_objective(a, m, a_pattern, m_pattern)
+        (2.0 * f).backward()
+        assert f.device.type == a.grad.device.type == m.grad.device.type == torch.device(where).type
+        grads[str(where)] = (f.item(), a.grad.cpu().numpy(), m.grad.cpu().numpy())
+    assert grads["cpu"][0] == grads["cuda:0"][0]
+    assert np.array_equal(grads["cpu"][1], grads["cuda:0"][1]) and np.array_equal(grads["cpu"][2], grads["cuda:0"][2])
+
+    R = sparse.csr_matrix(problems.diffusion_2d(20, 1.0, 7))
+    R.sort_indices()
+    P = sparse.csr_matrix(problems.diagonal_inverse(R))
+    rng = np.random.default_rng(4)
+    x_t = rng.standard_normal(R.shape[0])
+    b0 = R @ x_t
+    solve = dict(a_indices=R.indices, a_offsets=R.indptr, m_values=P.data, m_indices=P.indices, m_offsets=P.indptr,
+                 max_iterations=4000, tolerance=1e-12, refresh_period=9)
+    out = {}
+    for where in ("cpu", dev):
+        a = torch.from_numpy(R.data.copy()).to(where).requires_grad_(True)
+        b = torch.from_numpy(b0.copy()).to(where).requires_grad_(True)
+        x = adjoint.pcg_solve(a, b, **solve)
+        assert x.device.type == torch.device(where).type
+        loss = torch.sum((x - torch.from_numpy(x_t).to(where)) ** 2)
+        loss.backward()
+        out[str(where)] = (x.detach().cpu().numpy(), a.grad.cpu().numpy(), b.grad.cpu().numpy())
+    for h, d in zip(out["cpu"], out["cuda:0"]):
+        assert np.array_equal(h, d)
+
+
+def test_device_entry_points_reject_host_pointers_and_aliases(require_gpu):
+    import ctypes
+
+    import torch
+    from parallellocallyoptimalapproximatesparsematrixinverses_b200 import _lib
+    A = sparse.csr_matrix(problems.laplacian_2d(8))
+    n = A.shape[0]
+    dev = torch.device("cuda:0")
+    t = lambda v: torch.from_numpy(np.ascontiguousarray(v)).to(dev)  # noqa: E731
+    av, ai, ao = t(A.data), t(A.indices.astype(np.int64)), t(A.indptr.astype(np.int64))
+    b = torch.ones(n, dtype=torch.float64, device=dev)
+    p = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    params = _lib.PcgParams(100, 1e-10, 0, 0, 0, 0)
+    hist = np.zeros(100)
+    status = ctypes.c_int64(0)
+    err = _lib.error_buffer()
+    lib = _lib.load()
+    torch.cuda.synchronize()
+    rc = lib.spai_pcg_device(n, av.numel(), p(av), p(ai), p(ao), av.numel(), p(av), p(ai), p(ao), p(b), params,
+                             hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(status), p(b), err,
+                             len(err))
+    assert rc == -1 and b"x overlaps b" in err.value
+    host_b = np.ones(n)
+    x = torch.empty(n, dtype=torch.float64, device=dev)
+    rc = lib.spai_pcg_device(n, av.numel(), p(av), p(ai), p(ao), av.numel(), p(av), p(ai), p(ao),
+                             ctypes.c_void_p(host_b.ctypes.data), params,
+                             hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(status), p(x), err,
+                             len(err))
+    assert rc == -1 and b"b must point to device memory" in err.value
+    bad = ao.clone()
+    bad[3] = bad[4] + 1
+    rc = lib.spai_pcg_device(n, av.numel(), p(av), p(ai), p(bad), av.numel(), p(av), p(ai), p(ao), p(b), params,
+                             hist.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(status), p(x), err,
+                             len(err))
+    assert rc == -1 and b"CSR offsets" in err.value
