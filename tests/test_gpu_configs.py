@@ -9,7 +9,7 @@
   off-diagonals per row, diagonal 1.05 x row sum), 5 outer x 10 inner, top-12:
   FP64 bit for bit against the oracle at n = 2^11, and the mixed error at
   n = 2^14.  n = 2^20 does not fit one GPU: the inner products Z = M_outer R
-  and A Z are not dropped (inner_outer_common.hpp:40-60), and with random
+  and A Z are not dropped (inner_outer_common.hpp:41-42), and with random
   long-range couplings A Z holds tens of thousands of entries per column
   after the first outer iteration -- about 10^10 entries at n = 2^20 -- which
   the whole-matrix products cannot hold in 180 GB.
