@@ -515,60 +515,8 @@ __device__ __forceinline__ double SumStaged(double s, const double* src, int cou
   return s;
 }
 
-// Row i of A (its ELL copy: columns and values) and pr_i, held in registers so
-// that a round of rows can be loaded while the previous round is summed.
 template <class T, int kEll>
-struct EllRow {
-  int4 k[kEll / 4];
-  T v[kEll];
-  T pr;
-};
-
-template <class T, int kEll>
-__device__ __forceinline__ void FetchRow(const FusedArgs<T>& a, int32_t i, EllRow<T, kEll>& row) {
-  const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
-  const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
-#pragma unroll
-  for (int u = 0; u < kEll / 4; ++u) {
-    row.k[u] = ks[u];
-    T v4[4];
-    LoadFour(vs + 4 * u, v4);
-#pragma unroll
-    for (int e = 0; e < 4; ++e) row.v[4 * u + e] = v4[e];
-  }
-  row.pr = a.pr[i];
-}
-
-// sum over the entries k of row i of A, in ascending k, of A(i, k) B(k, j), B(:, j) in a bucketed hash
-template <class T, int kEll>
-__device__ __forceinline__ T RowTimesColumn(const EllRow<T, kEll>& row, const int32_t* keys, const T* vals, int bits,
-                                            bool displaced) {
-  T acc = T(-0.0);
-#pragma unroll
-  for (int u = 0; u < kEll / 4; ++u) {
-    const int32_t kk[4] = {row.k[u].x, row.k[u].y, row.k[u].z, row.k[u].w};
-#pragma unroll
-    for (int e = 0; e < 4; ++e) {
-      T bv;
-      if (kk[e] >= 0 && BucketFind(keys, vals, bits, displaced, kk[e], bv)) acc = Add(acc, Mul(row.v[4 * u + e], bv));
-    }
-  }
-  return acc;
-}
-
-// Rows are fetched a round ahead when a row's values take at most 32 bytes
-// (FP32 with ELL <= 8, FP64 with ELL 4): the second row set then fits in
-// registers at five blocks per SM; wider rows are fetched in their round, at
-// up to seven blocks per SM (shared memory allows six).
-template <class T, int kEll>
-struct ResidualShape {
-  static constexpr bool kAhead = kEll * sizeof(T) <= 32;
-  static constexpr int kMinBlocks = kAhead ? 5 : 7;
-};
-
-template <class T, int kEll>
-__global__ void __launch_bounds__(kResidualWarps * kWarp, (ResidualShape<T, kEll>::kMinBlocks))
-    FusedResidualKernel(FusedArgs<T> a) {
+__global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(FusedArgs<T> a) {
   extern __shared__ __align__(16) unsigned char fused_res_smem[];
   const int lane = threadIdx.x & 31;
   constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
@@ -652,86 +600,46 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp, (ResidualShape<T, kEll
       }
       __syncwarp();
       const int count = DrainRows(bm, summary, SummaryWords(words), rows, lane);
-      if constexpr (ResidualShape<T, kEll>::kAhead) {
-        // rows of A fetched one round ahead of the round that uses them (ResidualShape)
-        EllRow<T, kEll> next;
-        int32_t i_next = 0;
-        if (lane < count) {
-          i_next = seg_lo + static_cast<int32_t>(rows[lane]);
-          FetchRow(a, i_next, next);
-        }
-        for (int r0 = 0; r0 < count; r0 += kWarp) {
-          const int r = r0 + lane;
-          const int32_t i = i_next;
-          const EllRow<T, kEll> row = next;
-          if (r + kWarp < count) {
-            i_next = seg_lo + static_cast<int32_t>(rows[r + kWarp]);
-            FetchRow(a, i_next, next);
-          }
-          bool keep = false;
-          T v = T(0);
-          if (r < count) {
-            v = -RowTimesColumn(row, mkeys, mvals, mbits, m_displaced);
-            if (static_cast<int64_t>(i) == j) v = Add(v, T(1));
-            const double sd = static_cast<double>(v);
-            stage0[lane] = Mul(sd, sd);
-            keep = !(v == T(0));  // Eigen prune(0.0)
-          }
-          const unsigned mask = __ballot_sync(0xffffffffu, keep);
-          if (keep) {
-            const int o = kept + __popc(mask & LaneMaskBelow());
-            const T z = Mul(row.pr, v);
-            zr_out[o] = i;
-            zv_out[o] = z;
-            z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
-          }
-          kept += __popc(mask);
-          __syncwarp();
-          if (lane == 0) sq = SumStaged(sq, stage0, min(kWarp, count - r0));
-          __syncwarp();
-        }
-      } else {
-        for (int r0 = 0; r0 < count; r0 += kWarp) {
-          const int r = r0 + lane;
-          bool keep = false;
-          int32_t i = 0;
-          T v = T(0);
-          if (r < count) {
-            i = seg_lo + static_cast<int32_t>(rows[r]);
-            T acc = T(-0.0);
-            const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
-            const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
+      for (int r0 = 0; r0 < count; r0 += kWarp) {
+        const int r = r0 + lane;
+        bool keep = false;
+        int32_t i = 0;
+        T v = T(0);
+        if (r < count) {
+          i = seg_lo + static_cast<int32_t>(rows[r]);
+          T acc = T(-0.0);
+          const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
+          const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
 #pragma unroll
-            for (int u = 0; u < kEll / 4; ++u) {
-              const int4 k4 = ks[u];
-              T v4[4];
-              LoadFour(vs + 4 * u, v4);
-              const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+          for (int u = 0; u < kEll / 4; ++u) {
+            const int4 k4 = ks[u];
+            T v4[4];
+            LoadFour(vs + 4 * u, v4);
+            const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
 #pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                T bv;
-                if (kk[e] >= 0 && BucketFind(mkeys, mvals, mbits, m_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
-              }
+            for (int e = 0; e < 4; ++e) {
+              T bv;
+              if (kk[e] >= 0 && BucketFind(mkeys, mvals, mbits, m_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
             }
-            v = -acc;
-            if (static_cast<int64_t>(i) == j) v = Add(v, T(1));
-            const double sd = static_cast<double>(v);
-            stage0[lane] = Mul(sd, sd);
-            keep = !(v == T(0));  // Eigen prune(0.0)
           }
-          const unsigned mask = __ballot_sync(0xffffffffu, keep);
-          if (keep) {
-            const int o = kept + __popc(mask & LaneMaskBelow());
-            const T z = Mul(a.pr[i], v);
-            zr_out[o] = i;
-            zv_out[o] = z;
-            z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
-          }
-          kept += __popc(mask);
-          __syncwarp();
-          if (lane == 0) sq = SumStaged(sq, stage0, min(kWarp, count - r0));
-          __syncwarp();
+          v = -acc;
+          if (static_cast<int64_t>(i) == j) v = Add(v, T(1));
+          const double sd = static_cast<double>(v);
+          stage0[lane] = Mul(sd, sd);
+          keep = !(v == T(0));  // Eigen prune(0.0)
         }
+        const unsigned mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) {
+          const int o = kept + __popc(mask & LaneMaskBelow());
+          const T z = Mul(a.pr[i], v);
+          zr_out[o] = i;
+          zv_out[o] = z;
+          z_placed &= BucketInsert(zkeys, zvals, zbits, i, z);
+        }
+        kept += __popc(mask);
+        __syncwarp();
+        if (lane == 0) sq = SumStaged(sq, stage0, min(kWarp, count - r0));
+        __syncwarp();
       }
     }
     if (lane == 0) {
@@ -778,67 +686,36 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp, (ResidualShape<T, kEll
       }
       __syncwarp();
       const int count2 = DrainRows(bm, summary, SummaryWords(words2), rows, lane);
-      if constexpr (ResidualShape<T, kEll>::kAhead) {
-        EllRow<T, kEll> next;
-        int32_t i_next = 0;
-        if (lane < count2) {
-          i_next = seg_lo + static_cast<int32_t>(rows[lane]);
-          FetchRow(a, i_next, next);
-        }
-        for (int r0 = 0; r0 < count2; r0 += kWarp) {
-          const int r = r0 + lane;
-          const int32_t i = i_next;
-          const EllRow<T, kEll> row = next;
-          if (r + kWarp < count2) {
-            i_next = seg_lo + static_cast<int32_t>(rows[r + kWarp]);
-            FetchRow(a, i_next, next);
-          }
-          if (r < count2) {
-            const T acc = RowTimesColumn(row, zkeys, zvals, zbits, z_displaced);
-            const double td = static_cast<double>(Mul(row.pr, acc));
-            T zi;
-            stage0[lane] = Mul(td, td);
-            // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
-            stage1[lane] = BucketFind(zkeys, zvals, zbits, z_displaced, i, zi) ? Mul(static_cast<double>(zi), td) : 0.0;
-          }
-          __syncwarp();
-          // lane 0 extends tt and lane 1 bt, side by side in one instruction stream
-          const int span = min(kWarp, count2 - r0);
-          if (lane < 2) proj = SumStaged(proj, lane == 0 ? stage0 : stage1, span);
-          __syncwarp();
-        }
-      } else {
-        for (int r0 = 0; r0 < count2; r0 += kWarp) {
-          const int r = r0 + lane;
-          if (r < count2) {
-            const int32_t i = seg_lo + static_cast<int32_t>(rows[r]);
-            T acc = T(-0.0);
-            const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
-            const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
+      for (int r0 = 0; r0 < count2; r0 += kWarp) {
+        const int r = r0 + lane;
+        if (r < count2) {
+          const int32_t i = seg_lo + static_cast<int32_t>(rows[r]);
+          T acc = T(-0.0);
+          const int4* ks = reinterpret_cast<const int4*>(a.a_rows_ell + static_cast<int64_t>(i) * kEll);
+          const T* vs = a.a_rows_ell_val + static_cast<int64_t>(i) * kEll;
 #pragma unroll
-            for (int u = 0; u < kEll / 4; ++u) {
-              const int4 k4 = ks[u];
-              T v4[4];
-              LoadFour(vs + 4 * u, v4);
-              const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
+          for (int u = 0; u < kEll / 4; ++u) {
+            const int4 k4 = ks[u];
+            T v4[4];
+            LoadFour(vs + 4 * u, v4);
+            const int32_t kk[4] = {k4.x, k4.y, k4.z, k4.w};
 #pragma unroll
-              for (int e = 0; e < 4; ++e) {
-                T bv;
-                if (kk[e] >= 0 && BucketFind(zkeys, zvals, zbits, z_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
-              }
+            for (int e = 0; e < 4; ++e) {
+              T bv;
+              if (kk[e] >= 0 && BucketFind(zkeys, zvals, zbits, z_displaced, kk[e], bv)) acc = Add(acc, Mul(v4[e], bv));
             }
-            const double td = static_cast<double>(Mul(a.pr[i], acc));
-            T zi;
-            stage0[lane] = Mul(td, td);
-            // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
-            stage1[lane] = BucketFind(zkeys, zvals, zbits, z_displaced, i, zi) ? Mul(static_cast<double>(zi), td) : 0.0;
           }
-          __syncwarp();
-          // lane 0 extends tt and lane 1 bt, side by side in one instruction stream
-          const int span = min(kWarp, count2 - r0);
-          if (lane < 2) proj = SumStaged(proj, lane == 0 ? stage0 : stage1, span);
-          __syncwarp();
+          const double td = static_cast<double>(Mul(a.pr[i], acc));
+          T zi;
+          stage0[lane] = Mul(td, td);
+          // rows of Z absent from the product add +0.0, which leaves a sum started at +0.0 unchanged
+          stage1[lane] = BucketFind(zkeys, zvals, zbits, z_displaced, i, zi) ? Mul(static_cast<double>(zi), td) : 0.0;
         }
+        __syncwarp();
+        // lane 0 extends tt and lane 1 bt, side by side in one instruction stream
+        const int span = min(kWarp, count2 - r0);
+        if (lane < 2) proj = SumStaged(proj, lane == 0 ? stage0 : stage1, span);
+        __syncwarp();
       }
     }
     if (lane == 0) a.tt[j] = proj;

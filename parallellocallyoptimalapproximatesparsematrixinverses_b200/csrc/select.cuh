@@ -222,17 +222,7 @@ inline __device__ void KeepLargest(DropSlab& s, int count, int64_t col, int cand
 // in row order by one lane, the diagonal always kept, exact zeros dropped,
 // then at most topk entries (topk > 0) by the largest (|v|, row).  Leaves
 // s.keep[i] set for the survivors and returns their number.
-//
-// The row-order sum is a chain of 2 * count dependent operations on one lane,
-// and it decides only entries within a few ulps of the cut.  So the squares
-// are first summed by all lanes in any order: both sums of count <= 256
-// nonnegative squares lie within 2 * 256 * 2^-53 < 1e-13 (relative) of the
-// exact one, so when no nonzero entry has |v| within 1e-12 (relative) of
-// eps * sqrt(that sum), every entry falls on the same side of the exact
-// threshold as of the estimate and the row-order sum is not needed.  It is
-// still formed (and used) whenever an entry lies in that band, or the
-// estimate is not a finite normal number: the decisions are the same either way.
-inline __device__ double RowOrderThreshold(const DropSlab& s, int count, int lane) {
+inline __device__ int DecideDrops(DropSlab& s, int count, int64_t j, int64_t topk, int lane) {
   double thr = 0.0;
   if (lane == 0) {
     double sq = 0.0;
@@ -246,29 +236,7 @@ inline __device__ double RowOrderThreshold(const DropSlab& s, int count, int lan
     if (i < count) sq = Add(sq, Mul(s.vals[i], s.vals[i]));
     thr = Mul(kDblEps, sqrt(sq));
   }
-  return __shfl_sync(0xffffffffu, thr, 0);
-}
-
-inline __device__ int DecideDrops(DropSlab& s, int count, int64_t j, int64_t topk, int lane) {
-  double part = 0.0;
-  for (int i = lane; i < count; i += kWarp) part = Add(part, Mul(s.vals[i], s.vals[i]));
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) part = Add(part, __shfl_xor_sync(0xffffffffu, part, o));
-  double thr;
-  if (!(part >= 1e-280 && part <= 1e280)) {
-    thr = RowOrderThreshold(s, count, lane);
-  } else {
-    const double estimate = Mul(kDblEps, sqrt(part));
-    const double band_lo = estimate * (1.0 - 1e-12);
-    const double band_hi = estimate * (1.0 + 1e-12);
-    bool near = false;
-    for (int i = lane; i < count; i += kWarp) {
-      const double a = fabs(s.vals[i]);
-      near |= a != 0.0 && a >= band_lo && a <= band_hi;
-    }
-    // outside the band an entry compares with the exact threshold as with band_hi
-    thr = __any_sync(0xffffffffu, near) ? RowOrderThreshold(s, count, lane) : band_hi;
-  }
+  thr = __shfl_sync(0xffffffffu, thr, 0);
   int kept = 0;
   bool has_diag = false;
   for (int base = 0; base < count; base += kWarp) {
