@@ -38,9 +38,9 @@ constexpr int kDropWarps = 4;       // warps per block of the drop kernel
 constexpr int kDropWindowWords = 512;  // bitmap words of the drop kernel: windows of 16,384 rows
 constexpr int kDropWindowRows = kDropWindowWords * 32;
 constexpr int kResidualWarps = 4;   // warps per block of the residual kernel
-constexpr int kWindowWords = 512;   // bitmap words of the residual kernel: windows of 16,384 rows
+constexpr int kWindowWords = 1024;  // bitmap words of the residual kernel: windows of 32,768 rows
 constexpr int kWindowRows = kWindowWords * 32;
-constexpr int kRowsCap = 1024;      // bound on a product column's row list (cap_z * longest column of A)
+constexpr int kRowsCap = 1024;      // longest row list of one product column
 constexpr int kMaxTopK = 32;
 constexpr int kDropRowsCap = 512;  // candidate rows of one drop column; also bounds Z's slots per column
 
@@ -89,7 +89,6 @@ struct FusedArgs {
   int ell;  // ELL slots of A (multiple of 4)
   int m_hash_slots;   // residual kernel: M(:, j)
   int z_hash_slots;   // residual kernel: Z(:, j)
-  int res_rows;       // residual kernel: row list (cap_z * longest column of A)
   int d_mt_slots;     // drop kernel: M(j, :)
   int d_r_slots;      // drop kernel: R(j, :)
   int64_t max_iterations;
@@ -493,9 +492,9 @@ __global__ void __launch_bounds__(kDropWarps * kWarp) FusedDropKernel(FusedArgs<
 // accumulator started at -0.0, sums sequential in row order on one lane.
 
 template <class T>
-__host__ __device__ size_t ResidualSlabBytes(int m_slots, int z_slots, int rows) {
+__host__ __device__ size_t ResidualSlabBytes(int m_slots, int z_slots) {
   return Round16(static_cast<size_t>(kWindowWords) * 4) + Round16(static_cast<size_t>(SummaryWords(kWindowWords)) * 4) +
-         Round16(static_cast<size_t>(rows) * 2) + Round16(static_cast<size_t>(m_slots) * 4) +
+         Round16(static_cast<size_t>(kRowsCap) * 2) + Round16(static_cast<size_t>(m_slots) * 4) +
          Round16(static_cast<size_t>(m_slots) * sizeof(T)) + Round16(static_cast<size_t>(z_slots) * 4) +
          Round16(static_cast<size_t>(z_slots) * sizeof(T)) + 2 * Round16(kWarp * sizeof(double));
 }
@@ -521,14 +520,13 @@ __global__ void __launch_bounds__(kResidualWarps * kWarp) FusedResidualKernel(Fu
   extern __shared__ __align__(16) unsigned char fused_res_smem[];
   const int lane = threadIdx.x & 31;
   constexpr int kSummary = (kWindowWords + kWarp * kWarp - 1) / (kWarp * kWarp) * kWarp;
-  unsigned char* base =
-      fused_res_smem + (threadIdx.x >> 5) * ResidualSlabBytes<T>(a.m_hash_slots, a.z_hash_slots, a.res_rows);
+  unsigned char* base = fused_res_smem + (threadIdx.x >> 5) * ResidualSlabBytes<T>(a.m_hash_slots, a.z_hash_slots);
   uint32_t* bm = reinterpret_cast<uint32_t*>(base);
   base += Round16(static_cast<size_t>(kWindowWords) * 4);
   uint32_t* summary = reinterpret_cast<uint32_t*>(base);
   base += Round16(static_cast<size_t>(kSummary) * 4);
   uint16_t* rows = reinterpret_cast<uint16_t*>(base);
-  base += Round16(static_cast<size_t>(a.res_rows) * 2);
+  base += Round16(static_cast<size_t>(kRowsCap) * 2);
   int32_t* mkeys = reinterpret_cast<int32_t*>(base);
   base += Round16(static_cast<size_t>(a.m_hash_slots) * 4);
   T* mvals = reinterpret_cast<T*>(base);
@@ -1068,8 +1066,6 @@ class FusedMr final : public FusedMrBase {
     a.ell = p.ell_width;
     a.m_hash_slots = NextPow2Int(std::max(4 * p.topk, kWarp));
     a.z_hash_slots = NextPow2Int(std::max(2 * cap_z, kWarp));
-    // a window's rows: at most cap_z (residual) or cap_z * longest column of A (projection)
-    a.res_rows = static_cast<int>(std::min<int64_t>(static_cast<int64_t>(cap_z) * p.a_longest, kRowsCap));
     a.d_mt_slots = NextPow2Int(std::max(2 * cap_mt, kWarp));
     a.d_r_slots = DropRowSlots(p);
     a.max_iterations = p.max_iterations;
@@ -1107,7 +1103,7 @@ class FusedMr final : public FusedMrBase {
     bool same = x.n == y.n && x.topk == y.topk && x.cap_z == y.cap_z && x.cap_mt == y.cap_mt &&
                 x.ell == y.ell && x.m_hash_slots == y.m_hash_slots && x.d_r_slots == y.d_r_slots &&
                 x.d_mt_slots == y.d_mt_slots &&
-                x.z_hash_slots == y.z_hash_slots && x.res_rows == y.res_rows && x.max_iterations == y.max_iterations &&
+                x.z_hash_slots == y.z_hash_slots && x.max_iterations == y.max_iterations &&
                 x.tolerance == y.tolerance && x.a_cols_ell == y.a_cols_ell && x.a_rows_ell == y.a_rows_ell &&
                 x.a_rows_ell_val == y.a_rows_ell_val && x.pr == y.pr && x.m_rows == y.m_rows &&
                 x.m_vals == y.m_vals && x.m_cnt == y.m_cnt && x.z_rows == y.z_rows && x.z_vals == y.z_vals &&
@@ -1131,8 +1127,7 @@ class FusedMr final : public FusedMrBase {
     }
     drop_smem_ = static_cast<size_t>(kDropWarps) *
                  DropWarpBytes<T>(args_.topk + args_.cap_z, args_.d_mt_slots, args_.d_r_slots);
-    res_smem_ = static_cast<size_t>(kResidualWarps) *
-                ResidualSlabBytes<T>(args_.m_hash_slots, args_.z_hash_slots, args_.res_rows);
+    res_smem_ = static_cast<size_t>(kResidualWarps) * ResidualSlabBytes<T>(args_.m_hash_slots, args_.z_hash_slots);
     SPAI_CUDA(cudaFuncSetAttribute(FusedDropKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    static_cast<int>(drop_smem_)));
     SPAI_CUDA(cudaFuncSetAttribute(res_kernel_, cudaFuncAttributeMaxDynamicSharedMemorySize,
