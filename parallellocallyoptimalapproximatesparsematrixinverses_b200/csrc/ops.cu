@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <vector>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -785,29 +786,145 @@ __global__ void SegmentSortBlockKernel(const int64_t* __restrict__ ptr, int64_t 
   }
 }
 
-// Segments longer than the shared-memory cap: insertion sort in global memory
-// (one thread per segment; only reached by very dense columns).
+// Segments longer than the shared-memory cap (rows of very dense columns):
+// chunks of kBlockSortCap entries are sorted in shared memory, then the sorted
+// runs are merged in pairs through a scratch copy, pass after pass.  The keys
+// of one segment are distinct (the column indices of one row), so an entry's
+// place in a merged pair is its place in its own run plus the number of keys
+// of the other run below it, found by binary search: every entry moves
+// independently.  `starts` / `lens` list the long segments only.
 template <class T>
-__global__ void SegmentSortLongKernel(const int64_t* __restrict__ ptr, int64_t segments, int32_t* __restrict__ idx,
-                                      T* __restrict__ val) {
-  for (int64_t s = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; s < segments;
-       s += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const int64_t start = ptr[s];
-    const int64_t end = ptr[s + 1];
-    if (end - start <= kBlockSortCap) continue;
-    for (int64_t i = start + 1; i < end; ++i) {
-      const int32_t key = idx[i];
-      const T v = val[i];
-      int64_t j = i - 1;
-      while (j >= start && idx[j] > key) {
-        idx[j + 1] = idx[j];
-        val[j + 1] = val[j];
-        --j;
+__global__ void LongChunkSortKernel(const int64_t* __restrict__ starts, const int64_t* __restrict__ lens, int64_t count,
+                                    int32_t* __restrict__ idx, T* __restrict__ val) {
+  extern __shared__ unsigned char smem_raw[];
+  int32_t* keys = reinterpret_cast<int32_t*>(smem_raw);
+  T* vals = reinterpret_cast<T*>(smem_raw + kBlockSortCap * sizeof(int32_t));
+  for (int64_t s = blockIdx.y; s < count; s += gridDim.y) {
+    const int64_t len = lens[s];
+    for (int64_t c0 = static_cast<int64_t>(blockIdx.x) * kBlockSortCap; c0 < len;
+         c0 += static_cast<int64_t>(gridDim.x) * kBlockSortCap) {
+      const int64_t start = starts[s] + c0;
+      const int n = static_cast<int>(len - c0 < kBlockSortCap ? len - c0 : kBlockSortCap);
+      int size = 1;
+      while (size < n) size <<= 1;
+      for (int i = threadIdx.x; i < size; i += blockDim.x) {
+        keys[i] = i < n ? idx[start + i] : INT32_MAX;
+        vals[i] = i < n ? val[start + i] : T(0);
       }
-      idx[j + 1] = key;
-      val[j + 1] = v;
+      __syncthreads();
+      BitonicSortPairs(keys, vals, size, threadIdx.x, blockDim.x, true);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        idx[start + i] = keys[i];
+        val[start + i] = vals[i];
+      }
+      __syncthreads();
     }
   }
+}
+
+// Number of keys in sorted keys[0, n) below key.
+__device__ __forceinline__ int64_t CountBelow(const int32_t* keys, int64_t n, int32_t key) {
+  int64_t lo = 0;
+  int64_t hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (keys[mid] < key) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+// One merge pass over runs of `width` entries: src -> dst (same offsets).
+template <class T>
+__global__ void LongMergeKernel(const int64_t* __restrict__ starts, const int64_t* __restrict__ lens, int64_t count,
+                                int64_t width, const int32_t* __restrict__ src_idx, const T* __restrict__ src_val,
+                                int32_t* __restrict__ dst_idx, T* __restrict__ dst_val) {
+  for (int64_t s = blockIdx.y; s < count; s += gridDim.y) {
+    const int64_t start = starts[s];
+    const int64_t len = lens[s];
+    for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < len;
+         q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      const int64_t pair = q / (2 * width) * (2 * width);
+      const int64_t mid = pair + width < len ? pair + width : len;
+      const int64_t end = pair + 2 * width < len ? pair + 2 * width : len;
+      const int32_t key = src_idx[start + q];
+      const int64_t place = q < mid ? (q - pair) + CountBelow(src_idx + start + mid, end - mid, key)
+                                    : (q - mid) + CountBelow(src_idx + start + pair, mid - pair, key);
+      dst_idx[start + pair + place] = key;
+      dst_val[start + pair + place] = src_val[start + q];
+    }
+  }
+}
+
+template <class T>
+__global__ void LongCopyKernel(const int64_t* __restrict__ starts, const int64_t* __restrict__ lens, int64_t count,
+                               const int32_t* __restrict__ src_idx, const T* __restrict__ src_val,
+                               int32_t* __restrict__ dst_idx, T* __restrict__ dst_val) {
+  for (int64_t s = blockIdx.y; s < count; s += gridDim.y) {
+    for (int64_t q = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; q < lens[s];
+         q += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+      dst_idx[starts[s] + q] = src_idx[starts[s] + q];
+      dst_val[starts[s] + q] = src_val[starts[s] + q];
+    }
+  }
+}
+
+template <class T>
+void SortLongSegments(Ctx& ctx, const int64_t* ptr, int64_t segments, int32_t* idx, T* val, int64_t longest) {
+  // the long segments, listed on the host (this path serves only very dense columns)
+  std::vector<int64_t> h_ptr(static_cast<size_t>(segments + 1));
+  SPAI_CUDA(cudaMemcpyAsync(h_ptr.data(), ptr, sizeof(int64_t) * (segments + 1), cudaMemcpyDeviceToHost, ctx.stream));
+  ctx.Sync();
+  std::vector<int64_t> list;  // starts, then lengths
+  std::vector<int64_t> lengths;
+  for (int64_t s = 0; s < segments; ++s) {
+    const int64_t len = h_ptr[s + 1] - h_ptr[s];
+    if (len > kBlockSortCap) {
+      list.push_back(h_ptr[s]);
+      lengths.push_back(len);
+    }
+  }
+  const int64_t count = static_cast<int64_t>(list.size());
+  if (count == 0) return;
+  list.insert(list.end(), lengths.begin(), lengths.end());
+  DevBuf<int64_t> table;
+  table.Reserve(list.size(), ctx.stream);
+  SPAI_CUDA(cudaMemcpyAsync(table.data(), list.data(), sizeof(int64_t) * list.size(), cudaMemcpyHostToDevice,
+                            ctx.stream));
+  const int64_t* starts = table.data();
+  const int64_t* lens = table.data() + count;
+  const unsigned grid_y = static_cast<unsigned>(count < 65535 ? count : 65535);
+  const size_t block_smem = kBlockSortCap * (sizeof(int32_t) + sizeof(T));
+  SPAI_CUDA(cudaFuncSetAttribute(LongChunkSortKernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(block_smem)));
+  const unsigned chunks = static_cast<unsigned>((longest + kBlockSortCap - 1) / kBlockSortCap);
+  LongChunkSortKernel<T><<<dim3(chunks, grid_y), 1024, block_smem, ctx.stream>>>(starts, lens, count, idx, val);
+  SPAI_LAUNCH_CHECK();
+  // scratch at the same offsets as the segments
+  DevBuf<int32_t> scratch_idx;
+  DevBuf<T> scratch_val;
+  scratch_idx.Reserve(static_cast<size_t>(h_ptr[segments]), ctx.stream);
+  scratch_val.Reserve(static_cast<size_t>(h_ptr[segments]), ctx.stream);
+  int32_t* src_idx = idx;
+  T* src_val = val;
+  int32_t* dst_idx = scratch_idx.data();
+  T* dst_val = scratch_val.data();
+  const unsigned grid_x = static_cast<unsigned>(std::min<int64_t>((longest + 255) / 256, 4096));
+  for (int64_t width = kBlockSortCap; width < longest; width *= 2) {
+    LongMergeKernel<T><<<dim3(grid_x, grid_y), 256, 0, ctx.stream>>>(starts, lens, count, width, src_idx, src_val,
+                                                                     dst_idx, dst_val);
+    SPAI_LAUNCH_CHECK();
+    std::swap(src_idx, dst_idx);
+    std::swap(src_val, dst_val);
+  }
+  if (src_idx != idx) {
+    LongCopyKernel<T><<<dim3(grid_x, grid_y), 256, 0, ctx.stream>>>(starts, lens, count, src_idx, src_val, idx, val);
+    SPAI_LAUNCH_CHECK();
+  }
+  ctx.Sync();  // the table and the scratch are released on return
 }
 
 // Sorts every segment [ptr[s], ptr[s+1]) by index; `longest` bounds the
@@ -830,10 +947,7 @@ void SortSegments(Ctx& ctx, const int64_t* ptr, int64_t segments, int32_t* idx, 
                                                                                                val);
     SPAI_LAUNCH_CHECK();
   }
-  if (longest > kBlockSortCap) {
-    SegmentSortLongKernel<T><<<GridFor(segments, 128), 128, 0, ctx.stream>>>(ptr, segments, idx, val);
-    SPAI_LAUNCH_CHECK();
-  }
+  if (longest > kBlockSortCap) SortLongSegments(ctx, ptr, segments, idx, val, longest);
 }
 
 // ---------------------------------------------------------------------------

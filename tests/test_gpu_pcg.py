@@ -77,3 +77,23 @@ def test_pcg_rejects_an_out_of_range_column(require_gpu):
     hist, status = backward_error.pcg(A.data, A.indices, A.indptr, M.data, M.indices, M.indptr,
                                       np.ones(A.shape[0]), 50, 1, 1e-8)
     assert status == 1
+
+
+def test_pcg_symmetric_part_with_a_row_longer_than_the_shared_memory_sort(require_gpu):
+    """(M + M^T)/2 on the device when M has a dense column: its transpose has a
+    row of n > 8,192 entries, which the transpose sorts by chunks and merge
+    passes (three chunks here).  The device preconditioner must equal scipy's
+    (M + M^T) * 0.5, so PCG with it matches PCG given scipy's result, bit for bit."""
+    A = _csr(problems.laplacian_2d(142))
+    n = A.shape[0]
+    assert n > 2 * 8192
+    rng = np.random.default_rng(6)
+    dense_column = sparse.csr_matrix((1e-4 * rng.standard_normal(n), (np.arange(n), np.full(n, 7))), shape=(n, n))
+    M = _csr(problems.diagonal_inverse(A) + dense_column)
+    S = _csr((M + M.T) * 0.5)
+    b, _ = problems.solution_rhs(A, seed=3)
+    h1, s1 = backward_error.pcg(A.data, A.indices, A.indptr, M.data, M.indices, M.indptr, b, 800, 1, 1e-8,
+                                symmetric_part=True)
+    h2, s2 = backward_error.pcg(A.data, A.indices, A.indptr, S.data, S.indices, S.indptr, b, 800, 1, 1e-8)
+    assert s1 == s2
+    assert np.array_equal(h1.view(np.int64), h2.view(np.int64))
