@@ -62,7 +62,7 @@ RUNS = {
     ("dropping", 100, "0.030", "wathen100"): 5,
     ("dropping", 1000, "0.030", "bcsstk21"): 100,
     ("dropping", 500, "0.030", "4bw100eigs20k"): 50,
-    ("dropping", 500, "0.030", "bundle1"): 10,
+    ("dropping", 500, "0.030", "bundle1"): 5,
     ("dropping", 500, "0.030", "rand20k"): 5,
     ("dropping", 500, "0.030", "rand20k2"): 3,
     ("dropping", 500, "0.030", "tri100eigs4k"): None,
